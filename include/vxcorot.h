@@ -1,0 +1,233 @@
+/*
+ * vxcorot.h — C ABI of the B200 corotational elastic solve.
+ *
+ * This is the drop-in boundary for the Voxel-sim solver (TheLastie/Voxel-sim).
+ * In the reference, control crosses to the GPU in one place,
+ * `cuda_solver::solve_pcg` (src/cuda_solver.rs:301-309), called from
+ * `solve_coupled` (src/solver.rs:1778-1786). Everything else on the hot path
+ * (rotation fit, bond assembly, bond stress) runs on the host there. Here every
+ * part of the path has an entry point:
+ *
+ *   vx_solve_pcg_f32            replaces cuda_solver::solve_pcg (same arguments,
+ *                               same layouts, same convergence rule)
+ *   vx_fit_rotations            replaces solver::fit_rotations (src/solver.rs:327-417)
+ *   vx_corotational_pass        replaces solver::solve_coupled (src/solver.rs:1542-1929):
+ *                               assembly (make_constraint, :1325-1345), RHS/diagonal
+ *                               (:1576-1636), block-Jacobi PCG (:1833-1911),
+ *                               position update (:1921-1923)
+ *   vx_bond_stress              replaces the stress/limit part of the fracture loop
+ *                               (src/solver.rs:627-665 -> bond_limits :124-158 ->
+ *                               fracture::pair_limits / update, src/fracture.rs:76-133,
+ *                               :210-292)
+ *
+ * Conventions
+ *   - Every function returns an int32_t status (VX_OK = 0). No exception crosses
+ *     the boundary. vx_last_error() returns a thread-local message that names
+ *     the failing operation, like the reference's Err(String).
+ *   - Host pointers are borrowed for the duration of the call only.
+ *   - Vectors are xyz-interleaved (3 values per REV, like glam::Vec3 slices);
+ *     quaternions are xyzw (glam::Quat); 3x3 matrices are row-major, which is
+ *     the packing of src/solver.rs:1741-1751.
+ *   - Per-bond arrays are axis-major: bond (axis, i) is element axis*n + i, the
+ *     layout of Scene::bonds (src/scene.rs:322), whose owner is the lower
+ *     endpoint i and whose partner is neighbor[axis*n + i] (the +axis cell).
+ *   - VX_EMPTY (u32::MAX, src/bond.rs:2) marks a missing neighbour.
+ *   - A scene handle is single-threaded: calls on one handle must not overlap.
+ */
+#ifndef VXCOROT_H
+#define VXCOROT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VX_EMPTY 0xFFFFFFFFu
+#define VX_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+    VX_OK = 0,
+    VX_NOT_CONVERGED = 1, /* iteration cap reached above tolerance (outputs still written) */
+    VX_NONFINITE = 2,     /* NaN/Inf in an input or produced by the solve */
+    VX_OOM = 3,           /* device allocation failed or admission refused */
+    VX_BAD_INPUT = 4,     /* invalid argument (null pointer, size, index) */
+    VX_CUDA_ERROR = 5,    /* a CUDA runtime call failed */
+    VX_TIMEOUT = 6,       /* a bounded device-side wait ran out */
+    VX_NO_DEVICE = 7      /* no CUDA device, or the device was lost */
+};
+
+/* Fracture modes, src/material.rs:3-8. */
+enum { VX_BRITTLE = 0, VX_DUCTILE = 1, VX_MIXED = 2 };
+
+/* Precision forms of a corotational pass. */
+enum {
+    VX_PRECISION_FP64 = 0,  /* plain FP64 block-Jacobi PCG */
+    VX_PRECISION_MIXED = 1  /* FP32 inner PCG inside FP64 iterative refinement */
+};
+
+/*
+ * Material fields read by the stiffness and limit laws: the subset of
+ * material::Material (src/material.rs:20-63) that tensor_compliance
+ * (src/solver.rs:37-63), bond_thermal_rest (:78-95) and pair_limits
+ * (src/fracture.rs:76-133) use. Values are the f32 values of the reference.
+ */
+typedef struct vx_material {
+    float density;
+    float young;
+    float young_perp;
+    float shear;
+    float tensile_strength;
+    float tensile_strength_perp;
+    float compressive_strength;
+    float compressive_strength_perp;
+    float shear_strength;
+    float shear_strength_perp;
+    float yield_strength;
+    float hardening_modulus;
+    float failure_plastic_strain;
+    float fracture_energy;
+    float fracture_energy_perp;
+    float thermal_expansion_parallel;
+    float thermal_expansion_perpendicular;
+    int32_t fracture_mode; /* VX_BRITTLE / VX_DUCTILE / VX_MIXED */
+} vx_material;
+
+/*
+ * One scene (a REV lattice). Mirrors the fields of Scene (src/scene.rs:309-351)
+ * and Voxel (src/voxel.rs:7-21) that the elastic solve reads. Phase-dependent
+ * values (solid fraction, pre-melt strength scale, temperature change since
+ * creation) are derived by the host from its thermal state, as
+ * Material::phase_state / thermal_strength_scale do (src/material.rs:485-565).
+ * Optional arrays may be NULL (then zero, or one for solid/thermal_strength).
+ */
+typedef struct vx_scene_desc {
+    uint32_t n;                       /* REV count */
+    const double* position;           /* 3n, metres */
+    const double* rotation;           /* 4n xyzw, or NULL = identity */
+    const uint8_t* kinematic;         /* n, Voxel::kinematic */
+    const float* mass;                /* n, kg (density * CELL^3) */
+    const uint32_t* material;         /* n, index into materials */
+    const vx_material* materials;
+    uint32_t material_count;
+    const float* fiber;               /* 3n, Microstructure::fibers() = orientation * Z */
+    const float* anisotropy;          /* n, Microstructure::anisotropy */
+    const float* solid_fraction;      /* n or NULL (1) */
+    const float* thermal_strength;    /* n or NULL (1) */
+    const float* thermal_delta;       /* n or NULL (0): T - T_reference, kelvin */
+    const uint32_t* neighbor;         /* 3n axis-major, Bond::neighbor */
+    const float* formation_offset;    /* 9n ((axis*n+i)*3+c) or NULL */
+    const float* plastic_strain;      /* 9n or NULL */
+    const float* damage;              /* 3n or NULL */
+} vx_scene_desc;
+
+/* Parameters of one corotational pass (one call of solve_coupled). */
+typedef struct vx_pass_params {
+    double h;                    /* substep length, s (fixed_dt / substeps, src/solver.rs:475) */
+    double tolerance;            /* relative residual target */
+    uint32_t max_iterations;     /* PCG iteration cap (inner iterations for MIXED) */
+    int32_t precision;           /* VX_PRECISION_FP64 or VX_PRECISION_MIXED */
+    int32_t reuse_preconditioner;/* 1: keep the block-Jacobi inverse of the previous pass
+                                    (CPU path, src/solver.rs:554 and :1639) */
+    double inner_tolerance;      /* MIXED only: relative target of each FP32 inner solve
+                                    (0 = default 1e-4) */
+    uint32_t max_outer;          /* MIXED only: refinement cap (0 = default 30) */
+} vx_pass_params;
+
+typedef struct vx_pass_stats {
+    uint32_t iterations;         /* PCG iterations (FP32 inner iterations for MIXED) */
+    uint32_t outer_iterations;   /* FP64 refinement steps (MIXED), else 1 */
+    double residual;             /* recursive relative residual |r|/|r0| (FP64 form), as
+                                    Scene::solver_residual (src/solver.rs:1882) */
+    double true_residual;        /* |b - A dx|/|b| recomputed in FP64 with the FP64 operator */
+    uint32_t active;             /* REVs with at least one free axis */
+    uint32_t bonds_assembled;    /* bonds that entered the system */
+    int32_t converged;
+} vx_pass_stats;
+
+/* Last error message of the calling thread ("" when none). */
+const char* vx_last_error(void);
+int32_t vx_abi_version(void);
+
+/*
+ * Compatibility shim: the exact contract of cuda_solver::solve_pcg
+ * (src/cuda_solver.rs:301-501). Inputs are the engine's packed active-REV
+ * system (src/solver.rs:1731-1777): rhs[3n], neighbors[6n] (VX_EMPTY = unused
+ * slot), diagonal[9n], blocks[54n] (six row-major 3x3 off-diagonal blocks per
+ * row), inverse_diagonal[9n]. Block-Jacobi PCG with f32 vectors, f64 dot
+ * accumulation and f32 alpha/beta; the residual |r|/|b| is checked every 16
+ * iterations and at the cap, converging when <= tolerance. Returns VX_OK with
+ * out_dx[3n] written, or VX_NOT_CONVERGED / VX_NONFINITE (out_dx still written)
+ * where the reference returns Err and the engine falls back.
+ */
+int32_t vx_solve_pcg_f32(const float* rhs, const uint32_t* neighbors, const float* diagonal,
+                         const float* blocks, const float* inverse_diagonal, uint32_t n,
+                         uint32_t max_iterations, float tolerance, float* out_dx,
+                         uint32_t* out_iterations, float* out_relative);
+
+/* Device context (one per GPU and host thread of control). */
+typedef struct vx_ctx vx_ctx;
+typedef struct vx_scene vx_scene;
+
+int32_t vx_ctx_create(int32_t device, vx_ctx** out_ctx);
+int32_t vx_ctx_destroy(vx_ctx* ctx);
+
+/*
+ * Bond topology from lattice cells, on the device: for each REV i and axis,
+ * neighbor[axis*n+i] = the REV at cell + e_axis when both have the same
+ * kinematic flag, else VX_EMPTY. Same indices as Scene::from_voxels
+ * (src/scene.rs:558-570) and Scene::new (:1668-1681). cells[3n] are integer
+ * lattice coordinates and must be unique.
+ */
+int32_t vx_build_topology(vx_ctx* ctx, const int32_t* cells, const uint8_t* kinematic,
+                          uint32_t n, uint32_t* out_neighbor);
+
+int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* desc, vx_scene** out_scene);
+int32_t vx_scene_destroy(vx_scene* scene);
+/* Device bytes held by a scene of n REVs (admission estimate). */
+uint64_t vx_scene_footprint_bytes(uint32_t n);
+
+int32_t vx_scene_set_positions(vx_scene* scene, const double* xyz);
+int32_t vx_scene_get_positions(vx_scene* scene, double* xyz);
+int32_t vx_scene_set_rotations(vx_scene* scene, const double* xyzw);
+int32_t vx_scene_get_rotations(vx_scene* scene, double* xyzw);
+/*
+ * Axis targets of this substep (the merged persistent + per-step targets of
+ * src/solver.rs:449-460). mask[i] bit a set = axis a of REV i is targeted;
+ * a targeted axis leaves the PCG system (free = 0, src/solver.rs:1554-1565).
+ * xyz may be NULL when only the mask matters.
+ */
+int32_t vx_scene_set_targets(vx_scene* scene, const uint8_t* mask, const double* xyz);
+/* Applied nodal loads in newtons (applied_loads, src/solver.rs:461-474). */
+int32_t vx_scene_set_loads(vx_scene* scene, const double* xyz);
+/* Predicted positions of this substep (src/solver.rs:542); NULL = current positions. */
+int32_t vx_scene_set_predicted(vx_scene* scene, const double* xyz);
+/* Bond state written by fracture (neighbor, plastic strain, damage, formation offset). */
+int32_t vx_scene_set_bonds(vx_scene* scene, const uint32_t* neighbor, const float* plastic_strain,
+                           const float* damage, const float* formation_offset);
+int32_t vx_scene_get_neighbors(vx_scene* scene, uint32_t* neighbor);
+
+/* Polar-decomposition rotation fit; returns the largest angle change (rad). */
+int32_t vx_fit_rotations(vx_scene* scene, double* out_max_angle);
+
+/* One corotational pass: assemble, solve, x += dx. */
+int32_t vx_corotational_pass(vx_scene* scene, const vx_pass_params* params, vx_pass_stats* out);
+
+/*
+ * Stress ratio of every bond against its directional limits, evaluated with
+ * the frames and undamaged stiffness of the last pass and the current
+ * rotations and positions (src/solver.rs:627-647). ratio[3n] (axis-major);
+ * -1 where the fracture loop skips the bond (no neighbour, kinematic owner,
+ * or not part of the last assembly). Bonds with |ratio - 1| <= 1e-6 are
+ * listed in near[] (bond index axis*n+i, at most cap) and counted in
+ * *near_count. force[9n] (or NULL) receives Bond workspace last_force, N.
+ */
+int32_t vx_bond_stress(vx_scene* scene, float* ratio, float* force, uint32_t* near,
+                       uint32_t cap, uint32_t* near_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VXCOROT_H */
