@@ -1,0 +1,387 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 corotational elastic solve (PCG DOF-iterations per second).
+
+One step = one fixed step of the 64^3 mixed-material block (262,144 REVs,
+wood/iron/stone/aluminium, bottom layer fixed, gravity -9.81, dt 1 ms): the
+rotation fit, 5 corotational passes (assembly + FP32 inner block-Jacobi PCG
+inside FP64 iterative refinement to a true relative residual of 1e-8, the
+rotation re-fit between passes) and the bond-stress evaluation. Every step
+starts from the same resident state (device-side checkpoint restore).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With --gpus N > 1 it runs under torchrun with one rank per GPU; every rank
+solves its own scene (weak scaling, no data-path collective) and the device
+time is the max over ranks. --impl reference times the reference's own CPU
+block-Jacobi PCG loop (restated f32 port, all host threads) on the same
+system and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "voxel-sim_b200"), str(ROOT / "oracle")]
+
+import numpy as np  # noqa: E402
+
+BYTES_PER_REV = {  # canonical algorithmic bytes per active REV and PCG iteration
+    "matvec_f32": 136, "update_f32": 108, "direction_f32": 36,
+    "matvec_f64": 256, "update_f64": 216, "direction_f64": 72,
+}
+METRIC = "PCG DOF-iters/s (FP32 inner PCG in FP64 refinement to 1e-8)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixed_block", choices=["mixed_block", "wood_cube", "damaged_lattice"])
+    ap.add_argument("--edge", type=int, default=None)
+    ap.add_argument("--passes", type=int, default=None)
+    ap.add_argument("--tolerance", type=float, default=1e-8)
+    ap.add_argument("--max-iterations", type=int, default=50000)
+    ap.add_argument("--cpu-iterations", type=int, default=40, help="PCG iterations per CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def build_workload(name, edge, seed):
+    from vxsim import scenes as S
+    if name == "mixed_block":
+        return S.mixed_block(edge or 64, seed=seed)
+    if name == "wood_cube":
+        return S.wood_cube(edge or 10)
+    return S.damaged_lattice(edge or 160, seed=seed)
+
+
+def predicted_positions(scene, h, gravity):
+    """Explicit prediction of src/solver.rs:500-523 from rest (v0 = 0)."""
+    g = np.asarray(gravity, np.float64)
+    v = np.zeros_like(scene.position)
+    free = scene.kinematic == 0
+    v[free] = g * h
+    for a in range(3):
+        v[((scene.target_mask >> a) & 1).astype(bool), a] = 0.0
+    x = scene.position + v * h
+    for a in range(3):
+        m = ((scene.target_mask >> a) & 1).astype(bool)
+        x[m, a] = scene.target[m, a]
+    return x
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    p = ROOT / "profiles" / "roofline_traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_rate(scene, h, pred, iterations, threads):
+    """The reference's CPU block-Jacobi PCG loop (f32 port) on pass 0 of the scene."""
+    import pyoracle as O
+    o = O.OracleScene(scene)
+    o.fit_rotations()
+    o.assemble(h, pred)
+    rows = o.pack_rows()
+    dof = 3 * rows["n"]
+    t0 = time.perf_counter()
+    _, it, _ = O.pcg_rows_f32(rows, iterations, 0.0, threads)
+    dt = time.perf_counter() - t0
+    return rows, dof, it, dt
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import pyoracle as O
+    scene = build_workload(args.workload, args.edge, seed=1)
+    meta = scene.meta
+    h = meta["dt"] / meta["substeps"]
+    pred = predicted_positions(scene, h, meta["gravity"])
+    threads = os.cpu_count() or 1
+    o = O.OracleScene(scene)
+    o.fit_rotations()
+    o.assemble(h, pred)
+    rows = o.pack_rows()
+    dof = 3 * rows["n"]
+    for _ in range(args.warmup):
+        O.pcg_rows_f32(rows, max(2, args.cpu_iterations // 4), 0.0, threads)
+    total_it, total_s = 0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, it, _ = O.pcg_rows_f32(rows, args.cpu_iterations, 0.0, threads)
+        total_s += time.perf_counter() - t0
+        total_it += it
+    value = dof * total_it / total_s
+    sample = (f"{args.cpu_iterations} iterations per step of the reference's CPU block-Jacobi PCG loop "
+              f"(src/solver.rs:1833-1911, restated in C, f32 vectors, f64 dots) on pass 0 of {meta['workload']} "
+              f"{meta.get('edge')}^3 ({rows['n']} active REVs)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF-iter/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n, "dof_active": dof},
+        "cpu_baseline": {"value": value, "unit": "DOF-iter/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "DOF-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def our_arm(args):
+    import torch
+    from vxsim import native as N
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+
+    scene = build_workload(args.workload, args.edge, seed=1 + rank)
+    meta = scene.meta
+    passes = args.passes or meta["passes"]
+    h = meta["dt"] / meta["substeps"]
+    pred = predicted_positions(scene, h, meta["gravity"])
+    free_dof = int(scene.free_mask().sum())
+    active = scene.active_count()
+    precision = N.PRECISION_MIXED
+
+    ctx = N.Context(local)
+    ds = N.DeviceScene(ctx, scene)
+    ds.set_predicted(pred)
+    ds.save_state()
+    ext = torch.cuda.ExternalStream(ds.stream_ptr, device=torch.device("cuda", local))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step(fetch=False):
+        ds.restore_state()
+        ds.fit_rotations()
+        it = 0
+        launches = 1
+        worst = 0.0
+        for p in range(passes):
+            st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision)
+            it += st["iterations"]
+            launches += st["kernel_launches"]
+            worst = max(worst, st["true_residual"])
+            if p + 1 < passes:
+                ds.fit_rotations()
+                launches += 1
+        ds.bond_stress(with_force=False, with_ratio=fetch)
+        launches += 1
+        return it, launches, worst
+
+    for _ in range(args.warmup):
+        step()
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    total_ms, total_it, total_launch, worst = 0.0, 0, 0, 0.0
+    for k in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.fill_(k & 0xFF)  # L2 flush between timed steps
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        it, launches, w = step()
+        e1.record(ext)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        total_it += it
+        total_launch += launches
+        worst = max(worst, w)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+
+    # aggregate: max device time over ranks, summed work
+    dof_iters = float(free_dof) * total_it
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        w_ = torch.tensor([dof_iters, float(passes * args.steps)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(w_, op=dist.ReduceOp.SUM)
+        job_ms = float(t.item())
+        job_dof_iters, job_solves = float(w_[0].item()), float(w_[1].item())
+    else:
+        job_ms, job_dof_iters, job_solves = total_ms, dof_iters, float(passes * args.steps)
+    value = job_dof_iters / (job_ms / 1000.0)
+
+    # kernel roofline (cold L2 and in-solve warm L2), CUDA events on the scene stream
+    cold = ds.kernel_times(precision, reps=20, flush_ptr=flush.data_ptr(), flush_bytes=flush.numel())
+    warm = ds.kernel_times(precision, reps=20)
+    peak, peak_kind = measured_peak()
+    mv_bytes = BYTES_PER_REV["matvec_f32"] * active
+    achieved = mv_bytes / (cold["matvec_us"] * 1e-6) / 1e9
+    traffic = None
+    prof = profiled_traffic()
+    if prof and "matvec_f32_dram_bytes_per_rev" in prof:
+        traffic = prof["matvec_f32_dram_bytes_per_rev"] * scene.n
+
+    # end to end through the C ABI with host buffers (pinned staging inside the library)
+    e2e = None
+    if not args.no_e2e:
+        x0 = np.ascontiguousarray(scene.position)
+        q0 = np.ascontiguousarray(scene.rotation)
+        e2e_ms, e2e_it = 0.0, 0
+        h2d = scene.n * (24 * 4 + 32 + 1)
+        d2h = scene.n * (24 + 12)
+        for k in range(max(1, min(args.steps, 3))):
+            with torch.cuda.stream(ext):
+                flush.fill_(k & 0xFF)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            ds.set_positions(x0)
+            ds.set_rotations(q0)
+            ds.set_predicted(pred)
+            ds.set_targets(scene.target_mask, scene.target)
+            ds.set_loads(scene.loads)
+            ds.fit_rotations()
+            it = 0
+            for p in range(passes):
+                st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision)
+                it += st["iterations"]
+                if p + 1 < passes:
+                    ds.fit_rotations()
+            out = ds.bond_stress(with_force=False)
+            xs = ds.positions()
+            e1.record(ext)
+            e1.synchronize()
+            e2e_ms += e0.elapsed_time(e1)
+            e2e_it += it
+            assert np.all(np.isfinite(xs)) and out["ratio"].shape == (3, scene.n)
+        e2e_value = float(free_dof) * e2e_it / (e2e_ms / 1000.0) * world
+        e2e = {"value": e2e_value, "unit": "DOF-iter/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_ms / max(1, min(args.steps, 3))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rows, dof, it, dt = cpu_reference_rate(scene, h, pred, args.cpu_iterations, threads)
+        cpu = {"value": dof * it / dt, "unit": "DOF-iter/s", "cores": threads, "kind": "port",
+               "sample": f"{it} iterations of the reference's CPU block-Jacobi PCG loop (f32 restatement, "
+                         f"OpenMP) on pass 0 of this workload, {rows['n']} active REVs"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "DOF-iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n,
+                       "dof_nominal": 3 * scene.n, "dof_active": free_dof, "passes": passes,
+                       "tolerance": args.tolerance, "precision": "FP32 inner PCG, FP64 refinement",
+                       "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
+            "solves_per_s": job_solves / (job_ms / 1000.0),
+            "iterations_per_solve": total_it / (passes * args.steps),
+            "worst_true_residual": worst,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": "k_matvec<float>",
+                         "bytes_per_launch": mv_bytes, "launch_us_cold_l2": cold["matvec_us"],
+                         "launch_us_warm_l2": warm["matvec_us"], "update_us_cold_l2": cold["update_us"],
+                         "update_us_warm_l2": warm["update_us"], "peak_source": f"{peak_kind} hbm_gbs"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": total_launch,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    ds.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return our_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

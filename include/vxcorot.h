@@ -145,6 +145,7 @@ typedef struct vx_pass_stats {
     uint32_t active;             /* REVs with at least one free axis */
     uint32_t bonds_assembled;    /* bonds that entered the system */
     int32_t converged;
+    uint32_t kernel_launches;    /* kernels this pass launched (early-exit ones included) */
 } vx_pass_stats;
 
 /* Last error message of the calling thread ("" when none). */
@@ -226,6 +227,23 @@ int32_t vx_corotational_pass(vx_scene* scene, const vx_pass_params* params, vx_p
  */
 int32_t vx_bond_stress(vx_scene* scene, float* ratio, float* force, uint32_t* near,
                        uint32_t cap, uint32_t* near_count);
+
+/* ---- state checkpoint and measurement hooks (no counterpart in the reference) ---- */
+
+/* op 0 saves the scene's positions and rotations on the device, op 1 restores them. */
+int32_t vx_scene_checkpoint(vx_scene* scene, int32_t op);
+/* The scene's CUDA stream (a cudaStream_t), for callers that order or time work around it. */
+void* vx_scene_stream(vx_scene* scene);
+/*
+ * Average device time of one launch of the PCG matvec and update kernels on the
+ * scene's assembled system (precision VX_PRECISION_FP64 or VX_PRECISION_MIXED
+ * for the FP32 kernels), timed with CUDA events on the scene stream over reps
+ * launches each. When flush_bytes > 0 the device buffer flush is overwritten
+ * before every timed launch so the kernels read from HBM, not L2.
+ * out_us[0] = matvec, out_us[1] = update, in microseconds.
+ */
+int32_t vx_scene_kernel_times(vx_scene* scene, int32_t precision, uint32_t reps, void* flush,
+                              uint64_t flush_bytes, double* out_us);
 
 #ifdef __cplusplus
 }

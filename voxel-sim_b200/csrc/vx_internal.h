@@ -1,0 +1,146 @@
+// vx_internal.h — host-side structures behind the C ABI (include/vxcorot.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/vxcorot.h"
+
+namespace vx {
+
+// Thread-local error message returned by vx_last_error().
+void set_error(const char* fmt, ...);
+void clear_error();
+
+// Device-side recurrence scalars of one PCG solve (FP64 or FP32 inner).
+struct PcgScalars {
+    double rz;          // r . z of the current iterate
+    double pap;         // p . Ap
+    double rr;          // r . r
+    double initial;     // |r0|
+    double alpha;
+    double beta;
+    double residual;    // |r| / |r0|
+    double tolerance;   // stop when residual < tolerance
+    double b_norm;      // |b| (outer FP64 residual)
+    double r64_norm;    // |b - A x| (outer)
+    uint32_t max_iterations;
+    uint32_t iterations;
+    int32_t done;       // 1 = stop issuing work
+    int32_t status;     // VX_OK, VX_NOT_CONVERGED, VX_NONFINITE
+    uint32_t counter[4];  // last-block tickets of the fused reductions
+};
+
+// Per-bond storage of the last assembly (SoA, bond e = axis * n + i).
+struct BondArrays {
+    double* k64;        // [18][n]  world K (sym6) per axis, 0 if not assembled
+    float* k32;         // [18][n]
+    double* mat_k;      // [6][3n]  undamaged local K (sym6) for stress
+    double4* frame_q;   // [3n]     bond frame quaternion (slerp midpoint)
+    double* force;      // [3][3n]  K (x_j - x_i - rest) of assembled bonds
+    uint8_t* state;     // [3n]     0 none, 1 fracture only, 2 assembled
+};
+
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0;
+    size_t used = 0;
+    template <typename T>
+    T* take(size_t count) {
+        size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        T* p = reinterpret_cast<T*>(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+}  // namespace vx
+
+struct vx_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+};
+
+struct vx_scene {
+    vx_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    uint32_t blocks = 0;          // grid of the per-REV kernels (256 threads)
+    cudaStream_t stream = nullptr;
+    vx::Arena arena;
+
+    // REV state
+    double* pos;                  // [3][n]
+    double* pred;                 // [3][n]
+    double* loads;                // [3][n]
+    double* target;               // [3][n]
+    double4* rot;                 // [n]
+    uint8_t* kin;                 // [n]
+    uint8_t* tmask;               // [n]
+    uint8_t* flags;               // [n] free axes (bit a)
+    float4* param0;               // [n] fibre xyz, anisotropy
+    float4* param1;               // [n] solid, thermal strength, thermal delta, mass
+    uint32_t* matid;              // [n]
+    vx_material* materials;       // [material_count]
+    uint32_t material_count;
+    uint32_t* nbr;                // [3][n]
+    uint32_t* rev;                // [3][n]
+    float4* bond_a;               // [3n] formation xyz, damage
+    float4* bond_b;               // [3n] plastic xyz, equivalent plastic strain
+
+    vx::BondArrays bonds;
+
+    // assembled system
+    double* d64;                  // [6][n] projected diagonal block
+    double* dinv64;               // [6][n]
+    float* d32;
+    float* dinv32;
+    double* b64;                  // [3][n]
+
+    // solver vectors
+    double* x64;                  // [3][n] correction dx
+    double* r64;
+    double* z64;
+    double* p64[2];
+    double* ap64;
+    float* x32;
+    float* r32;
+    float* z32;
+    float* p32[2];
+    float* ap32;
+    double* save_pos;             // [3][n] checkpoint
+    double4* save_rot;            // [n]
+    float* out_ratio;             // [3n] bond stress outputs
+    float* out_force;             // [9n]
+    uint32_t* out_near;           // [3n]
+    double* partials;             // [4 * blocks]
+    vx::PcgScalars* sc;           // device scalars (FP64 solve / outer)
+    vx::PcgScalars* sc32;         // device scalars (FP32 inner solve)
+    unsigned long long* max_angle_bits;
+    uint32_t* near_count;
+    uint32_t* bond_count;         // bonds assembled by the last pass
+
+    // host mirrors
+    double* h_stage = nullptr;       // pinned staging of host copies [4n doubles]
+    vx::PcgScalars* h_sc = nullptr;  // pinned
+    int32_t* h_done = nullptr;       // pinned [2]
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+
+    // cached CUDA graphs of PCG iteration chunks
+    cudaGraphExec_t chunk64 = nullptr;
+    cudaGraphExec_t chunk32 = nullptr;
+
+    uint32_t launches = 0;        // kernels launched by the current pass
+    uint32_t active = 0;          // REVs with a free axis (cached per target set)
+    bool active_cached = false;
+    bool assembled = false;
+    bool have_dinv = false;
+};
+
+namespace vx {
+uint64_t scene_bytes(uint32_t n, uint32_t material_count);
+}

@@ -1,0 +1,56 @@
+// vx_kernels.h — launchers of the corotational-solve kernels.
+#pragma once
+
+#include "vx_internal.h"
+
+namespace vx {
+
+// Plain-pointer view of a scene passed by value to kernels.
+struct SceneView {
+    uint32_t n;
+    const double* pos;
+    const double* pred;
+    const double* loads;
+    const double4* rot;
+    const uint8_t* kin;
+    const uint8_t* flags;
+    const float4* param0;
+    const float4* param1;
+    const uint32_t* matid;
+    const vx_material* materials;
+    const uint32_t* nbr;
+    const uint32_t* rev;
+    const float4* bond_a;
+    const float4* bond_b;
+};
+
+SceneView view_of(const vx_scene* s);
+
+// free-axis flags from kinematic flags and target masks
+cudaError_t launch_flags(vx_scene* s);
+// reverse neighbour table rev[a][j] = i where nbr[a][i] == j
+cudaError_t launch_reverse_neighbors(vx_scene* s);
+// dense-grid topology build (vx_build_topology)
+cudaError_t launch_topology(const int32_t* d_cells, const uint8_t* d_kin, uint32_t n, const int32_t* lo,
+                            const int32_t* ext, int32_t* d_grid, uint32_t* d_nbr, uint32_t* d_dup,
+                            cudaStream_t stream);
+// polar-decomposition rotation fit; writes the max angle bits to s->max_angle_bits
+cudaError_t launch_fit_rotations(vx_scene* s);
+// bond and REV assembly of one pass (h = substep)
+cudaError_t launch_assembly(vx_scene* s, double h, bool reuse_preconditioner);
+// x += dx for active axes
+cudaError_t launch_apply_correction(vx_scene* s);
+// bond stress / ratio / force
+cudaError_t launch_bond_stress(vx_scene* s, float* d_ratio, float* d_force, uint32_t* d_near, uint32_t cap);
+
+// PCG drivers (vx_pcg.cu)
+int32_t solve_fp64(vx_scene* s, double tolerance, uint32_t max_iterations, vx_pass_stats* out);
+int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, double inner_tolerance,
+                    uint32_t max_outer, vx_pass_stats* out);
+// |b - A x64| / |b| with the FP64 operator (device scalars updated)
+int32_t true_residual(vx_scene* s, double* out);
+// CUDA-event timing of the matvec and update kernels (microseconds per launch)
+int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush, uint64_t flush_bytes,
+                     double* out_us);
+
+}  // namespace vx

@@ -1,0 +1,316 @@
+"""ctypes binding of libvxcorot.so (the C ABI declared in include/vxcorot.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+import numpy as np
+
+from . import materials as M
+
+PKG = Path(__file__).resolve().parents[1]
+ROOT = PKG.parent
+LIB_PATH = PKG / "lib" / "libvxcorot.so"
+HEADER = ROOT / "include" / "vxcorot.h"
+
+VX_OK, VX_NOT_CONVERGED, VX_NONFINITE, VX_OOM, VX_BAD_INPUT, VX_CUDA_ERROR, VX_TIMEOUT, VX_NO_DEVICE = range(8)
+PRECISION_FP64, PRECISION_MIXED = 0, 1
+EMPTY = 0xFFFFFFFF
+
+u8p = C.POINTER(C.c_uint8)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+f32p = C.POINTER(C.c_float)
+f64p = C.POINTER(C.c_double)
+
+
+class VxError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+class VxMaterial(C.Structure):
+    _fields_ = [(name, C.c_float) for name in M.MATERIAL_DTYPE.names[:-1]] + [("fracture_mode", C.c_int32)]
+
+
+class VxSceneDesc(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint32), ("position", f64p), ("rotation", f64p), ("kinematic", u8p), ("mass", f32p),
+        ("material", u32p), ("materials", C.POINTER(VxMaterial)), ("material_count", C.c_uint32),
+        ("fiber", f32p), ("anisotropy", f32p), ("solid_fraction", f32p), ("thermal_strength", f32p),
+        ("thermal_delta", f32p), ("neighbor", u32p), ("formation_offset", f32p), ("plastic_strain", f32p),
+        ("damage", f32p),
+    ]
+
+
+class VxPassParams(C.Structure):
+    _fields_ = [("h", C.c_double), ("tolerance", C.c_double), ("max_iterations", C.c_uint32),
+                ("precision", C.c_int32), ("reuse_preconditioner", C.c_int32), ("inner_tolerance", C.c_double),
+                ("max_outer", C.c_uint32)]
+
+
+class VxPassStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("outer_iterations", C.c_uint32), ("residual", C.c_double),
+                ("true_residual", C.c_double), ("active", C.c_uint32), ("bonds_assembled", C.c_uint32),
+                ("converged", C.c_int32), ("kernel_launches", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/vxcorot.h."""
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vx_[a-z0-9_]+)\s*\(", text)))
+
+
+def load(path: Path | None = None):
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path or os.environ.get("VXCOROT_LIB", LIB_PATH))
+    if not p.exists():
+        raise RuntimeError(f"libvxcorot.so not built at {p}; run __graft_entry__.build() or make -C voxel-sim_b200")
+    L = C.CDLL(str(p))
+    L.vx_last_error.restype = C.c_char_p
+    L.vx_abi_version.restype = C.c_int32
+    L.vx_ctx_create.argtypes = [C.c_int32, C.POINTER(C.c_void_p)]
+    L.vx_ctx_destroy.argtypes = [C.c_void_p]
+    L.vx_build_topology.argtypes = [C.c_void_p, i32p, u8p, C.c_uint32, u32p]
+    L.vx_scene_create.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), C.POINTER(C.c_void_p)]
+    L.vx_scene_destroy.argtypes = [C.c_void_p]
+    L.vx_scene_footprint_bytes.restype = C.c_uint64
+    L.vx_scene_footprint_bytes.argtypes = [C.c_uint32]
+    for name in ("vx_scene_set_positions", "vx_scene_get_positions", "vx_scene_set_rotations",
+                 "vx_scene_get_rotations", "vx_scene_set_loads", "vx_scene_set_predicted"):
+        getattr(L, name).argtypes = [C.c_void_p, f64p]
+    L.vx_scene_set_targets.argtypes = [C.c_void_p, u8p, f64p]
+    L.vx_scene_set_bonds.argtypes = [C.c_void_p, u32p, f32p, f32p, f32p]
+    L.vx_scene_get_neighbors.argtypes = [C.c_void_p, u32p]
+    L.vx_fit_rotations.argtypes = [C.c_void_p, f64p]
+    L.vx_corotational_pass.argtypes = [C.c_void_p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
+    L.vx_bond_stress.argtypes = [C.c_void_p, f32p, f32p, u32p, C.c_uint32, u32p]
+    L.vx_solve_pcg_f32.argtypes = [f32p, u32p, f32p, f32p, f32p, C.c_uint32, C.c_uint32, C.c_float, f32p, u32p, f32p]
+    L.vx_scene_checkpoint.argtypes = [C.c_void_p, C.c_int32]
+    L.vx_scene_stream.restype = C.c_void_p
+    L.vx_scene_stream.argtypes = [C.c_void_p]
+    L.vx_scene_kernel_times.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_uint64, f64p]
+    for name in header_symbols():
+        getattr(L, name)  # every declared entry point is exported
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().vx_last_error().decode()
+
+
+def check(status, allow=()):
+    if status != VX_OK and status not in allow:
+        raise VxError(status, last_error())
+    return status
+
+
+def _p(a, ct):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        check(load().vx_ctx_create(device, C.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            load().vx_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build_topology(self, cells, kinematic) -> np.ndarray:
+        cells = np.ascontiguousarray(cells, np.int32).reshape(-1, 3)
+        kin = np.ascontiguousarray(kinematic, np.uint8)
+        out = np.zeros(3 * len(cells), np.uint32)
+        check(load().vx_build_topology(self.h, _p(cells, C.c_int32), _p(kin, C.c_uint8), len(cells),
+                                       _p(out, C.c_uint32)))
+        return out.reshape(3, -1)
+
+
+def material_array(materials):
+    arr = (VxMaterial * max(len(materials), 1))()
+    for k, m in enumerate(materials):
+        for name, _ in VxMaterial._fields_:
+            setattr(arr[k], name, getattr(m, name))
+    return arr
+
+
+class DeviceScene:
+    """A scene resident on the device (vx_scene handle)."""
+
+    def __init__(self, ctx: Context, scene):
+        self.ctx = ctx
+        self.n = scene.n
+        self._keep = dict(
+            pos=np.ascontiguousarray(scene.position, np.float64).reshape(-1),
+            rot=np.ascontiguousarray(scene.rotation, np.float64).reshape(-1),
+            kin=np.ascontiguousarray(scene.kinematic, np.uint8),
+            mass=np.ascontiguousarray(scene.mass, np.float32),
+            mat=np.ascontiguousarray(scene.material, np.uint32),
+            fib=np.ascontiguousarray(scene.fiber, np.float32).reshape(-1),
+            ani=np.ascontiguousarray(scene.anisotropy, np.float32),
+            solid=np.ascontiguousarray(scene.solid_fraction, np.float32),
+            therm=np.ascontiguousarray(scene.thermal_strength, np.float32),
+            dT=np.ascontiguousarray(scene.thermal_delta, np.float32),
+            nbr=np.ascontiguousarray(scene.neighbor, np.uint32).reshape(-1),
+            form=np.ascontiguousarray(scene.formation_offset, np.float32).reshape(-1),
+            plas=np.ascontiguousarray(scene.plastic_strain, np.float32).reshape(-1),
+            dmg=np.ascontiguousarray(scene.damage, np.float32).reshape(-1),
+        )
+        k = self._keep
+        self._mats = material_array(scene.materials)
+        desc = VxSceneDesc(
+            scene.n, _p(k["pos"], C.c_double), _p(k["rot"], C.c_double), _p(k["kin"], C.c_uint8),
+            _p(k["mass"], C.c_float), _p(k["mat"], C.c_uint32), self._mats, len(scene.materials),
+            _p(k["fib"], C.c_float), _p(k["ani"], C.c_float), _p(k["solid"], C.c_float),
+            _p(k["therm"], C.c_float), _p(k["dT"], C.c_float), _p(k["nbr"], C.c_uint32),
+            _p(k["form"], C.c_float), _p(k["plas"], C.c_float), _p(k["dmg"], C.c_float))
+        self.h = C.c_void_p()
+        check(load().vx_scene_create(ctx.h, C.byref(desc), C.byref(self.h)))
+        self.set_targets(scene.target_mask, scene.target)
+        self.set_loads(scene.loads)
+
+    def close(self):
+        if self.h:
+            load().vx_scene_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ----------------------------------------------------------------
+    def _vec(self, a):
+        return np.ascontiguousarray(a, np.float64).reshape(-1)
+
+    def set_positions(self, x):
+        x = self._vec(x)
+        check(load().vx_scene_set_positions(self.h, _p(x, C.c_double)))
+
+    def positions(self) -> np.ndarray:
+        out = np.zeros(3 * self.n, np.float64)
+        check(load().vx_scene_get_positions(self.h, _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def set_rotations(self, q):
+        q = self._vec(q)
+        check(load().vx_scene_set_rotations(self.h, _p(q, C.c_double)))
+
+    def rotations(self) -> np.ndarray:
+        out = np.zeros(4 * self.n, np.float64)
+        check(load().vx_scene_get_rotations(self.h, _p(out, C.c_double)))
+        return out.reshape(-1, 4)
+
+    def set_targets(self, mask, target=None):
+        mask = np.ascontiguousarray(mask, np.uint8)
+        t = None if target is None else self._vec(target)
+        check(load().vx_scene_set_targets(self.h, _p(mask, C.c_uint8), _p(t, C.c_double)))
+
+    def set_loads(self, loads):
+        x = self._vec(loads)
+        check(load().vx_scene_set_loads(self.h, _p(x, C.c_double)))
+
+    def set_predicted(self, x=None):
+        x = None if x is None else self._vec(x)
+        check(load().vx_scene_set_predicted(self.h, _p(x, C.c_double)))
+
+    def set_bonds(self, neighbor, plastic=None, damage=None, formation=None):
+        nb = np.ascontiguousarray(neighbor, np.uint32).reshape(-1)
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1)
+        pl, dm, fo = f(plastic), f(damage), f(formation)
+        check(load().vx_scene_set_bonds(self.h, _p(nb, C.c_uint32), _p(pl, C.c_float), _p(dm, C.c_float),
+                                        _p(fo, C.c_float)))
+
+    def neighbors(self) -> np.ndarray:
+        out = np.zeros(3 * self.n, np.uint32)
+        check(load().vx_scene_get_neighbors(self.h, _p(out, C.c_uint32)))
+        return out.reshape(3, -1)
+
+    def save_state(self):
+        check(load().vx_scene_checkpoint(self.h, 0))
+
+    def restore_state(self):
+        check(load().vx_scene_checkpoint(self.h, 1))
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(load().vx_scene_stream(self.h) or 0)
+
+    def kernel_times(self, precision, reps=20, flush_ptr=0, flush_bytes=0):
+        out = np.zeros(2, np.float64)
+        check(load().vx_scene_kernel_times(self.h, precision, reps, C.c_void_p(flush_ptr), flush_bytes,
+                                           _p(out, C.c_double)))
+        return {"matvec_us": float(out[0]), "update_us": float(out[1])}
+
+    # -- the solve ------------------------------------------------------------
+    def fit_rotations(self) -> float:
+        v = C.c_double()
+        check(load().vx_fit_rotations(self.h, C.byref(v)))
+        return v.value
+
+    def corotational_pass(self, h, tolerance, max_iterations, precision=PRECISION_FP64, reuse=False,
+                          inner_tolerance=0.0, max_outer=0, allow=(VX_NOT_CONVERGED,)):
+        p = VxPassParams(h, tolerance, max_iterations, precision, int(reuse), inner_tolerance, max_outer)
+        st = VxPassStats()
+        status = check(load().vx_corotational_pass(self.h, C.byref(p), C.byref(st)), allow=allow)
+        d = st.as_dict()
+        d["status"] = status
+        return d
+
+    def bond_stress(self, with_force=True, with_ratio=True, cap=None):
+        m = 3 * self.n
+        ratio = np.zeros(m, np.float32) if with_ratio else None
+        force = np.zeros(3 * m, np.float32) if with_force else None
+        cap = m if cap is None else cap
+        near = np.zeros(max(cap, 1), np.uint32)
+        cnt = C.c_uint32()
+        check(load().vx_bond_stress(self.h, _p(ratio, C.c_float), _p(force, C.c_float), _p(near, C.c_uint32), cap,
+                                    C.byref(cnt)))
+        out = dict(near=near[:min(cnt.value, cap)].copy(), near_count=cnt.value)
+        if with_ratio:
+            out["ratio"] = ratio.reshape(3, -1)
+        if with_force:
+            out["force"] = force.reshape(3, -1, 3)
+        return out
+
+
+def solve_pcg_f32(rows, max_iterations, tolerance):
+    """vx_solve_pcg_f32 on a packed active-row system (dict of flat arrays)."""
+    n = rows["n"]
+    dx = np.zeros(3 * max(n, 1), np.float32)
+    it = C.c_uint32()
+    rel = C.c_float()
+    a = {k: np.ascontiguousarray(rows[k]) for k in ("rhs", "nbr6", "diag9", "blocks54", "inv9")}
+    st = load().vx_solve_pcg_f32(_p(a["rhs"], C.c_float), _p(a["nbr6"], C.c_uint32), _p(a["diag9"], C.c_float),
+                                 _p(a["blocks54"], C.c_float), _p(a["inv9"], C.c_float), n, max_iterations,
+                                 tolerance, _p(dx, C.c_float), C.byref(it), C.byref(rel))
+    return st, dx[:3 * n].reshape(-1, 3), it.value, rel.value
