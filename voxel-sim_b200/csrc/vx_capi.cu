@@ -269,6 +269,7 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
     vx_scene* s = new (std::nothrow) vx_scene();
     if (!s) return VX_OOM;
     s->ctx = ctx;
+    s->device = ctx->device;
     s->n = n;
     s->blocks = (n + 255) / 256;
     s->material_count = d->material_count;
@@ -358,7 +359,7 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
 
 int32_t vx_scene_destroy(vx_scene* s) {
     if (!s) return VX_OK;
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->chunk64) cudaGraphExecDestroy(s->chunk64);
     if (s->chunk32) cudaGraphExecDestroy(s->chunk32);
@@ -380,7 +381,7 @@ int32_t vx_scene_destroy(vx_scene* s) {
             set_error("%s: null argument", __func__);             \
             return VX_BAD_INPUT;                                  \
         }                                                         \
-        cudaSetDevice((s)->ctx->device);                          \
+        cudaSetDevice((s)->device);                          \
     } while (0)
 
 int32_t vx_scene_set_positions(vx_scene* s, const double* xyz) {
@@ -432,7 +433,7 @@ int32_t vx_scene_set_loads(vx_scene* s, const double* xyz) {
 int32_t vx_scene_set_predicted(vx_scene* s, const double* xyz) {
     clear_error();
     if (!s) return VX_BAD_INPUT;
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     if (!xyz) {
         VX_TRY(cudaMemcpyAsync(s->pred, s->pos, 3 * (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice,
                                s->stream), "predicted");
@@ -474,7 +475,7 @@ int32_t vx_scene_get_neighbors(vx_scene* s, uint32_t* neighbor) {
 int32_t vx_fit_rotations(vx_scene* s, double* out_max_angle) {
     clear_error();
     if (!s) return VX_BAD_INPUT;
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     VX_TRY(launch_fit_rotations(s), "fit_rotations launch");
     unsigned long long bits = 0;
     VX_TRY(cudaMemcpyAsync(&bits, s->max_angle_bits, 8, cudaMemcpyDeviceToHost, s->stream), "fit_rotations");
@@ -512,7 +513,7 @@ int32_t vx_corotational_pass(vx_scene* s, const vx_pass_params* p, vx_pass_stats
         set_error("vx_corotational_pass: unknown precision %d", p->precision);
         return VX_BAD_INPUT;
     }
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     vx_pass_stats st{};
     bool reuse = p->reuse_preconditioner && s->have_dinv;
     s->launches = 2;
@@ -551,7 +552,7 @@ int32_t vx_bond_stress(vx_scene* s, float* ratio, float* force, uint32_t* near, 
         set_error("vx_bond_stress: no corotational pass has assembled the bonds yet");
         return VX_BAD_INPUT;
     }
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     size_t m = 3 * (size_t)s->n;
     VX_TRY(launch_bond_stress(s, s->out_ratio, force ? s->out_force : nullptr, s->out_near, (uint32_t)m),
            "bond stress launch");
@@ -579,7 +580,7 @@ int32_t vx_scene_checkpoint(vx_scene* s, int32_t op) {
         set_error("vx_scene_checkpoint: bad argument");
         return VX_BAD_INPUT;
     }
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     size_t n = s->n;
     if (op == 0) {
         VX_TRY(cudaMemcpyAsync(s->save_pos, s->pos, 3 * n * 8, cudaMemcpyDeviceToDevice, s->stream), "checkpoint");
@@ -606,7 +607,7 @@ int32_t vx_scene_kernel_times(vx_scene* s, int32_t precision, uint32_t reps, voi
         set_error("vx_scene_kernel_times: no assembled system");
         return VX_BAD_INPUT;
     }
-    cudaSetDevice(s->ctx->device);
+    cudaSetDevice(s->device);
     return kernel_times(s, precision, reps, flush, flush_bytes, out_us);
 }
 

@@ -67,7 +67,8 @@ struct vx_ctx {
 };
 
 struct vx_scene {
-    vx_ctx* ctx = nullptr;
+    vx_ctx* ctx = nullptr;        // creating context (not dereferenced after creation)
+    int device = 0;               // the scene's GPU; the scene may outlive its context
     uint32_t n = 0;
     uint32_t blocks = 0;          // grid of the per-REV kernels (256 threads)
     cudaStream_t stream = nullptr;
