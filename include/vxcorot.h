@@ -168,6 +168,36 @@ int32_t vx_solve_pcg_f32(const float* rhs, const uint32_t* neighbors, const floa
                          uint32_t max_iterations, float tolerance, float* out_dx,
                          uint32_t* out_iterations, float* out_relative);
 
+/*
+ * vx_solve_pcg_f32_noalloc — no counterpart in the reference.
+ *
+ * The same solve as vx_solve_pcg_f32 for callers that cannot allocate device
+ * memory: an engine that sizes and owns every byte of its GPU up front (a
+ * fixed per-GPU budget, as an admission-controlled server keeps), or a step
+ * loop in which a cudaMalloc/cudaFree, which can block on the device, is not
+ * acceptable. The caller passes device pointers: the packed system in the
+ * layouts of vx_solve_pcg_f32 and d_out_dx[3n] for the correction.
+ * out_iterations and out_relative are host pointers (or NULL); stream is a
+ * cudaStream_t (NULL = the legacy default stream). The function calls no
+ * cudaMalloc, cudaFree or other allocating routine: its work vectors,
+ * reduction partials and scalars live in one fixed device array of
+ * VX_NOALLOC_SCRATCH_BYTES that every GPU which loads this library keeps until
+ * the process exits. Systems of more than VX_NOALLOC_MAX_ROWS rows are
+ * rejected with VX_BAD_INPUT.
+ *
+ * The first call on each device looks up that array's device address, so make
+ * the first call on a device before any stream capture. All calls share the
+ * one array and each call starts by clearing the parts that must be zero;
+ * calls that overlap on the GPU (other threads or streams on the same device)
+ * race on it and must not run at the same time.
+ */
+#define VX_NOALLOC_MAX_ROWS 65536u
+#define VX_NOALLOC_SCRATCH_BYTES 4194304u
+int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* d_neighbors, const float* d_diagonal,
+                                 const float* d_blocks, const float* d_inverse_diagonal, uint32_t n,
+                                 uint32_t max_iterations, float tolerance, float* d_out_dx,
+                                 uint32_t* out_iterations, float* out_relative, void* stream);
+
 /* Device context (one per GPU and host thread of control). */
 typedef struct vx_ctx vx_ctx;
 typedef struct vx_scene vx_scene;

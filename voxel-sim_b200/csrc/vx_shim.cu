@@ -339,3 +339,231 @@ extern "C" int32_t vx_solve_pcg_f32(const float* rhs, const uint32_t* neighbors,
         }
     return VX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// vx_solve_pcg_f32_noalloc: the same block-Jacobi PCG as vx_solve_pcg_f32, for
+// callers that cannot allocate device memory. Inputs and the output correction
+// are caller-owned device buffers; the solver's own work vectors, reduction
+// partials and scalars live in the fixed array below, which every GPU that
+// loads this library holds until the process exits.
+
+static __device__ __align__(256) unsigned char vx_noalloc_scratch[VX_NOALLOC_SCRATCH_BYTES];
+
+namespace vx {
+namespace {
+
+constexpr size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+// r, z, p (two), Ap, then the reduction partials, the scalars and a status word
+constexpr size_t noalloc_bytes(size_t n) {
+    return 5 * al256(3 * n * sizeof(float)) + al256(2 * ((n + kThreads - 1) / kThreads) * sizeof(double)) +
+           al256(sizeof(ShimScalars)) + al256(sizeof(uint32_t));
+}
+static_assert(noalloc_bytes(VX_NOALLOC_MAX_ROWS) <= VX_NOALLOC_SCRATCH_BYTES,
+              "the scratch array must hold a system of VX_NOALLOC_MAX_ROWS rows");
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_lock;
+void* g_noalloc_base[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device. Host code cannot use the array's name as a device pointer.
+int32_t noalloc_base(char** out) {
+    int device = -1;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        set_error("vx_solve_pcg_f32_noalloc: no current CUDA device: %s", cudaGetErrorString(e));
+        return VX_NO_DEVICE;
+    }
+    if (device < 0 || device >= kMaxDevices) {
+        set_error("vx_solve_pcg_f32_noalloc: device %d is beyond the %d devices supported", device, kMaxDevices);
+        return VX_BAD_INPUT;
+    }
+    std::lock_guard<std::mutex> guard(g_noalloc_lock);
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, vx_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("vx_solve_pcg_f32_noalloc: scratch address lookup failed on device %d: %s", device,
+                      cudaGetErrorString(e));
+            return VX_CUDA_ERROR;
+        }
+        g_noalloc_base[device] = p;
+    }
+    *out = static_cast<char*>(g_noalloc_base[device]);
+    return VX_OK;
+}
+
+// Neighbour slots must name a row of the system (or be empty).
+__global__ void k_noalloc_validate(uint32_t n, const uint32_t* __restrict__ nbr6, uint32_t* __restrict__ status) {
+    size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (e < 6 * (size_t)n) {
+        uint32_t j = nbr6[e];
+        if (j != VX_EMPTY_U32 && j >= n) atomicOr(status, 2u);
+    }
+}
+
+// r = rhs, z = inverse r, dx = 0, p = 0; r.z and r.r.
+__global__ void __launch_bounds__(kThreads) k_noalloc_init(ShimArgs a, const float* __restrict__ rhs) {
+    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < a.n) {
+        float r[3] = {rhs[3 * (size_t)i], rhs[3 * (size_t)i + 1], rhs[3 * (size_t)i + 2]};
+        float z[3];
+        m3v(a.inv9 + 9 * (size_t)i, r, z);
+        for (int c = 0; c < 3; ++c) {
+            a.r[3 * (size_t)i + c] = r[c];
+            a.z[3 * (size_t)i + c] = z[c];
+            a.dx[3 * (size_t)i + c] = 0.0f;
+            const_cast<float*>(a.p_old)[3 * (size_t)i + c] = 0.0f;
+        }
+        v[0] = dot_ptx(r, z);
+        v[1] = dot_ptx(r, r);
+    }
+    if (grid_sum<2>(v, a.partials, &a.sc->counter[0]) && threadIdx.x == 0) {
+        a.sc->rho = v[0];
+        a.sc->rr = v[1];
+        a.sc->beta = 0.0;
+    }
+}
+
+__global__ void k_noalloc_finite(uint32_t count, const float* __restrict__ dx, uint32_t* __restrict__ status) {
+    size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < count && !isfinite(dx[t])) atomicOr(status, 1u);
+}
+
+}  // namespace
+}  // namespace vx
+
+extern "C" int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* d_neighbors,
+                                            const float* d_diagonal, const float* d_blocks,
+                                            const float* d_inverse_diagonal, uint32_t n, uint32_t max_iterations,
+                                            float tolerance, float* d_out_dx, uint32_t* out_iterations,
+                                            float* out_relative, void* stream) {
+    clear_error();
+    if (out_iterations) *out_iterations = 0;
+    if (out_relative) *out_relative = 0.0f;
+    if (n == 0) return VX_OK;
+    if (!d_rhs || !d_neighbors || !d_diagonal || !d_blocks || !d_inverse_diagonal || !d_out_dx) {
+        set_error("vx_solve_pcg_f32_noalloc: null argument");
+        return VX_BAD_INPUT;
+    }
+    if (n > VX_NOALLOC_MAX_ROWS) {
+        set_error("vx_solve_pcg_f32_noalloc: %u rows exceed the fixed scratch limit of %u rows (%u bytes); "
+                  "use vx_solve_pcg_f32 for larger systems",
+                  n, (unsigned)VX_NOALLOC_MAX_ROWS, (unsigned)VX_NOALLOC_SCRATCH_BYTES);
+        return VX_BAD_INPUT;
+    }
+    // a non-sticky error left by an earlier, unrelated call on this thread
+    // would otherwise be reported as a failure of this call's own launches
+    (void)cudaGetLastError();
+    char* B = nullptr;
+    int32_t st = noalloc_base(&B);
+    if (st != VX_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    size_t m = n;
+    unsigned blocks_n = (unsigned)((m + kThreads - 1) / kThreads);
+    size_t vec = al256(3 * m * sizeof(float));
+    size_t off_r = 0, off_z = vec, off_p0 = 2 * vec, off_p1 = 3 * vec, off_ap = 4 * vec, off_part = 5 * vec,
+           off_sc = off_part + al256(2 * (size_t)blocks_n * sizeof(double)), off_status = off_sc + al256(sizeof(ShimScalars));
+    ShimArgs A[2];
+    for (int k = 0; k < 2; ++k) {
+        A[k].n = n;
+        A[k].nbr6 = d_neighbors;
+        A[k].diag9 = d_diagonal;
+        A[k].blocks54 = d_blocks;
+        A[k].inv9 = d_inverse_diagonal;
+        A[k].z_in = (const float*)(B + off_z);
+        A[k].p_old = (const float*)(B + (k ? off_p1 : off_p0));
+        A[k].p_new = (float*)(B + (k ? off_p0 : off_p1));
+        A[k].ap = (float*)(B + off_ap);
+        A[k].dx = d_out_dx;
+        A[k].r = (float*)(B + off_r);
+        A[k].z = (float*)(B + off_z);
+        A[k].partials = (double*)(B + off_part);
+        A[k].sc = (ShimScalars*)(B + off_sc);
+    }
+    uint32_t* d_status = (uint32_t*)(B + off_status);
+    // the array keeps the previous call's contents: the reduction tickets,
+    // scalars and status word must start at zero
+    cudaError_t e = cudaMemsetAsync(B + off_sc, 0, al256(sizeof(ShimScalars)) + sizeof(uint32_t), s);
+    if (e == cudaSuccess) {
+        k_noalloc_validate<<<(unsigned)((6 * m + 255) / 256), 256, 0, s>>>(n, d_neighbors, d_status);
+        k_noalloc_init<<<blocks_n, kThreads, 0, s>>>(A[0], d_rhs);
+        e = cudaGetLastError();
+    }
+    ShimScalars h{};
+    uint32_t status = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, A[0].sc, sizeof(ShimScalars), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error("vx_solve_pcg_f32_noalloc: set-up failed: %s", cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    if (status & 2u) {
+        set_error("vx_solve_pcg_f32_noalloc: a neighbour slot names a row outside the %u-row system", n);
+        return VX_BAD_INPUT;
+    }
+    double initial = std::sqrt(h.rr);
+    if (!(initial > 1e-12)) {
+        // (src/cuda_solver.rs:316-324) a zero right-hand side returns a zero correction
+        e = cudaMemsetAsync(d_out_dx, 0, 3 * m * sizeof(float), s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error("vx_solve_pcg_f32_noalloc: %s", cudaGetErrorString(e));
+            return VX_CUDA_ERROR;
+        }
+        if (!std::isfinite(h.rr)) {
+            set_error("CUDA PCG produced a non-finite residual norm");
+            return VX_NONFINITE;
+        }
+        return VX_OK;
+    }
+    uint32_t it = 0;
+    double rr = INFINITY;
+    int ping = 0;
+    while (it < max_iterations) {
+        uint32_t step = max_iterations - it < (uint32_t)kShimChunk ? max_iterations - it : (uint32_t)kShimChunk;
+        for (uint32_t k = 0; k < step; ++k) {
+            k_shim_matvec<<<blocks_n, kThreads, 0, s>>>(A[ping]);
+            k_shim_update<<<blocks_n, kThreads, 0, s>>>(A[ping]);
+            ping ^= 1;
+        }
+        it += step;
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&h, A[0].sc, sizeof(ShimScalars), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_error("vx_solve_pcg_f32_noalloc: iteration failed: %s", cudaGetErrorString(e));
+            return VX_CUDA_ERROR;
+        }
+        rr = h.rr;
+        if (!std::isfinite(rr) || rr < 0.0) break;
+        if ((float)(std::sqrt(rr) / initial) <= tolerance) break;
+    }
+    if (out_iterations) *out_iterations = it;
+    if (!std::isfinite(rr) || rr < 0.0) {
+        set_error("CUDA PCG produced a non-finite residual norm");
+        return VX_NONFINITE;
+    }
+    float relative = (float)(std::sqrt(rr) / initial);
+    if (out_relative) *out_relative = relative;
+    if (!std::isfinite(relative) || relative > tolerance) {
+        set_error("CUDA PCG did not converge: iterations=%u, relative residual=%.3e, tolerance=%.3e", it, relative,
+                  tolerance);
+        return VX_NOT_CONVERGED;
+    }
+    k_noalloc_finite<<<(unsigned)((3 * m + 255) / 256), 256, 0, s>>>((uint32_t)(3 * m), d_out_dx, d_status);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        set_error("vx_solve_pcg_f32_noalloc: %s", cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    if (status & 1u) {
+        set_error("CUDA PCG produced a non-finite correction");
+        return VX_NONFINITE;
+    }
+    return VX_OK;
+}

@@ -102,6 +102,8 @@ def load(path: Path | None = None):
     L.vx_corotational_pass.argtypes = [C.c_void_p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
     L.vx_bond_stress.argtypes = [C.c_void_p, f32p, f32p, u32p, C.c_uint32, u32p]
     L.vx_solve_pcg_f32.argtypes = [f32p, u32p, f32p, f32p, f32p, C.c_uint32, C.c_uint32, C.c_float, f32p, u32p, f32p]
+    L.vx_solve_pcg_f32_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_uint32, C.c_float, C.c_void_p, u32p, f32p, C.c_void_p]
     L.vx_scene_checkpoint.argtypes = [C.c_void_p, C.c_int32]
     L.vx_scene_stream.restype = C.c_void_p
     L.vx_scene_stream.argtypes = [C.c_void_p]
