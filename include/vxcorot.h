@@ -62,6 +62,13 @@ enum {
 /* Fracture modes, src/material.rs:3-8. */
 enum { VX_BRITTLE = 0, VX_DUCTILE = 1, VX_MIXED = 2 };
 
+/* Kernel choice for the FP32 inner solve of the MIXED form. */
+enum {
+    VX_KERNEL_AUTO = 0,       /* persistent when the scene fits on chip, else streaming */
+    VX_KERNEL_STREAMING = 1,  /* two grid-stride kernels per iteration, replayed as CUDA graphs */
+    VX_KERNEL_PERSISTENT = 2  /* one cooperative kernel per inner solve, state in shared memory */
+};
+
 /* Precision forms of a corotational pass. */
 enum {
     VX_PRECISION_FP64 = 0,  /* plain FP64 block-Jacobi PCG */
@@ -134,6 +141,7 @@ typedef struct vx_pass_params {
     double inner_tolerance;      /* MIXED only: relative target of each FP32 inner solve
                                     (0 = default 1e-4) */
     uint32_t max_outer;          /* MIXED only: refinement cap (0 = default 30) */
+    int32_t kernel;              /* MIXED only: VX_KERNEL_AUTO / _STREAMING / _PERSISTENT */
 } vx_pass_params;
 
 typedef struct vx_pass_stats {
@@ -270,7 +278,10 @@ void* vx_scene_stream(vx_scene* scene);
  * for the FP32 kernels), timed with CUDA events on the scene stream over reps
  * launches each. When flush_bytes > 0 the device buffer flush is overwritten
  * before every timed launch so the kernels read from HBM, not L2.
- * out_us[0] = matvec, out_us[1] = update, in microseconds.
+ * out_us[0] = matvec, out_us[1] = update, in microseconds. For
+ * VX_PRECISION_MIXED on a scene that takes the persistent inner solve,
+ * out_us[2] = its time per iteration (one launch of out_us[3] iterations),
+ * else both are 0. out_us has four entries.
  */
 int32_t vx_scene_kernel_times(vx_scene* scene, int32_t precision, uint32_t reps, void* flush,
                               uint64_t flush_bytes, double* out_us);

@@ -248,3 +248,64 @@ def test_empty_scene(ctx):
     st = d.corotational_pass(1e-3, 1e-8, 10)
     assert st["iterations"] == 0 and st["converged"] == 1
     assert d.fit_rotations() == 0.0
+
+
+# -- persistent on-chip inner solve ----------------------------------------------------------
+@pytest.mark.parametrize("edge", [8, 24])
+def test_persistent_inner_solve_matches_streaming_and_oracle(ctx, edge):
+    s = S.mixed_block(edge, seed=5)
+    o = O.OracleScene(s)
+    o.fit_rotations()
+    o.assemble(1e-3)
+    o.factor_block_jacobi()
+    ref, _, _ = o.pcg(200000, 1e-14)
+    x0 = s.position.copy()
+    out = {}
+    for kernel in (N.KERNEL_STREAMING, N.KERNEL_PERSISTENT):
+        d = N.DeviceScene(ctx, s)
+        d.fit_rotations()
+        st = d.corotational_pass(1e-3, 1e-8, 50000, precision=N.PRECISION_MIXED, kernel=kernel)
+        assert st["converged"] == 1 and st["true_residual"] <= 1e-8, (kernel, st)
+        out[kernel] = d.positions() - x0
+        d.close()
+    for dx in out.values():
+        assert rel(dx, ref) < 1e-5
+    assert rel(out[N.KERNEL_PERSISTENT], out[N.KERNEL_STREAMING]) < 2e-5
+
+
+def test_persistent_solve_on_wood_cube_meets_fp64_target(ctx):
+    s = S.wood_cube()
+    d = N.DeviceScene(ctx, s)
+    d.fit_rotations()
+    st = d.corotational_pass(1e-3, 1e-10, 20000, precision=N.PRECISION_MIXED, kernel=N.KERNEL_PERSISTENT)
+    assert st["converged"] == 1 and st["true_residual"] <= 1e-10, st
+
+
+def test_persistent_barrier_wait_runs_out_and_reports_timeout():
+    """A grid-barrier wait bounded at a handful of spins runs out (no block is
+    missing, the bound is simply too small); the kernel records VX_TIMEOUT and
+    returns, and the context stays usable."""
+    import subprocess
+    import sys
+    import textwrap
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = textwrap.dedent(f"""
+        import sys
+        sys.path[:0] = [{str(root / 'voxel-sim_b200')!r}]
+        from vxsim import native as N, scenes as S
+        ctx = N.Context(0)
+        d = N.DeviceScene(ctx, S.mixed_block(24, seed=5))
+        d.fit_rotations()
+        try:
+            d.corotational_pass(1e-3, 1e-8, 5000, precision=N.PRECISION_MIXED, kernel=N.KERNEL_PERSISTENT)
+            print("NO_TIMEOUT")
+        except N.VxError as e:
+            print("STATUS", e.status)
+        st = d.corotational_pass(1e-3, 1e-8, 5000, precision=N.PRECISION_MIXED, kernel=N.KERNEL_STREAMING)
+        print("AFTER", st["converged"])
+    """)
+    env = dict(__import__("os").environ, VXCOROT_BARRIER_SPINS="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+    assert f"STATUS {N.VX_TIMEOUT}" in out.stdout, out.stdout + out.stderr
+    assert "AFTER 1" in out.stdout

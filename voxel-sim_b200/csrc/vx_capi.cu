@@ -80,6 +80,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->max_angle_bits = A.take<unsigned long long>(1);
     s->near_count = A.take<uint32_t>(1);
     s->bond_count = A.take<uint32_t>(1);
+    s->barrier = A.take<unsigned>(4);
 }
 
 uint64_t scene_bytes(uint32_t n, uint32_t material_count) {
@@ -270,6 +271,7 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
     if (!s) return VX_OOM;
     s->ctx = ctx;
     s->device = ctx->device;
+    s->sm_count = ctx->sm_count > 0 ? ctx->sm_count : 1;
     s->n = n;
     s->blocks = (n + 255) / 256;
     s->material_count = d->material_count;
@@ -509,6 +511,10 @@ int32_t vx_corotational_pass(vx_scene* s, const vx_pass_params* p, vx_pass_stats
         set_error("vx_corotational_pass: invalid h=%g or tolerance=%g", p->h, p->tolerance);
         return VX_BAD_INPUT;
     }
+    if (p->kernel < VX_KERNEL_AUTO || p->kernel > VX_KERNEL_PERSISTENT) {
+        set_error("vx_corotational_pass: unknown kernel selection %d", p->kernel);
+        return VX_BAD_INPUT;
+    }
     if (p->precision != VX_PRECISION_FP64 && p->precision != VX_PRECISION_MIXED) {
         set_error("vx_corotational_pass: unknown precision %d", p->precision);
         return VX_BAD_INPUT;
@@ -524,7 +530,7 @@ int32_t vx_corotational_pass(vx_scene* s, const vx_pass_params* p, vx_pass_stats
     if (p->precision == VX_PRECISION_FP64)
         status = solve_fp64(s, p->tolerance, p->max_iterations, &st);
     else
-        status = solve_mixed(s, p->tolerance, p->max_iterations, p->inner_tolerance, p->max_outer, &st);
+        status = solve_mixed(s, p->tolerance, p->max_iterations, p->inner_tolerance, p->max_outer, p->kernel, &st);
     if (status == VX_CUDA_ERROR) return status;
     double tr = 0.0;
     int32_t r = true_residual(s, &tr);

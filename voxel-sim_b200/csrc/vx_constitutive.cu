@@ -10,6 +10,7 @@
 // fracture::update (src/fracture.rs:76-133, :210-262).
 #include "vx_device.cuh"
 #include "vx_kernels.h"
+#include "vx_layout.cuh"
 
 namespace vx {
 
@@ -137,11 +138,8 @@ __global__ void k_assemble_bonds(SceneView s, BondArrays b, uint32_t* __restrict
     b.state[e] = st;
     unsigned ballot = __ballot_sync(__activemask(), st == 2);
     if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot) atomicAdd(assembled, __popc(ballot));
-#pragma unroll
-    for (int t = 0; t < 6; ++t) {
-        b.k64[((size_t)a * 6 + t) * n + i] = W.s[t];
-        b.k32[((size_t)a * 6 + t) * n + i] = (float)W.s[t];
-    }
+    store_sym(b.k64 + (size_t)a * 6 * n, n, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
+    store_sym(b.k32 + (size_t)a * 6 * n, n, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
     b.force[e] = force.x;
     b.force[m3n + e] = force.y;
     b.force[2 * m3n + e] = force.z;
@@ -171,16 +169,16 @@ __global__ void k_assemble_revs(SceneView s, BondArrays b, RevOut o, double h, i
     for (int a = 0; a < 3; ++a) {
         size_t e = (size_t)a * n + i;
         if (b.state[e] == 2) {
-#pragma unroll
-            for (int t = 0; t < 6; ++t) D[t] += b.k64[((size_t)a * 6 + t) * n + i];
+            Sym<double> k = load_sym(b.k64 + (size_t)a * 6 * n, n, i);
+            D[0] += k.xx, D[1] += k.yy, D[2] += k.zz, D[3] += k.xy, D[4] += k.xz, D[5] += k.yz;
             rhs = rhs + mk(b.force[e], b.force[m3n + e], b.force[2 * m3n + e]);
         }
         uint32_t k = s.rev[e];
         if (k != VX_EMPTY_U32) {
             size_t ek = (size_t)a * n + k;
             if (b.state[ek] == 2) {
-#pragma unroll
-                for (int t = 0; t < 6; ++t) D[t] += b.k64[((size_t)a * 6 + t) * n + k];
+                Sym<double> kk = load_sym(b.k64 + (size_t)a * 6 * n, n, k);
+                D[0] += kk.xx, D[1] += kk.yy, D[2] += kk.zz, D[3] += kk.xy, D[4] += kk.xz, D[5] += kk.yz;
                 rhs = rhs - mk(b.force[ek], b.force[m3n + ek], b.force[2 * m3n + ek]);
             }
         }
@@ -190,21 +188,15 @@ __global__ void k_assemble_revs(SceneView s, BondArrays b, RevOut o, double h, i
     rhs = mk(rhs.x * f0, rhs.y * f1, rhs.z * f2);
     sym6 P = sym6{{D[0] * f0 * f0 + (1.0 - f0), D[1] * f1 * f1 + (1.0 - f1), D[2] * f2 * f2 + (1.0 - f2),
                    f0 * D[3] * f1, f0 * D[4] * f2, f1 * D[5] * f2}};
-#pragma unroll
-    for (int t = 0; t < 6; ++t) {
-        o.d64[(size_t)t * n + i] = P.s[t];
-        o.d32[(size_t)t * n + i] = (float)P.s[t];
-    }
+    store_sym(o.d64, n, i, P.s[0], P.s[1], P.s[2], P.s[3], P.s[4], P.s[5]);
+    store_sym(o.d32, n, i, P.s[0], P.s[1], P.s[2], P.s[3], P.s[4], P.s[5]);
     o.b64[i] = rhs.x;
     o.b64[n + i] = rhs.y;
     o.b64[2 * (size_t)n + i] = rhs.z;
     if (!reuse) {
         sym6 inv = inverse(P);
-#pragma unroll
-        for (int t = 0; t < 6; ++t) {
-            o.dinv64[(size_t)t * n + i] = inv.s[t];
-            o.dinv32[(size_t)t * n + i] = (float)inv.s[t];
-        }
+        store_sym(o.dinv64, n, i, inv.s[0], inv.s[1], inv.s[2], inv.s[3], inv.s[4], inv.s[5]);
+        store_sym(o.dinv32, n, i, inv.s[0], inv.s[1], inv.s[2], inv.s[3], inv.s[4], inv.s[5]);
     }
 }
 

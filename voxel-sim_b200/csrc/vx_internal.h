@@ -18,7 +18,7 @@ void clear_error();
 
 // Device-side recurrence scalars of one PCG solve (FP64 or FP32 inner).
 struct PcgScalars {
-    double rz;          // r . z of the current iterate
+    double rz[2];       // r . z of iteration k in slot k & 1
     double pap;         // p . Ap
     double rr;          // r . r
     double initial;     // |r0|
@@ -118,12 +118,13 @@ struct vx_scene {
     float* out_ratio;             // [3n] bond stress outputs
     float* out_force;             // [9n]
     uint32_t* out_near;           // [3n]
-    double* partials;             // [4 * blocks]
+    double* partials;             // [4 * blocks]: p.Ap partials, then r.z / r.r partials
     vx::PcgScalars* sc;           // device scalars (FP64 solve / outer)
     vx::PcgScalars* sc32;         // device scalars (FP32 inner solve)
     unsigned long long* max_angle_bits;
     uint32_t* near_count;
     uint32_t* bond_count;         // bonds assembled by the last pass
+    unsigned* barrier;            // [4] persistent-kernel grid barrier: count, generation, error, pad
 
     // host mirrors
     double* h_stage = nullptr;       // pinned staging of host copies [4n doubles]
@@ -136,6 +137,14 @@ struct vx_scene {
     cudaGraphExec_t chunk32 = nullptr;
 
     uint32_t launches = 0;        // kernels launched by the current pass
+    int sm_count = 148;           // SMs of the scene's GPU
+    unsigned grid32 = 0;          // grid of the FP32 / FP64 PCG kernels (0 = not yet chosen)
+    unsigned grid64 = 0;
+    // persistent (on-chip) inner solve plan
+    bool persist_checked = false;
+    bool persist_ok = false;
+    unsigned persist_G = 0, persist_cap = 0, persist_R = 0;
+    size_t persist_smem = 0;
     uint32_t active = 0;          // REVs with a free axis (cached per target set)
     bool active_cached = false;
     bool assembled = false;

@@ -46,7 +46,10 @@ cudaError_t launch_bond_stress(vx_scene* s, float* d_ratio, float* d_force, uint
 // PCG drivers (vx_pcg.cu)
 int32_t solve_fp64(vx_scene* s, double tolerance, uint32_t max_iterations, vx_pass_stats* out);
 int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, double inner_tolerance,
-                    uint32_t max_outer, vx_pass_stats* out);
+                    uint32_t max_outer, int32_t kernel, vx_pass_stats* out);
+// persistent on-chip FP32 inner solve (vx_persistent.cu)
+bool persistent_plan(vx_scene* s);
+int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations);
 // |b - A x64| / |b| with the FP64 operator (device scalars updated)
 int32_t true_residual(vx_scene* s, double* out);
 // CUDA-event timing of the matvec and update kernels (microseconds per launch)

@@ -3,23 +3,29 @@
 // Follows the CPU PCG of solve_coupled (src/solver.rs:1833-1911): x0 = 0,
 // z = M^-1 r, p = z; alpha = rz / p.Ap (stop when p.Ap <= 1e-30); x += alpha p,
 // r -= alpha Ap; stop when |r|/|r0| < tolerance (checked every iteration);
-// z = M^-1 r; beta = r.z'/r.z; p = z + beta p. Dots accumulate in FP64.
+// z = M^-1 r; beta = r.z'/r.z; p = z + beta p. Dots accumulate in FP64; in the
+// FP32 form alpha and beta are rounded to f32 as the reference does
+// (src/solver.rs:1867, :1900).
 //
-// One iteration is two kernels:
-//   k_matvec  p_new = z + beta p_old (ping-pong buffers, computed for the REV
-//             and, on the fly, for its six neighbours), Ap = D p - P sum K p_nbr,
-//             fused p.Ap grid reduction; its last block forms alpha.
-//   k_update  x += alpha p, r -= alpha Ap, z = D^-1 r, fused r.z and r.r grid
-//             reductions; its last block tests convergence and forms beta.
-// Grid reductions are single-pass and deterministic: each block writes one
-// partial, the last block to finish (atomic ticket) sums the partials in a
-// fixed order. Kernels return at once when the device `done` flag is set, so
-// a CUDA graph of a fixed chunk of iterations can be replayed until the host
-// sees convergence.
+// One iteration is two grid-stride kernels sized to fill the GPU once:
+//   k_matvec  p_new = z + beta p_old (ping-pong buffers, formed for the REV and,
+//             on the fly, for its six neighbours) and Ap = D p - P sum K p_nbr;
+//             writes per-block partials of p.Ap.
+//   k_update  x += alpha p, r -= alpha Ap, z = D^-1 r; writes per-block partials
+//             of r.z and r.r.
+// Each kernel starts by summing the previous kernel's partials in a fixed order
+// in every block, so every block derives the same alpha, beta, convergence and
+// iteration-cap decisions without an atomic ticket or a serial tail; block 0
+// records them for the host. Every load of a REV's data is issued before any of
+// it is used (neighbour indices are clamped instead of branched on), so a
+// thread keeps its whole stencil in flight. A chunk of 16 iterations is
+// captured once as a CUDA graph and replayed; kernels after the stop decision
+// return at entry.
 #include <cstring>
 
 #include "vx_device.cuh"
 #include "vx_kernels.h"
+#include "vx_layout.cuh"
 #include "vx_reduce.cuh"
 
 namespace vx {
@@ -30,9 +36,9 @@ template <typename T>
 struct IterArgs {
     uint32_t n;
     const uint8_t* flags;
-    const T* D;       // [6][n] projected diagonal
-    const T* K;       // [18][n] bond K per axis (sym6), zero when not assembled
-    const T* Dinv;    // [6][n]
+    const T* D;       // projected diagonal (sym layout)
+    const T* K;       // per-axis bond K (3 sym layouts), zero when not assembled
+    const T* Dinv;
     const uint32_t* nbr;
     const uint32_t* rev;
     const T* z_in;    // matvec: z
@@ -42,94 +48,147 @@ struct IterArgs {
     T* x;
     T* r;
     T* z;
-    double* partials;
+    double* pm;       // [G] partials of p.Ap
+    double* pu;       // [2][G] partials of r.z, r.r
     PcgScalars* sc;
 };
 
 template <typename T>
-__device__ __forceinline__ T round_scalar(double v) {
-    return (T)v;
-}
-
-// ---- operator -------------------------------------------------------------------
-template <typename T>
-struct Vec3T {
+struct V3 {
     T x, y, z;
 };
 
 template <typename T>
-__device__ __forceinline__ Vec3T<T> sym_mul(const T* S, size_t stride, size_t i, Vec3T<T> v) {
-    T xx = S[i], yy = S[stride + i], zz = S[2 * stride + i];
-    T xy = S[3 * stride + i], xz = S[4 * stride + i], yz = S[5 * stride + i];
-    return {xx * v.x + xy * v.y + xz * v.z, xy * v.x + yy * v.y + yz * v.z, xz * v.x + yz * v.y + zz * v.z};
+__device__ __forceinline__ V3<T> mul(const Sym<T>& s, V3<T> v) {
+    return {s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
+            s.xz * v.x + s.yz * v.y + s.zz * v.z};
+}
+template <typename T>
+__device__ __forceinline__ V3<T> load_v(const T* p, size_t n, size_t i) {
+    return {p[i], p[n + i], p[2 * n + i]};
+}
+template <typename T>
+__device__ __forceinline__ V3<T> ldg_v(const T* __restrict__ p, size_t n, size_t i) {
+    return {__ldg(p + i), __ldg(p + n + i), __ldg(p + 2 * n + i)};
+}
+template <typename T>
+__device__ __forceinline__ void store_v(T* p, size_t n, size_t i, V3<T> v) {
+    p[i] = v.x;
+    p[n + i] = v.y;
+    p[2 * n + i] = v.z;
+}
+template <typename T>
+__device__ __forceinline__ double dot_d(V3<T> a, V3<T> b) {
+    return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z;
 }
 
-// A v at REV i: D_i v_i - P_i (sum over the three owned bonds K_(a,i) v_nbr
-// + sum over the three bonds owned by the -axis neighbours K_(a,k) v_k).
-// `fetch(j)` returns v_j. Neighbours with no free axis hold v = 0.
-template <typename T, typename Fetch>
-__device__ __forceinline__ Vec3T<T> apply_row(const IterArgs<T>& a, uint32_t i, Vec3T<T> vi, Fetch fetch) {
-    const uint32_t n = a.n;
-    Vec3T<T> y = sym_mul<T>(a.D, n, i, vi);
-    Vec3T<T> s = {T(0), T(0), T(0)};
+// ---- block totals of the previous kernel's partials -----------------------------
+// Every thread gets the totals; the summation order is fixed (thread t adds
+// partials t, t+256, ... then the block tree), identical in every block.
+template <int NV>
+__device__ __forceinline__ void block_total(const double* part, unsigned G, double (&out)[NV]) {
+    __shared__ double sh[NV][kThreads / 32];
+    __shared__ double tot[NV];
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        v[k] = 0.0;
+        for (unsigned b = threadIdx.x; b < G; b += kThreads) v[k] += __ldcg(part + (size_t)k * G + b);
+    }
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) tot[k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = tot[k];
+}
+
+template <int NV>
+__device__ __forceinline__ void block_partial(double (&v)[NV], double* part, unsigned G) {
+    __shared__ double sh[NV][kThreads / 32];
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[(size_t)k * G + blockIdx.x] = v[k];
+    }
+}
+
+// ---- one row of the operator ----------------------------------------------------------
+// A v at REV i = D_i v_i - P_i (sum over the three owned bonds K_(a,i) v_nbr(a)
+// + the three bonds owned by the -axis neighbours K_(a,k) v_k). `get(j)` returns
+// v_j. All loads are issued before the arithmetic: missing neighbours read REV
+// i itself and are masked to zero.
+template <typename T, typename Get>
+__device__ __forceinline__ V3<T> apply_row(const IterArgs<T>& a, uint32_t i, V3<T> vi, Get get) {
+    const size_t n = a.n;
+    uint32_t nb[6];
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-        uint32_t j = a.nbr[(size_t)ax * n + i];
-        if (j != VX_EMPTY_U32) {
-            Vec3T<T> kv = sym_mul<T>(a.K + (size_t)ax * 6 * n, n, i, fetch(j));
-            s.x += kv.x;
-            s.y += kv.y;
-            s.z += kv.z;
-        }
-        uint32_t k = a.rev[(size_t)ax * n + i];
-        if (k != VX_EMPTY_U32) {
-            Vec3T<T> kv = sym_mul<T>(a.K + (size_t)ax * 6 * n, n, k, fetch(k));
-            s.x += kv.x;
-            s.y += kv.y;
-            s.z += kv.z;
-        }
+        nb[ax] = __ldg(a.nbr + ax * n + i);
+        nb[3 + ax] = __ldg(a.rev + ax * n + i);
     }
-    uint8_t fl = a.flags[i];
+    const uint8_t fl = __ldg(a.flags + i);
+    const Sym<T> D = load_sym(a.D, n, i);
+    Sym<T> Ko[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) Ko[ax] = load_sym(a.K + ax * 6 * n, n, i);
+    uint32_t jj[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) jj[s] = nb[s] == VX_EMPTY_U32 ? i : nb[s];
+    V3<T> vj[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) vj[s] = get(jj[s]);
+    Sym<T> Kr[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) Kr[ax] = load_sym(a.K + ax * 6 * n, n, jj[3 + ax]);
+    V3<T> y = mul(D, vi);
+    V3<T> s = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const bool ok = nb[t] != VX_EMPTY_U32;
+        V3<T> v = ok ? vj[t] : V3<T>{T(0), T(0), T(0)};
+        V3<T> kv = mul(t < 3 ? Ko[t] : Kr[t - 3], v);
+        s.x += kv.x;
+        s.y += kv.y;
+        s.z += kv.z;
+    }
     if (fl & 1) y.x -= s.x;
     if (fl & 2) y.y -= s.y;
     if (fl & 4) y.z -= s.z;
     return y;
 }
 
-// ---- kernels ----------------------------------------------------------------------
-// r = scale * src (src FP64), x = 0, z = D^-1 r, p_old = 0; r.z and r.r.
+// ---- kernels ----------------------------------------------------------------------------
+// r = scale * src (src FP64), x = 0, z = D^-1 r, p_old = 0; the r.z and r.r
+// partials go to pu; the last block to finish sets the solve's scalars.
 template <typename T>
 __global__ void __launch_bounds__(kThreads) k_init(IterArgs<T> a, const double* __restrict__ src,
                                                    const double* __restrict__ scale_from, double tolerance,
                                                    uint32_t max_iterations) {
-    const uint32_t n = a.n;
-    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = a.n;
+    const size_t stride = (size_t)gridDim.x * kThreads;
     double scale = 1.0;
     if (scale_from) {
         double rn = *scale_from;
         scale = rn > 0.0 ? 1.0 / rn : 1.0;
     }
     double v[2] = {0.0, 0.0};
-    if (i < n) {
-        Vec3T<T> r = {(T)(src[i] * scale), (T)(src[n + i] * scale), (T)(src[2 * (size_t)n + i] * scale)};
-        Vec3T<T> z = sym_mul<T>(a.Dinv, n, i, r);
-        a.r[i] = r.x;
-        a.r[n + i] = r.y;
-        a.r[2 * (size_t)n + i] = r.z;
-        a.z[i] = z.x;
-        a.z[n + i] = z.y;
-        a.z[2 * (size_t)n + i] = z.z;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            a.x[(size_t)c * n + i] = T(0);
-            const_cast<T*>(a.p_old)[(size_t)c * n + i] = T(0);
-        }
-        v[0] = (double)r.x * (double)z.x + (double)r.y * (double)z.y + (double)r.z * (double)z.z;
-        v[1] = (double)r.x * (double)r.x + (double)r.y * (double)r.y + (double)r.z * (double)r.z;
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        V3<T> r = {(T)(src[i] * scale), (T)(src[n + i] * scale), (T)(src[2 * n + i] * scale)};
+        V3<T> z = mul(load_sym(a.Dinv, n, i), r);
+        store_v(a.r, n, i, r);
+        store_v(a.z, n, i, z);
+        store_v(a.x, n, i, V3<T>{T(0), T(0), T(0)});
+        store_v(const_cast<T*>(a.p_old), n, i, V3<T>{T(0), T(0), T(0)});
+        v[0] += dot_d(r, z);
+        v[1] += dot_d(r, r);
     }
-    if (grid_sum<2>(v, a.partials, &a.sc->counter[0]) && threadIdx.x == 0) {
+    if (grid_sum<2>(v, a.pu, &a.sc->counter[0]) && threadIdx.x == 0) {
         PcgScalars* sc = a.sc;
-        sc->rz = v[0];
+        sc->rz[0] = v[0];
+        sc->rz[1] = INFINITY;  // beta of the first iteration is rz0 / inf = 0
         sc->rr = v[1];
         sc->initial = sqrt(v[1]);
         sc->beta = 0.0;
@@ -140,121 +199,148 @@ __global__ void __launch_bounds__(kThreads) k_init(IterArgs<T> a, const double* 
         sc->max_iterations = max_iterations;
         sc->iterations = 0;
         sc->status = VX_OK;
-        bool trivial = !(sc->initial > 1e-12);
-        sc->done = (trivial || max_iterations == 0) ? 1 : 0;
+        const bool trivial = !(sc->initial > 1e-12);
+        int32_t done = (trivial || max_iterations == 0) ? 1 : 0;
         if (!isfinite(v[1]) || !isfinite(v[0])) {
-            sc->done = 1;
+            done = 1;
             sc->status = VX_NONFINITE;
         } else if (!trivial && max_iterations == 0) {
             sc->status = VX_NOT_CONVERGED;
         }
+        sc->done = done;
     }
 }
 
-template <typename T>
+// Iteration k (PAR = k & 1): convergence test of iteration k-1, beta, then
+// p_new = z + beta p_old and Ap = A p_new with p.Ap partials.
+template <typename T, int PAR>
 __global__ void __launch_bounds__(kThreads) k_matvec(IterArgs<T> a) {
-    if (*(volatile int32_t*)&a.sc->done) return;
-    const uint32_t n = a.n;
-    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
-    const T beta = (T)a.sc->beta;
-    double v[1] = {0.0};
-    if (i < n) {
-        auto fetch = [&](uint32_t j) {
-            return Vec3T<T>{fma(beta, a.p_old[j], a.z_in[j]), fma(beta, a.p_old[n + j], a.z_in[n + j]),
-                            fma(beta, a.p_old[2 * (size_t)n + j], a.z_in[2 * (size_t)n + j])};
-        };
-        Vec3T<T> pi = fetch(i);
-        a.p_new[i] = pi.x;
-        a.p_new[n + i] = pi.y;
-        a.p_new[2 * (size_t)n + i] = pi.z;
-        Vec3T<T> y = apply_row<T>(a, i, pi, fetch);
-        a.ap[i] = y.x;
-        a.ap[n + i] = y.y;
-        a.ap[2 * (size_t)n + i] = y.z;
-        v[0] = (double)pi.x * (double)y.x + (double)pi.y * (double)y.y + (double)pi.z * (double)y.z;
-    }
-    if (grid_sum<1>(v, a.partials, &a.sc->counter[1]) && threadIdx.x == 0) {
-        PcgScalars* sc = a.sc;
-        double pap = v[0];
-        sc->pap = pap;
-        sc->iterations += 1;
-        if (!isfinite(pap)) {
-            sc->done = 1;
-            sc->status = VX_NONFINITE;
-        } else if (pap <= 1e-30) {
-            sc->done = 1;  // breakdown: the reference stops without an error
-        } else {
-            sc->alpha = (double)round_scalar<T>(sc->rz / pap);
-        }
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_update(IterArgs<T> a) {
-    if (*(volatile int32_t*)&a.sc->done) return;
-    const uint32_t n = a.n;
-    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
-    const T alpha = (T)a.sc->alpha;
-    double v[2] = {0.0, 0.0};
-    if (i < n) {
-        Vec3T<T> r;
-        T* rc[3] = {&r.x, &r.y, &r.z};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            size_t t = (size_t)c * n + i;
-            T p = a.p_new[t];
-            a.x[t] = fma(alpha, p, a.x[t]);
-            *rc[c] = fma(-alpha, a.ap[t], a.r[t]);
-            a.r[t] = *rc[c];
-        }
-        Vec3T<T> z = sym_mul<T>(a.Dinv, n, i, r);
-        a.z[i] = z.x;
-        a.z[n + i] = z.y;
-        a.z[2 * (size_t)n + i] = z.z;
-        v[0] = (double)r.x * (double)z.x + (double)r.y * (double)z.y + (double)r.z * (double)z.z;
-        v[1] = (double)r.x * (double)r.x + (double)r.y * (double)r.y + (double)r.z * (double)r.z;
-    }
-    if (grid_sum<2>(v, a.partials, &a.sc->counter[2]) && threadIdx.x == 0) {
-        PcgScalars* sc = a.sc;
-        double rz_new = v[0], rr = v[1];
-        sc->rr = rr;
-        double residual = sqrt(rr) / sc->initial;
-        sc->residual = residual;
-        if (!isfinite(rr) || !isfinite(rz_new)) {
-            sc->done = 1;
-            sc->status = VX_NONFINITE;
+    __shared__ int32_t s_done;
+    const unsigned G = gridDim.x;
+    if (threadIdx.x == 0) s_done = *(volatile int32_t*)&a.sc->done;
+    double t[2];
+    block_total<2>(a.pu, G, t);  // its barrier publishes s_done
+    if (s_done) return;
+    PcgScalars* sc = a.sc;
+    const uint32_t its = sc->iterations;
+    const double rz = t[0], rr = t[1];
+    const double residual = sqrt(rr) / sc->initial;
+    int stop = 0, status = VX_OK;
+    if (its > 0) {
+        if (!isfinite(rr) || !isfinite(rz)) {
+            stop = 1;
+            status = VX_NONFINITE;
         } else if (residual < sc->tolerance) {
-            sc->done = 1;
-            sc->status = VX_OK;
-        } else if (sc->iterations >= sc->max_iterations) {
-            sc->done = 1;
-            sc->status = VX_NOT_CONVERGED;
-        } else {
-            sc->beta = (double)round_scalar<T>(rz_new / sc->rz);
-            sc->rz = rz_new;
+            stop = 1;
         }
     }
+    if (!stop && its >= sc->max_iterations) {
+        stop = 1;
+        status = VX_NOT_CONVERGED;
+    }
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    if (stop) {
+        if (leader) {
+            sc->status = status;
+            if (its > 0) sc->residual = residual;
+            sc->rr = rr;
+            sc->done = 1;
+        }
+        return;
+    }
+    const T beta = (T)(rz / sc->rz[PAR ^ 1]);
+    if (leader) {
+        sc->rz[PAR] = rz;
+        sc->beta = (double)beta;
+        sc->rr = rr;
+        if (its > 0) sc->residual = residual;
+    }
+    const size_t n = a.n;
+    const size_t stride = (size_t)G * kThreads;
+    const T* __restrict__ z_in = a.z_in;
+    const T* __restrict__ p_old = a.p_old;
+    auto get = [&](uint32_t j) {
+        return V3<T>{fma(beta, __ldg(p_old + j), __ldg(z_in + j)), fma(beta, __ldg(p_old + n + j), __ldg(z_in + n + j)),
+                     fma(beta, __ldg(p_old + 2 * n + j), __ldg(z_in + 2 * n + j))};
+    };
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        V3<T> pi = get((uint32_t)i);
+        V3<T> y = apply_row<T>(a, (uint32_t)i, pi, get);
+        store_v(a.p_new, n, i, pi);
+        store_v(a.ap, n, i, y);
+        acc += dot_d(pi, y);
+    }
+    double v[1] = {acc};
+    block_partial<1>(v, a.pm, G);
 }
 
-// r64 = b - A64 x64 with |r64| and |b|; residual = |r64| / |b|.
+// Iteration k: alpha = rz_k / p.Ap, x += alpha p, r -= alpha Ap, z = D^-1 r with
+// r.z and r.r partials; p.Ap <= 1e-30 stops like the reference (src/solver.rs:1864-1866).
+template <typename T, int PAR>
+__global__ void __launch_bounds__(kThreads) k_update(IterArgs<T> a) {
+    __shared__ int32_t s_done;
+    const unsigned G = gridDim.x;
+    if (threadIdx.x == 0) s_done = *(volatile int32_t*)&a.sc->done;
+    double t[1];
+    block_total<1>(a.pm, G, t);
+    if (s_done) return;
+    PcgScalars* sc = a.sc;
+    const double pap = t[0];
+    const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+    if (!isfinite(pap) || pap <= 1e-30) {
+        if (leader) {
+            sc->pap = pap;
+            sc->iterations += 1;
+            if (!isfinite(pap)) sc->status = VX_NONFINITE;
+            sc->done = 1;
+        }
+        return;
+    }
+    const T alpha = (T)(sc->rz[PAR] / pap);
+    if (leader) {
+        sc->pap = pap;
+        sc->alpha = (double)alpha;
+        sc->iterations += 1;
+    }
+    const size_t n = a.n;
+    const size_t stride = (size_t)G * kThreads;
+    double v[2] = {0.0, 0.0};
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        V3<T> p = ldg_v(a.p_new, n, i);
+        V3<T> ap = ldg_v(a.ap, n, i);
+        V3<T> x = load_v(a.x, n, i);
+        V3<T> r = load_v(a.r, n, i);
+        Sym<T> M = load_sym(a.Dinv, n, i);
+        x = {fma(alpha, p.x, x.x), fma(alpha, p.y, x.y), fma(alpha, p.z, x.z)};
+        r = {fma(-alpha, ap.x, r.x), fma(-alpha, ap.y, r.y), fma(-alpha, ap.z, r.z)};
+        V3<T> z = mul(M, r);
+        store_v(a.x, n, i, x);
+        store_v(a.r, n, i, r);
+        store_v(a.z, n, i, z);
+        v[0] += dot_d(r, z);
+        v[1] += dot_d(r, r);
+    }
+    block_partial<2>(v, a.pu, G);
+}
+
+// r64 = b - A64 x64 with |r64| and |b|; residual = |r64| / |b| (last-block finalize).
 __global__ void __launch_bounds__(kThreads) k_residual64(IterArgs<double> a, const double* __restrict__ b,
                                                          double* __restrict__ r_out, PcgScalars* sc) {
-    const uint32_t n = a.n;
-    uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    const size_t n = a.n;
+    const size_t stride = (size_t)gridDim.x * kThreads;
+    const double* x = a.x;
+    auto get = [&](uint32_t j) { return V3<double>{x[j], x[n + j], x[2 * n + j]}; };
     double v[2] = {0.0, 0.0};
-    if (i < n) {
-        const double* x = a.x;
-        auto fetch = [&](uint32_t j) { return Vec3T<double>{x[j], x[n + j], x[2 * (size_t)n + j]}; };
-        Vec3T<double> y = apply_row<double>(a, i, fetch(i), fetch);
-        double bx = b[i], by = b[n + i], bz = b[2 * (size_t)n + i];
-        double rx = bx - y.x, ry = by - y.y, rz = bz - y.z;
-        r_out[i] = rx;
-        r_out[n + i] = ry;
-        r_out[2 * (size_t)n + i] = rz;
-        v[0] = rx * rx + ry * ry + rz * rz;
-        v[1] = bx * bx + by * by + bz * bz;
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+        V3<double> y = apply_row<double>(a, (uint32_t)i, get((uint32_t)i), get);
+        V3<double> bb = load_v(b, n, i);
+        V3<double> r = {bb.x - y.x, bb.y - y.y, bb.z - y.z};
+        store_v(r_out, n, i, r);
+        v[0] += r.x * r.x + r.y * r.y + r.z * r.z;
+        v[1] += bb.x * bb.x + bb.y * bb.y + bb.z * bb.z;
     }
-    if (grid_sum<2>(v, a.partials, &sc->counter[3]) && threadIdx.x == 0) {
+    if (grid_sum<2>(v, a.pu, &sc->counter[3]) && threadIdx.x == 0) {
         sc->r64_norm = sqrt(v[0]);
         sc->b_norm = sqrt(v[1]);
         sc->residual = sc->b_norm > 0.0 ? sc->r64_norm / sc->b_norm : 0.0;
@@ -268,7 +354,7 @@ __global__ void k_accumulate(uint32_t n, double* __restrict__ x64, const float* 
     if (t < 3 * (size_t)n) x64[t] += (*scale_from) * (double)x32[t];
 }
 
-// ---- drivers ------------------------------------------------------------------------
+// ---- drivers ------------------------------------------------------------------------------
 static IterArgs<double> args64(vx_scene* s, int ping) {
     IterArgs<double> a;
     a.n = s->n;
@@ -285,7 +371,8 @@ static IterArgs<double> args64(vx_scene* s, int ping) {
     a.x = s->x64;
     a.r = s->r64;
     a.z = s->z64;
-    a.partials = s->partials;
+    a.pm = s->partials;
+    a.pu = s->partials + s->blocks;
     a.sc = s->sc;
     return a;
 }
@@ -306,21 +393,45 @@ static IterArgs<float> args32(vx_scene* s, int ping) {
     a.x = s->x32;
     a.r = s->r32;
     a.z = s->z32;
-    a.partials = s->partials;
+    a.pm = s->partials;
+    a.pu = s->partials + s->blocks;
     a.sc = s->sc32;
     return a;
 }
 
+// Grid of the PCG kernels: enough blocks to fill every SM once, never more
+// than there are 256-REV tiles.
+template <typename T>
+static unsigned pcg_grid(vx_scene* s) {
+    unsigned* cached = sizeof(T) == 8 ? &s->grid64 : &s->grid32;
+    if (*cached) return *cached;
+    int occ_m = 0, occ_u = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_matvec<T, 0>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_update<T, 0>, kThreads, 0);
+    int occ = occ_m < occ_u ? occ_m : occ_u;
+    if (occ < 1) occ = 1;
+    unsigned g = (unsigned)(s->sm_count * occ);
+    unsigned tiles = s->blocks ? s->blocks : 1;
+    *cached = g < tiles ? g : tiles;
+    return *cached;
+}
+
 template <typename T>
 static void enqueue_chunk(vx_scene* s, cudaStream_t st) {
-    for (int it = 0; it < kChunk; ++it) {
-        int ping = it & 1;
-        IterArgs<T> a;
-        if constexpr (sizeof(T) == 8) a = args64(s, ping);
-        else a = args32(s, ping);
-        k_matvec<T><<<s->blocks, kThreads, 0, st>>>(a);
-        // the update reads the new direction
-        k_update<T><<<s->blocks, kThreads, 0, st>>>(a);
+    const unsigned G = pcg_grid<T>(s);
+    for (int it = 0; it < kChunk; it += 2) {
+        IterArgs<T> a0, a1;
+        if constexpr (sizeof(T) == 8) {
+            a0 = args64(s, 0);
+            a1 = args64(s, 1);
+        } else {
+            a0 = args32(s, 0);
+            a1 = args32(s, 1);
+        }
+        k_matvec<T, 0><<<G, kThreads, 0, st>>>(a0);
+        k_update<T, 0><<<G, kThreads, 0, st>>>(a0);
+        k_matvec<T, 1><<<G, kThreads, 0, st>>>(a1);
+        k_update<T, 1><<<G, kThreads, 0, st>>>(a1);
     }
 }
 
@@ -339,7 +450,8 @@ static cudaError_t chunk_graph(vx_scene* s, cudaGraphExec_t* out) {
 }
 
 // Replays iteration chunks until the device reports done; one chunk stays in
-// flight ahead of the host's check of the previous one.
+// flight ahead of the host's check of the previous one. The device stops at
+// the iteration cap, so at most cap/16 + 2 chunks run.
 template <typename T>
 static int32_t run_chunks(vx_scene* s, PcgScalars* sc, uint32_t max_iterations) {
     cudaGraphExec_t* g = sizeof(T) == 8 ? &s->chunk64 : &s->chunk32;
@@ -348,8 +460,9 @@ static int32_t run_chunks(vx_scene* s, PcgScalars* sc, uint32_t max_iterations) 
         set_error("PCG graph capture failed: %s", cudaGetErrorString(e));
         return VX_CUDA_ERROR;
     }
-    uint32_t chunks = (max_iterations + kChunk - 1) / kChunk;
-    for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t chunks = max_iterations / kChunk + 2;
+    bool seen_done = false;
+    for (uint32_t c = 0; c < chunks && !seen_done; ++c) {
         e = cudaGraphLaunch(*g, s->stream);
         s->launches += 2 * kChunk;
         if (e == cudaSuccess)
@@ -365,7 +478,7 @@ static int32_t run_chunks(vx_scene* s, PcgScalars* sc, uint32_t max_iterations) 
                 set_error("PCG chunk failed: %s", cudaGetErrorString(e));
                 return VX_CUDA_ERROR;
             }
-            if (s->h_done[(c - 1) & 1]) break;
+            seen_done = s->h_done[(c - 1) & 1] != 0;
         }
     }
     return VX_OK;
@@ -387,7 +500,7 @@ int32_t true_residual(vx_scene* s, double* out) {
         return VX_OK;
     }
     IterArgs<double> a = args64(s, 0);
-    k_residual64<<<s->blocks, kThreads, 0, s->stream>>>(a, s->b64, s->r64, s->sc);
+    k_residual64<<<pcg_grid<double>(s), kThreads, 0, s->stream>>>(a, s->b64, s->r64, s->sc);
     int32_t st = fetch_scalars(s, s->sc);
     if (st != VX_OK) return st;
     *out = s->h_sc->residual;
@@ -402,7 +515,7 @@ int32_t solve_fp64(vx_scene* s, double tolerance, uint32_t max_iterations, vx_pa
         return VX_OK;
     }
     IterArgs<double> a = args64(s, 0);
-    k_init<double><<<s->blocks, kThreads, 0, s->stream>>>(a, s->b64, nullptr, tolerance, max_iterations);
+    k_init<double><<<pcg_grid<double>(s), kThreads, 0, s->stream>>>(a, s->b64, nullptr, tolerance, max_iterations);
     s->launches += 1;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -422,7 +535,7 @@ int32_t solve_fp64(vx_scene* s, double tolerance, uint32_t max_iterations, vx_pa
 }
 
 int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, double inner_tolerance,
-                    uint32_t max_outer, vx_pass_stats* out) {
+                    uint32_t max_outer, int32_t kernel, vx_pass_stats* out) {
     out->iterations = 0;
     out->outer_iterations = 0;
     out->residual = 0.0;
@@ -436,9 +549,17 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
     cudaMemsetAsync(s->x64, 0, 3 * (size_t)s->n * sizeof(double), s->stream);
     uint32_t used = 0;
     int32_t status = VX_NOT_CONVERGED;
+    const unsigned G64 = pcg_grid<double>(s);
+    const unsigned G32 = pcg_grid<float>(s);
+    bool persistent = false;
+    if (kernel != VX_KERNEL_STREAMING) persistent = persistent_plan(s);
+    if (kernel == VX_KERNEL_PERSISTENT && !persistent) {
+        set_error("the persistent inner solve does not fit this scene on this GPU");
+        return VX_BAD_INPUT;
+    }
     for (uint32_t outer = 0;; ++outer) {
         IterArgs<double> a64 = args64(s, 0);
-        k_residual64<<<s->blocks, kThreads, 0, s->stream>>>(a64, s->b64, s->r64, s->sc);
+        k_residual64<<<G64, kThreads, 0, s->stream>>>(a64, s->b64, s->r64, s->sc);
         s->launches += 1;
         int32_t st = fetch_scalars(s, s->sc);
         if (st != VX_OK) return st;
@@ -457,10 +578,14 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
         // tighter than the FP32 operator allows
         double inner = fmax(inner_tolerance, 0.5 * tolerance / h.residual);
         uint32_t budget = max_iterations - used;
-        IterArgs<float> a32 = args32(s, 0);
-        k_init<float><<<s->blocks, kThreads, 0, s->stream>>>(a32, s->r64, &s->sc->r64_norm, inner, budget);
-        s->launches += 1;
-        st = run_chunks<float>(s, s->sc32, budget);
+        if (persistent) {
+            st = solve_inner_persistent(s, inner, budget);
+        } else {
+            IterArgs<float> a32 = args32(s, 0);
+            k_init<float><<<G32, kThreads, 0, s->stream>>>(a32, s->r64, &s->sc->r64_norm, inner, budget);
+            s->launches += 1;
+            st = run_chunks<float>(s, s->sc32, budget);
+        }
         if (st != VX_OK) return st;
         st = fetch_scalars(s, s->sc32);
         if (st != VX_OK) return st;
@@ -469,6 +594,10 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
         if (s->h_sc->status == VX_NONFINITE) {
             status = VX_NONFINITE;
             break;
+        }
+        if (s->h_sc->status == VX_TIMEOUT) {
+            set_error("persistent PCG: a grid barrier wait ran out");
+            return VX_TIMEOUT;
         }
         size_t m = 3 * (size_t)s->n;
         k_accumulate<<<(unsigned)((m + 255) / 256), 256, 0, s->stream>>>(s->n, s->x64, s->x32, &s->sc->r64_norm);
@@ -492,26 +621,28 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
     for (uint32_t r = 0; r < reps && err == cudaSuccess; ++r) {
         float a_ms = 0.f, b_ms = 0.f;
         if (precision == VX_PRECISION_FP64) {
+            const unsigned G = pcg_grid<double>(s);
             IterArgs<double> a = args64(s, 0);
-            k_init<double><<<s->blocks, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
+            k_init<double><<<G, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[0], s->stream);
-            k_matvec<double><<<s->blocks, kThreads, 0, s->stream>>>(a);
+            k_matvec<double, 0><<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[1], s->stream);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[2], s->stream);
-            k_update<double><<<s->blocks, kThreads, 0, s->stream>>>(a);
+            k_update<double, 0><<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[3], s->stream);
         } else {
+            const unsigned G = pcg_grid<float>(s);
             IterArgs<float> a = args32(s, 0);
-            k_init<float><<<s->blocks, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
+            k_init<float><<<G, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[0], s->stream);
-            k_matvec<float><<<s->blocks, kThreads, 0, s->stream>>>(a);
+            k_matvec<float, 0><<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[1], s->stream);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[2], s->stream);
-            k_update<float><<<s->blocks, kThreads, 0, s->stream>>>(a);
+            k_update<float, 0><<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[3], s->stream);
         }
         err = cudaEventSynchronize(ev[3]);
@@ -527,6 +658,35 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
     }
     out_us[0] = 1000.0 * tm / reps;
     out_us[1] = 1000.0 * tu / reps;
+    out_us[2] = out_us[3] = 0.0;
+    if (precision == VX_PRECISION_MIXED && persistent_plan(s)) {
+        // one persistent inner solve of a fixed iteration count on r = b
+        const uint32_t iters = 64;
+        cudaMemsetAsync(s->x64, 0, 3 * (size_t)s->n * sizeof(double), s->stream);
+        IterArgs<double> a64 = args64(s, 0);
+        k_residual64<<<pcg_grid<double>(s), kThreads, 0, s->stream>>>(a64, s->b64, s->r64, s->sc);
+        if (flush_bytes) cudaMemsetAsync(flush, 0x5a, flush_bytes, s->stream);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s->stream);
+        int32_t st = solve_inner_persistent(s, 0.0, iters);
+        cudaEventRecord(e1, s->stream);
+        float ms = 0.f;
+        err = cudaEventSynchronize(e1);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        int32_t its = 0;
+        if (err == cudaSuccess) err = cudaMemcpy(&its, &s->sc32->iterations, 4, cudaMemcpyDeviceToHost);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st != VX_OK) return st;
+        if (err != cudaSuccess) {
+            set_error("kernel timing failed: %s", cudaGetErrorString(err));
+            return VX_CUDA_ERROR;
+        }
+        out_us[2] = its > 0 ? 1000.0 * ms / its : 0.0;
+        out_us[3] = its;
+    }
     return VX_OK;
 }
 

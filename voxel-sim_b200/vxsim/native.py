@@ -21,6 +21,7 @@ HEADER = ROOT / "include" / "vxcorot.h"
 
 VX_OK, VX_NOT_CONVERGED, VX_NONFINITE, VX_OOM, VX_BAD_INPUT, VX_CUDA_ERROR, VX_TIMEOUT, VX_NO_DEVICE = range(8)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+KERNEL_AUTO, KERNEL_STREAMING, KERNEL_PERSISTENT = 0, 1, 2
 EMPTY = 0xFFFFFFFF
 
 u8p = C.POINTER(C.c_uint8)
@@ -53,7 +54,7 @@ class VxSceneDesc(C.Structure):
 class VxPassParams(C.Structure):
     _fields_ = [("h", C.c_double), ("tolerance", C.c_double), ("max_iterations", C.c_uint32),
                 ("precision", C.c_int32), ("reuse_preconditioner", C.c_int32), ("inner_tolerance", C.c_double),
-                ("max_outer", C.c_uint32)]
+                ("max_outer", C.c_uint32), ("kernel", C.c_int32)]
 
 
 class VxPassStats(C.Structure):
@@ -268,10 +269,11 @@ class DeviceScene:
         return int(load().vx_scene_stream(self.h) or 0)
 
     def kernel_times(self, precision, reps=20, flush_ptr=0, flush_bytes=0):
-        out = np.zeros(2, np.float64)
+        out = np.zeros(4, np.float64)
         check(load().vx_scene_kernel_times(self.h, precision, reps, C.c_void_p(flush_ptr), flush_bytes,
                                            _p(out, C.c_double)))
-        return {"matvec_us": float(out[0]), "update_us": float(out[1])}
+        return {"matvec_us": float(out[0]), "update_us": float(out[1]), "persistent_iter_us": float(out[2]),
+                "persistent_iterations": int(out[3])}
 
     # -- the solve ------------------------------------------------------------
     def fit_rotations(self) -> float:
@@ -280,8 +282,8 @@ class DeviceScene:
         return v.value
 
     def corotational_pass(self, h, tolerance, max_iterations, precision=PRECISION_FP64, reuse=False,
-                          inner_tolerance=0.0, max_outer=0, allow=(VX_NOT_CONVERGED,)):
-        p = VxPassParams(h, tolerance, max_iterations, precision, int(reuse), inner_tolerance, max_outer)
+                          inner_tolerance=0.0, max_outer=0, kernel=KERNEL_AUTO, allow=(VX_NOT_CONVERGED,)):
+        p = VxPassParams(h, tolerance, max_iterations, precision, int(reuse), inner_tolerance, max_outer, kernel)
         st = VxPassStats()
         status = check(load().vx_corotational_pass(self.h, C.byref(p), C.byref(st)), allow=allow)
         d = st.as_dict()
