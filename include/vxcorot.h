@@ -266,6 +266,43 @@ int32_t vx_corotational_pass(vx_scene* scene, const vx_pass_params* params, vx_p
 int32_t vx_bond_stress(vx_scene* scene, float* ratio, float* force, uint32_t* near,
                        uint32_t cap, uint32_t* near_count);
 
+/*
+ * ---- scene pool: many scenes resident in one arena, solved together ----
+ *
+ * Batched and served forms (no counterpart in the reference, which steps one
+ * scene at a time). A pool reserves device memory for max_revs REVs (in
+ * 256-REV tiles) and max_slots scenes up front; vx_pool_add places a scene in
+ * the first free tile range that holds it and returns VX_OOM when none does
+ * (admission by footprint). Scenes keep their state on the device between
+ * calls. `enabled[max_slots]` selects the slots a call works on (NULL = every
+ * occupied slot); the others are untouched. vx_pool_pass solves every selected
+ * scene's corotational pass together in the VX_PRECISION_MIXED form with
+ * per-scene scalars, so a scene's result does not depend on the other scenes
+ * in the call. out[max_slots] receives per-slot statistics. Per-slot arrays
+ * use the layouts of the single-scene calls for that scene's n REVs.
+ */
+#define VX_POOL_MATERIALS 16
+typedef struct vx_pool vx_pool;
+int32_t vx_pool_create(vx_ctx* ctx, uint64_t max_revs, uint32_t max_slots, vx_pool** out_pool);
+int32_t vx_pool_destroy(vx_pool* pool);
+uint64_t vx_pool_footprint_bytes(uint64_t max_revs, uint32_t max_slots);
+uint32_t vx_pool_capacity_slots(vx_pool* pool);
+int32_t vx_pool_free_revs(vx_pool* pool, uint64_t* out_free_revs, uint64_t* out_largest_range);
+int32_t vx_pool_add(vx_pool* pool, const vx_scene_desc* desc, uint32_t* out_slot);
+int32_t vx_pool_remove(vx_pool* pool, uint32_t slot);
+int32_t vx_pool_set_positions(vx_pool* pool, uint32_t slot, const double* xyz);
+int32_t vx_pool_get_positions(vx_pool* pool, uint32_t slot, double* xyz);
+int32_t vx_pool_get_rotations(vx_pool* pool, uint32_t slot, double* xyzw);
+int32_t vx_pool_set_targets(vx_pool* pool, uint32_t slot, const uint8_t* mask, const double* xyz);
+int32_t vx_pool_set_loads(vx_pool* pool, uint32_t slot, const double* xyz);
+int32_t vx_pool_set_predicted(vx_pool* pool, uint32_t slot, const double* xyz);
+int32_t vx_pool_fit_rotations(vx_pool* pool, const uint8_t* enabled, double* out_max_angle);
+int32_t vx_pool_pass(vx_pool* pool, const uint8_t* enabled, const vx_pass_params* params, vx_pass_stats* out);
+int32_t vx_pool_bond_stress(vx_pool* pool, uint32_t slot, float* ratio, float* force, uint32_t* near,
+                            uint32_t cap, uint32_t* near_count);
+int32_t vx_pool_checkpoint(vx_pool* pool, int32_t op);
+void* vx_pool_stream(vx_pool* pool);
+
 /* ---- state checkpoint and measurement hooks (no counterpart in the reference) ---- */
 
 /* op 0 saves the scene's positions and rotations on the device, op 1 restores them. */

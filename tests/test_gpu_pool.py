@@ -1,0 +1,134 @@
+"""The scene pool (batched and served forms) against single-scene solves.
+
+A pooled scene's pass must give the single scene's answer within the stated
+1e-8 target, be bit-identical whether it is alone in the pool or solved with
+other scenes, leave slots outside the call untouched, and refuse scenes that
+do not fit (admission by footprint).
+"""
+import numpy as np
+import pytest
+
+import pyoracle as O
+from vxsim import native as N
+from vxsim import scenes as S
+
+pytestmark = pytest.mark.gpu
+
+H, TOL, CAP = 1e-3, 1e-8, 50000
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = N.Context(0)
+    yield c
+    c.close()
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+def scenes():
+    rng = np.random.default_rng(11)
+    return [S.mixed_block(8, seed=1), S.wood_cube(), S.box_union_scene(rng, 8, 20), S.mixed_block(12, seed=3)]
+
+
+def single(ctx, scene):
+    d = N.DeviceScene(ctx, scene)
+    d.fit_rotations()
+    st = d.corotational_pass(H, TOL, CAP, precision=N.PRECISION_MIXED)
+    x = d.positions()
+    d.close()
+    return x, st
+
+
+def test_pool_pass_matches_single_scene_solves(ctx):
+    sc = scenes()
+    pool = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)
+    slots = [pool.add(s) for s in sc]
+    pool.fit_rotations()
+    status, stats = pool.corotational_pass(H, TOL, CAP)
+    assert status == N.VX_OK
+    for s, k in zip(sc, slots):
+        assert stats[k]["converged"] == 1 and stats[k]["true_residual"] <= TOL, stats[k]
+        x1, st1 = single(ctx, s)
+        x0 = s.position
+        # both meet 1e-8 against the FP64 operator; they agree to the solve error
+        assert rel(pool.positions(k) - x0, x1 - x0) < 1e-5
+    pool.close()
+
+
+def test_pool_scene_is_bit_identical_alone_and_in_a_mix(ctx):
+    sc = scenes()
+    alone = N.DevicePool(ctx, 1 << 16, 4)
+    a = alone.add(sc[0])
+    alone.fit_rotations()
+    alone.corotational_pass(H, TOL, CAP)
+    mix = N.DevicePool(ctx, 1 << 17, 8)
+    others = [mix.add(s) for s in sc[1:3]]
+    b = mix.add(sc[0])
+    mix.add(sc[3])
+    mix.fit_rotations()
+    mix.corotational_pass(H, TOL, CAP)
+    assert np.array_equal(alone.positions(a), mix.positions(b))
+    assert np.array_equal(alone.rotations(a), mix.rotations(b))
+    alone.close()
+    mix.close()
+
+
+def test_disabled_slots_are_untouched_and_rotations_match(ctx):
+    sc = scenes()
+    pool = N.DevicePool(ctx, 1 << 17, 8)
+    slots = [pool.add(s) for s in sc]
+    before = pool.positions(slots[1]).copy()
+    angles = pool.fit_rotations(enabled=[slots[0], slots[2]])
+    assert angles[slots[1]] == 0.0
+    pool.corotational_pass(H, TOL, CAP, enabled=[slots[0], slots[2]])
+    assert np.array_equal(pool.positions(slots[1]), before)
+    d = N.DeviceScene(ctx, sc[0])
+    ang = d.fit_rotations()
+    assert abs(ang - angles[slots[0]]) <= 1e-12 * max(ang, 1e-30)
+    d.close()
+    pool.close()
+
+
+def test_pool_admission_and_slot_reuse(ctx):
+    big = S.mixed_block(16, seed=2)     # 4096 REVs = 16 tiles
+    small = S.wood_cube()               # 1000 REVs = 4 tiles
+    pool = N.DevicePool(ctx, 20 * 256, 4)
+    a = pool.add(big)
+    b = pool.add(small)
+    with pytest.raises(N.VxError) as e:
+        pool.add(S.mixed_block(8, seed=9))  # 512 REVs: no 2-tile range left
+    assert e.value.status == N.VX_OOM
+    pool.remove(b)
+    c = pool.add(S.mixed_block(8, seed=9))
+    assert c == b
+    pool.fit_rotations()
+    status, stats = pool.corotational_pass(H, TOL, CAP)
+    assert status == N.VX_OK and stats[c]["converged"] == 1
+    x1, _ = single(ctx, S.mixed_block(8, seed=9))
+    x0 = S.mixed_block(8, seed=9).position
+    assert rel(pool.positions(c) - x0, x1 - x0) < 1e-5
+    pool.close()
+
+
+def test_pool_bond_stress_matches_single_scene(ctx):
+    s = S.mixed_block(8, seed=4)
+    pool = N.DevicePool(ctx, 1 << 14, 2)
+    k = pool.add(S.wood_cube())
+    j = pool.add(s)
+    pool.fit_rotations()
+    pool.corotational_pass(H, 1e-12, CAP)
+    d = N.DeviceScene(ctx, s)
+    d.set_positions(pool.positions(j))
+    d.set_rotations(pool.rotations(j))
+    d.corotational_pass(H, 1e-12, 10)  # assembles the same frames; positions then reset
+    d.set_positions(pool.positions(j))
+    g = d.bond_stress()
+    p = pool.bond_stress(j)
+    assert np.array_equal(g["ratio"] < 0, p["ratio"] < 0)
+    live = g["ratio"] >= 0
+    assert np.all(np.abs(g["ratio"][live] - p["ratio"][live]) <= 1e-5 * np.maximum(g["ratio"][live], 1e-3))
+    d.close()
+    pool.close()

@@ -25,6 +25,8 @@ void set_error(const char* fmt, ...) {
 }
 void clear_error() { g_error.clear(); }
 
+void scene_release(vx_scene* s);
+
 // Carves every device array of a scene out of one allocation. With a null
 // base it only measures.
 static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
@@ -122,6 +124,59 @@ static int32_t download_vec3(vx_scene* s, double* dst, const double* src) {
     for (size_t i = 0; i < n; ++i)
         for (int c = 0; c < 3; ++c) dst[3 * i + c] = tmp[c * n + i];
     return VX_OK;
+}
+
+// Allocates a scene's arena (n REVs, material_count materials), its stream and
+// pinned host buffers, and clears the arena.
+int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_count) {
+    s->ctx = ctx;
+    s->device = ctx->device;
+    s->sm_count = ctx->sm_count > 0 ? ctx->sm_count : 1;
+    s->n = n;
+    s->blocks = (n + 255) / 256;
+    s->material_count = material_count;
+    Arena probe;
+    carve(s, probe, n, material_count);
+    cudaError_t e = cudaMalloc(&s->arena.base, probe.used);
+    if (e != cudaSuccess) return cuda_fail(e, "scene allocation");
+    s->arena.size = probe.used;
+    s->arena.used = 0;
+    carve(s, s->arena, n, material_count);
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_stage, 4 * (size_t)(n ? n : 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_sc, sizeof(PcgScalars));
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_done, 2 * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->arena.base, 0, s->arena.size, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+        int32_t st = cuda_fail(e, "scene set-up");
+        scene_release(s);
+        return st;
+    }
+    return VX_OK;
+}
+
+void scene_release(vx_scene* s) {
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->chunk64) cudaGraphExecDestroy(s->chunk64);
+    if (s->chunk32) cudaGraphExecDestroy(s->chunk32);
+    for (int k = 0; k < 2; ++k)
+        if (s->ev[k]) cudaEventDestroy(s->ev[k]);
+    if (s->h_sc) cudaFreeHost(s->h_sc);
+    if (s->h_done) cudaFreeHost(s->h_done);
+    if (s->h_stage) cudaFreeHost(s->h_stage);
+    if (s->arena.base) cudaFree(s->arena.base);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    s->chunk64 = s->chunk32 = nullptr;
+    s->ev[0] = s->ev[1] = nullptr;
+    s->h_sc = nullptr;
+    s->h_done = nullptr;
+    s->h_stage = nullptr;
+    s->arena.base = nullptr;
+    s->stream = nullptr;
 }
 
 }  // namespace vx
@@ -269,37 +324,17 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
     cudaSetDevice(ctx->device);
     vx_scene* s = new (std::nothrow) vx_scene();
     if (!s) return VX_OOM;
-    s->ctx = ctx;
-    s->device = ctx->device;
-    s->sm_count = ctx->sm_count > 0 ? ctx->sm_count : 1;
-    s->n = n;
-    s->blocks = (n + 255) / 256;
-    s->material_count = d->material_count;
-    Arena probe;
-    carve(s, probe, n, d->material_count);
-    cudaError_t e = cudaMalloc(&s->arena.base, probe.used);
-    if (e != cudaSuccess) {
+    int32_t ar = scene_alloc(s, ctx, n, d->material_count);
+    if (ar != VX_OK) {
         delete s;
-        return cuda_fail(e, "scene allocation");
+        return ar;
     }
-    s->arena.size = probe.used;
-    carve(s, s->arena, n, d->material_count);
     auto fail = [&](cudaError_t err, const char* what) {
         int32_t st = cuda_fail(err, what);
         vx_scene_destroy(s);
         return st;
     };
-    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return fail(e, "stream");
-    e = cudaMallocHost(&s->h_stage, 4 * (size_t)(n ? n : 1) * sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_sc, sizeof(PcgScalars));
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_done, 2 * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev[1], cudaEventDisableTiming);
-    if (e != cudaSuccess) return fail(e, "host buffers");
-    e = cudaMemsetAsync(s->arena.base, 0, s->arena.size, s->stream);
-    if (e != cudaSuccess) return fail(e, "clear");
-
+    cudaError_t e = cudaSuccess;
     size_t m = n;
     // host staging in device layout
     std::vector<double4> rot(m);
@@ -361,17 +396,7 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
 
 int32_t vx_scene_destroy(vx_scene* s) {
     if (!s) return VX_OK;
-    cudaSetDevice(s->device);
-    if (s->stream) cudaStreamSynchronize(s->stream);
-    if (s->chunk64) cudaGraphExecDestroy(s->chunk64);
-    if (s->chunk32) cudaGraphExecDestroy(s->chunk32);
-    for (int k = 0; k < 2; ++k)
-        if (s->ev[k]) cudaEventDestroy(s->ev[k]);
-    if (s->h_sc) cudaFreeHost(s->h_sc);
-    if (s->h_stage) cudaFreeHost(s->h_stage);
-    if (s->h_done) cudaFreeHost(s->h_done);
-    if (s->arena.base) cudaFree(s->arena.base);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    scene_release(s);
     delete s;
     return VX_OK;
 }

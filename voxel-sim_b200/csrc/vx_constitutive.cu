@@ -92,6 +92,7 @@ __global__ void k_assemble_bonds(SceneView s, BondArrays b, uint32_t* __restrict
     if (e >= 3 * (size_t)n) return;
     int a = (int)(e / n);
     uint32_t i = (uint32_t)(e - (size_t)a * n);
+    if (!tile_active(s.tile_on, i)) return;
     uint32_t j = s.nbr[e];
     size_t m3n = 3 * (size_t)n;
     uint8_t st = 0;
@@ -158,7 +159,7 @@ struct RevOut {
 __global__ void k_assemble_revs(SceneView s, BondArrays b, RevOut o, double h, int reuse) {
     const uint32_t n = s.n;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || !tile_active(s.tile_on, i)) return;
     size_t m3n = 3 * (size_t)n;
     double m = (double)s.param1[i].w / (h * h);
     double D[6] = {m, m, m, 0.0, 0.0, 0.0};
@@ -211,15 +212,16 @@ cudaError_t launch_assembly(vx_scene* s, double h, bool reuse_preconditioner) {
     return cudaGetLastError();
 }
 
-__global__ void k_apply_correction(uint32_t n, double* __restrict__ pos, const double* __restrict__ dx) {
+__global__ void k_apply_correction(uint32_t n, double* __restrict__ pos, const double* __restrict__ dx,
+                                   const uint8_t* __restrict__ tile_on) {
     size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t < 3 * (size_t)n) pos[t] += dx[t];
+    if (t < 3 * (size_t)n && tile_active(tile_on, t % n)) pos[t] += dx[t];
 }
 
 cudaError_t launch_apply_correction(vx_scene* s) {
     size_t m = 3 * (size_t)s->n;
     if (m == 0) return cudaSuccess;
-    k_apply_correction<<<(unsigned)((m + 255) / 256), 256, 0, s->stream>>>(s->n, s->pos, s->x64);
+    k_apply_correction<<<(unsigned)((m + 255) / 256), 256, 0, s->stream>>>(s->n, s->pos, s->x64, s->tile_on);
     return cudaGetLastError();
 }
 
@@ -310,6 +312,7 @@ __global__ void k_bond_stress(SceneView s, BondArrays b, float* __restrict__ rat
     if (e >= m3n) return;
     int a = (int)(e / n);
     uint32_t i = (uint32_t)(e - (size_t)a * n);
+    if (!tile_active(s.tile_on, i)) return;
     uint32_t j = s.nbr[e];
     double r = -1.0;
     v3 f = mk(0.0, 0.0, 0.0);

@@ -22,7 +22,13 @@ struct SceneView {
     const uint32_t* rev;
     const float4* bond_a;
     const float4* bond_b;
+    const uint8_t* tile_on;  // per 256-REV tile: 0 = skip (pool tiles of disabled or free slots); null = all on
+    const uint32_t* tile_scene;  // per tile: pool slot (for per-slot maxima); null for a single scene
 };
+
+__device__ __forceinline__ bool tile_active(const uint8_t* tile_on, size_t i) {
+    return tile_on == nullptr || tile_on[i >> 8] != 0;
+}
 
 SceneView view_of(const vx_scene* s);
 

@@ -8,9 +8,9 @@
 namespace vx {
 
 SceneView view_of(const vx_scene* s) {
-    return SceneView{s->n,      s->pos,    s->pred,  s->loads,     s->rot,   s->kin,
-                     s->flags,  s->param0, s->param1, s->matid,    s->materials,
-                     s->nbr,    s->rev,    s->bond_a, s->bond_b};
+    return SceneView{s->n,      s->pos,    s->pred,   s->loads, s->rot,    s->kin,
+                     s->flags,  s->param0, s->param1, s->matid, s->materials,
+                     s->nbr,    s->rev,    s->bond_a, s->bond_b, s->tile_on, s->tile_scene};
 }
 
 // free[i] bit a = axis a is in the system: not kinematic, not targeted
@@ -106,7 +106,7 @@ __global__ void k_fit_rotations(SceneView s, double4* __restrict__ rot_out,
                                 unsigned long long* __restrict__ max_bits) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double angle = 0.0;
-    if (i < s.n && !s.kin[i]) {
+    if (i < s.n && !s.kin[i] && tile_active(s.tile_on, i)) {
         const uint32_t n = s.n;
         v3 xi = mk(s.pos[i], s.pos[n + i], s.pos[2 * (size_t)n + i]);
         m3 f;
@@ -175,12 +175,15 @@ __global__ void k_fit_rotations(SceneView s, double4* __restrict__ rot_out,
         double v = threadIdx.x < (blockDim.x >> 5) ? smax[threadIdx.x] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (threadIdx.x == 0 && v > 0.0) atomicMax(max_bits, (unsigned long long)__double_as_longlong(v));
+        // a 256-thread block is one tile, so its maximum belongs to one pool slot
+        unsigned long long* slot = max_bits + (s.tile_scene ? s.tile_scene[blockIdx.x] : 0u);
+        if (threadIdx.x == 0 && v > 0.0) atomicMax(slot, (unsigned long long)__double_as_longlong(v));
     }
 }
 
 cudaError_t launch_fit_rotations(vx_scene* s) {
-    cudaMemsetAsync(s->max_angle_bits, 0, sizeof(unsigned long long), s->stream);
+    cudaMemsetAsync(s->max_angle_bits, 0, sizeof(unsigned long long) * (s->pool_slots ? s->pool_slots : 1),
+                    s->stream);
     if (s->n == 0) return cudaGetLastError();
     // rotations are read (old column, previous quaternion) and written by the
     // same thread only, so in-place update is safe

@@ -1,0 +1,140 @@
+// vx_pcg_core.cuh — the operator row and vector helpers shared by the
+// single-scene PCG kernels (vx_pcg.cu) and the pool kernels (vx_pool.cu).
+#pragma once
+
+#include "vx_device.cuh"
+#include "vx_internal.h"
+#include "vx_layout.cuh"
+#include "vx_reduce.cuh"
+
+namespace vx {
+
+template <typename T>
+struct IterArgs {
+    uint32_t n;
+    const uint8_t* flags;
+    const T* D;       // projected diagonal (sym layout)
+    const T* K;       // per-axis bond K (3 sym layouts), zero when not assembled
+    const T* Dinv;
+    const uint32_t* nbr;
+    const uint32_t* rev;
+    const T* z_in;    // matvec: z
+    const T* p_old;   // matvec: previous direction
+    T* p_new;         // matvec: new direction
+    T* ap;
+    T* x;
+    T* r;
+    T* z;
+    double* pm;       // [G] partials of p.Ap
+    double* pu;       // [2][G] partials of r.z, r.r
+    PcgScalars* sc;
+};
+
+template <typename T>
+struct V3 {
+    T x, y, z;
+};
+
+template <typename T>
+__device__ __forceinline__ V3<T> mul(const Sym<T>& s, V3<T> v) {
+    return {s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
+            s.xz * v.x + s.yz * v.y + s.zz * v.z};
+}
+template <typename T>
+__device__ __forceinline__ V3<T> load_v(const T* p, size_t n, size_t i) {
+    return {p[i], p[n + i], p[2 * n + i]};
+}
+template <typename T>
+__device__ __forceinline__ V3<T> ldg_v(const T* __restrict__ p, size_t n, size_t i) {
+    return {__ldg(p + i), __ldg(p + n + i), __ldg(p + 2 * n + i)};
+}
+template <typename T>
+__device__ __forceinline__ void store_v(T* p, size_t n, size_t i, V3<T> v) {
+    p[i] = v.x;
+    p[n + i] = v.y;
+    p[2 * n + i] = v.z;
+}
+template <typename T>
+__device__ __forceinline__ double dot_d(V3<T> a, V3<T> b) {
+    return (double)a.x * (double)b.x + (double)a.y * (double)b.y + (double)a.z * (double)b.z;
+}
+
+// ---- block totals of the previous kernel's partials -----------------------------
+// Every thread gets the totals; the summation order is fixed (thread t adds
+// partials t, t+256, ... then the block tree), identical in every block.
+template <int NV>
+__device__ __forceinline__ void block_total(const double* part, unsigned G, double (&out)[NV]) {
+    __shared__ double sh[NV][kThreads / 32];
+    __shared__ double tot[NV];
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        v[k] = 0.0;
+        for (unsigned b = threadIdx.x; b < G; b += kThreads) v[k] += __ldcg(part + (size_t)k * G + b);
+    }
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) tot[k] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = tot[k];
+}
+
+template <int NV>
+__device__ __forceinline__ void block_partial(double (&v)[NV], double* part, unsigned G) {
+    __shared__ double sh[NV][kThreads / 32];
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) part[(size_t)k * G + blockIdx.x] = v[k];
+    }
+}
+
+// ---- one row of the operator ----------------------------------------------------------
+// A v at REV i = D_i v_i - P_i (sum over the three owned bonds K_(a,i) v_nbr(a)
+// + the three bonds owned by the -axis neighbours K_(a,k) v_k). `get(j)` returns
+// v_j. All loads are issued before the arithmetic: missing neighbours read REV
+// i itself and are masked to zero.
+template <typename T, typename Get>
+__device__ __forceinline__ V3<T> apply_row(const IterArgs<T>& a, uint32_t i, V3<T> vi, Get get) {
+    const size_t n = a.n;
+    uint32_t nb[6];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        nb[ax] = __ldg(a.nbr + ax * n + i);
+        nb[3 + ax] = __ldg(a.rev + ax * n + i);
+    }
+    const uint8_t fl = __ldg(a.flags + i);
+    const Sym<T> D = load_sym(a.D, n, i);
+    Sym<T> Ko[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) Ko[ax] = load_sym(a.K + ax * 6 * n, n, i);
+    uint32_t jj[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) jj[s] = nb[s] == VX_EMPTY_U32 ? i : nb[s];
+    V3<T> vj[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) vj[s] = get(jj[s]);
+    Sym<T> Kr[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) Kr[ax] = load_sym(a.K + ax * 6 * n, n, jj[3 + ax]);
+    V3<T> y = mul(D, vi);
+    V3<T> s = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const bool ok = nb[t] != VX_EMPTY_U32;
+        V3<T> v = ok ? vj[t] : V3<T>{T(0), T(0), T(0)};
+        V3<T> kv = mul(t < 3 ? Ko[t] : Kr[t - 3], v);
+        s.x += kv.x;
+        s.y += kv.y;
+        s.z += kv.z;
+    }
+    if (fl & 1) y.x -= s.x;
+    if (fl & 2) y.y -= s.y;
+    if (fl & 4) y.z -= s.z;
+    return y;
+}
+
+}  // namespace vx

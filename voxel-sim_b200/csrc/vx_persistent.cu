@@ -130,6 +130,17 @@ __device__ __forceinline__ F3 smul(const Sym<float>& s, F3 v) {
     return {s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
             s.xz * v.x + s.yz * v.y + s.zz * v.z};
 }
+// Inverse of a symmetric positive block by its adjugate, scaled by the largest
+// diagonal entry so the FP32 cofactors stay far from overflow.
+__device__ __forceinline__ Sym<float> sym_inverse(const Sym<float>& d) {
+    const float s = fmaxf(fmaxf(d.xx, d.yy), d.zz);
+    const float is = 1.0f / s;
+    const float xx = d.xx * is, yy = d.yy * is, zz = d.zz * is, xy = d.xy * is, xz = d.xz * is, yz = d.yz * is;
+    const float c00 = yy * zz - yz * yz, c01 = xz * yz - xy * zz, c02 = xy * yz - xz * yy;
+    const float c11 = xx * zz - xz * xz, c12 = xy * xz - xx * yz, c22 = xx * yy - xy * xy;
+    const float inv = is / (xx * c00 + xy * c01 + xz * c02);
+    return {c00 * inv, c11 * inv, c22 * inv, c01 * inv, c02 * inv, c12 * inv};
+}
 __device__ __forceinline__ Sym<float> ssym(const float* base, uint32_t cap, uint32_t li) {
     return {base[li], base[cap + li], base[2 * cap + li], base[3 * cap + li], base[4 * cap + li], base[5 * cap + li]};
 }
@@ -245,27 +256,22 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             F3 s = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
-                const uint32_t j = nb[t];
-                if (j == VX_EMPTY_U32) continue;
+                const uint32_t jraw = nb[t];
+                const bool ok = jraw != VX_EMPTY_U32;
+                const uint32_t j = ok ? jraw : i;
                 const int ax = t < 3 ? t : t - 3;
                 const uint32_t lj = j - lo;
-                F3 zj, pj;
-                if (lj < cnt) {
-                    zj = s3(sz, cap, lj);
-                    pj = s3(sp, cap, lj);
-                } else {
+                const bool inb = lj < cnt;
+                const uint32_t ls = inb ? lj : li;  // always a valid shared-memory slot
+                F3 zj = s3(sz, cap, ls), pj = s3(sp, cap, ls);
+                Sym<float> Kb = ssym(sK + (size_t)6 * ax * cap, cap, t < 3 ? li : ls);
+                if (!inb) {
                     zj = {__ldcg(a.zg + j), __ldcg(a.zg + n + j), __ldcg(a.zg + 2 * (size_t)n + j)};
                     pj = {__ldcg(a.pg + j), __ldcg(a.pg + n + j), __ldcg(a.pg + 2 * (size_t)n + j)};
+                    if (t >= 3) Kb = load_sym(a.K + (size_t)ax * 6 * n, n, j);
                 }
-                F3 pn = {fmaf(beta, pj.x, zj.x), fmaf(beta, pj.y, zj.y), fmaf(beta, pj.z, zj.z)};
-                Sym<float> Kb;
-                if (t < 3) {
-                    Kb = ssym(sK + (size_t)6 * ax * cap, cap, li);
-                } else if (lj < cnt) {
-                    Kb = ssym(sK + (size_t)6 * ax * cap, cap, lj);
-                } else {
-                    Kb = load_sym(a.K + (size_t)ax * 6 * n, n, j);
-                }
+                const float m = ok ? 1.f : 0.f;
+                F3 pn = {m * fmaf(beta, pj.x, zj.x), m * fmaf(beta, pj.y, zj.y), m * fmaf(beta, pj.z, zj.z)};
                 F3 kv = smul(Kb, pn);
                 s.x += kv.x, s.y += kv.y, s.z += kv.z;
             }
@@ -315,7 +321,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 r[k][c] = fmaf(-alpha, ap[k][c], r[k][c]);
             }
             F3 rr = {r[k][0], r[k][1], r[k][2]};
-            F3 z = smul(load_sym(a.Dinv, n, i), rr);
+            F3 z = smul(sym_inverse(ssym(sD, cap, li)), rr);
             w3(sz, cap, li, z);
             a.zg[i] = z.x, a.zg[n + i] = z.y, a.zg[2 * (size_t)n + i] = z.z;
             au[0] += (double)rr.x * z.x + (double)rr.y * z.y + (double)rr.z * z.z;

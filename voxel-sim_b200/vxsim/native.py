@@ -318,3 +318,175 @@ def solve_pcg_f32(rows, max_iterations, tolerance):
                                  _p(a["blocks54"], C.c_float), _p(a["inv9"], C.c_float), n, max_iterations,
                                  tolerance, _p(dx, C.c_float), C.byref(it), C.byref(rel))
     return st, dx[:3 * n].reshape(-1, 3), it.value, rel.value
+
+
+def scene_desc(scene, keep: dict):
+    """vx_scene_desc for a vxsim Scene; `keep` holds the arrays alive."""
+    keep.update(
+        pos=np.ascontiguousarray(scene.position, np.float64).reshape(-1),
+        rot=np.ascontiguousarray(scene.rotation, np.float64).reshape(-1),
+        kin=np.ascontiguousarray(scene.kinematic, np.uint8),
+        mass=np.ascontiguousarray(scene.mass, np.float32),
+        mat=np.ascontiguousarray(scene.material, np.uint32),
+        fib=np.ascontiguousarray(scene.fiber, np.float32).reshape(-1),
+        ani=np.ascontiguousarray(scene.anisotropy, np.float32),
+        solid=np.ascontiguousarray(scene.solid_fraction, np.float32),
+        therm=np.ascontiguousarray(scene.thermal_strength, np.float32),
+        dT=np.ascontiguousarray(scene.thermal_delta, np.float32),
+        nbr=np.ascontiguousarray(scene.neighbor, np.uint32).reshape(-1),
+        form=np.ascontiguousarray(scene.formation_offset, np.float32).reshape(-1),
+        plas=np.ascontiguousarray(scene.plastic_strain, np.float32).reshape(-1),
+        dmg=np.ascontiguousarray(scene.damage, np.float32).reshape(-1),
+        mats=material_array(scene.materials),
+    )
+    k = keep
+    return VxSceneDesc(
+        scene.n, _p(k["pos"], C.c_double), _p(k["rot"], C.c_double), _p(k["kin"], C.c_uint8),
+        _p(k["mass"], C.c_float), _p(k["mat"], C.c_uint32), k["mats"], len(scene.materials),
+        _p(k["fib"], C.c_float), _p(k["ani"], C.c_float), _p(k["solid"], C.c_float), _p(k["therm"], C.c_float),
+        _p(k["dT"], C.c_float), _p(k["nbr"], C.c_uint32), _p(k["form"], C.c_float), _p(k["plas"], C.c_float),
+        _p(k["dmg"], C.c_float))
+
+
+def _bind_pool(L):
+    L.vx_pool_create.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)]
+    L.vx_pool_destroy.argtypes = [C.c_void_p]
+    L.vx_pool_footprint_bytes.restype = C.c_uint64
+    L.vx_pool_footprint_bytes.argtypes = [C.c_uint64, C.c_uint32]
+    L.vx_pool_capacity_slots.restype = C.c_uint32
+    L.vx_pool_capacity_slots.argtypes = [C.c_void_p]
+    L.vx_pool_free_revs.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.vx_pool_add.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), C.POINTER(C.c_uint32)]
+    L.vx_pool_remove.argtypes = [C.c_void_p, C.c_uint32]
+    for name in ("vx_pool_set_positions", "vx_pool_get_positions", "vx_pool_get_rotations", "vx_pool_set_loads",
+                 "vx_pool_set_predicted"):
+        getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, f64p]
+    L.vx_pool_set_targets.argtypes = [C.c_void_p, C.c_uint32, u8p, f64p]
+    L.vx_pool_fit_rotations.argtypes = [C.c_void_p, u8p, f64p]
+    L.vx_pool_pass.argtypes = [C.c_void_p, u8p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
+    L.vx_pool_bond_stress.argtypes = [C.c_void_p, C.c_uint32, f32p, f32p, u32p, C.c_uint32, u32p]
+    L.vx_pool_checkpoint.argtypes = [C.c_void_p, C.c_int32]
+    L.vx_pool_stream.restype = C.c_void_p
+    L.vx_pool_stream.argtypes = [C.c_void_p]
+
+
+class DevicePool:
+    """Scenes resident in one device arena (vx_pool), solved together."""
+
+    def __init__(self, ctx: Context, max_revs: int, max_slots: int):
+        L = load()
+        if not getattr(L, "_pool_bound", False):
+            _bind_pool(L)
+            L._pool_bound = True
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        check(L.vx_pool_create(ctx.h, max_revs, max_slots, C.byref(self.h)))
+        self.slots = max_slots
+        self.n = {}
+
+    def close(self):
+        if self.h:
+            load().vx_pool_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, scene) -> int:
+        keep = {}
+        desc = scene_desc(scene, keep)
+        slot = C.c_uint32()
+        check(load().vx_pool_add(self.h, C.byref(desc), C.byref(slot)))
+        s = slot.value
+        self.n[s] = scene.n
+        self.set_targets(s, scene.target_mask, scene.target)
+        if np.any(scene.loads):
+            self.set_loads(s, scene.loads)
+        return s
+
+    def remove(self, slot):
+        check(load().vx_pool_remove(self.h, slot))
+        self.n.pop(slot, None)
+
+    def free_revs(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        check(load().vx_pool_free_revs(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def _v(self, a):
+        return np.ascontiguousarray(a, np.float64).reshape(-1)
+
+    def set_positions(self, slot, x):
+        x = self._v(x)
+        check(load().vx_pool_set_positions(self.h, slot, _p(x, C.c_double)))
+
+    def positions(self, slot):
+        out = np.zeros(3 * self.n[slot], np.float64)
+        check(load().vx_pool_get_positions(self.h, slot, _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def rotations(self, slot):
+        out = np.zeros(4 * self.n[slot], np.float64)
+        check(load().vx_pool_get_rotations(self.h, slot, _p(out, C.c_double)))
+        return out.reshape(-1, 4)
+
+    def set_targets(self, slot, mask, target=None):
+        m = np.ascontiguousarray(mask, np.uint8)
+        t = None if target is None else self._v(target)
+        check(load().vx_pool_set_targets(self.h, slot, _p(m, C.c_uint8), _p(t, C.c_double)))
+
+    def set_loads(self, slot, loads):
+        x = self._v(loads)
+        check(load().vx_pool_set_loads(self.h, slot, _p(x, C.c_double)))
+
+    def set_predicted(self, slot, x=None):
+        x = None if x is None else self._v(x)
+        check(load().vx_pool_set_predicted(self.h, slot, _p(x, C.c_double)))
+
+    def _mask(self, enabled):
+        if enabled is None:
+            return None
+        m = np.zeros(self.slots, np.uint8)
+        m[list(enabled)] = 1
+        return m
+
+    def fit_rotations(self, enabled=None):
+        m = self._mask(enabled)
+        out = np.zeros(self.slots, np.float64)
+        check(load().vx_pool_fit_rotations(self.h, _p(m, C.c_uint8), _p(out, C.c_double)))
+        return out
+
+    def corotational_pass(self, h, tolerance, max_iterations, enabled=None, reuse=False, inner_tolerance=0.0,
+                          max_outer=0, allow=(VX_NOT_CONVERGED,)):
+        m = self._mask(enabled)
+        p = VxPassParams(h, tolerance, max_iterations, PRECISION_MIXED, int(reuse), inner_tolerance, max_outer,
+                         KERNEL_AUTO)
+        stats = (VxPassStats * self.slots)()
+        status = check(load().vx_pool_pass(self.h, _p(m, C.c_uint8), C.byref(p), stats), allow=allow)
+        return status, [stats[k].as_dict() for k in range(self.slots)]
+
+    def bond_stress(self, slot, with_force=True):
+        n = self.n[slot]
+        ratio = np.zeros(3 * n, np.float32)
+        force = np.zeros(9 * n, np.float32) if with_force else None
+        near = np.zeros(3 * n, np.uint32)
+        cnt = C.c_uint32()
+        check(load().vx_pool_bond_stress(self.h, slot, _p(ratio, C.c_float), _p(force, C.c_float),
+                                         _p(near, C.c_uint32), 3 * n, C.byref(cnt)))
+        out = dict(ratio=ratio.reshape(3, -1), near=near[:cnt.value].copy())
+        if with_force:
+            out["force"] = force.reshape(3, -1, 3)
+        return out
+
+    def save_state(self):
+        check(load().vx_pool_checkpoint(self.h, 0))
+
+    def restore_state(self):
+        check(load().vx_pool_checkpoint(self.h, 1))
+
+    @property
+    def stream_ptr(self):
+        return int(load().vx_pool_stream(self.h) or 0)
