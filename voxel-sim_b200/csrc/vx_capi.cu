@@ -83,6 +83,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->near_count = A.take<uint32_t>(1);
     s->bond_count = A.take<uint32_t>(1);
     s->barrier = A.take<unsigned>(4);
+    s->zp32 = A.take<float>(6 * m);
 }
 
 uint64_t scene_bytes(uint32_t n, uint32_t material_count) {

@@ -124,7 +124,8 @@ struct vx_scene {
     unsigned long long* max_angle_bits;
     uint32_t* near_count;
     uint32_t* bond_count;         // bonds assembled by the last pass
-    unsigned* barrier;            // [4] persistent-kernel grid barrier: count, generation, error, pad
+    unsigned* barrier;            // [4] persistent kernel: u64 arrival count, error flag, pad
+    float* zp32;                  // [6n] persistent kernel's published (z, p_old): float4[n] then float2[n]
 
     // host mirrors
     double* h_stage = nullptr;       // pinned staging of host copies [4n doubles]

@@ -4,17 +4,20 @@
 // When a scene is small enough (up to ~1,900 REVs per SM), one cooperative
 // block of 512 threads per SM owns a contiguous range of REVs for the whole
 // inner solve. Its REVs' bond stiffness (three owned bonds), projected
-// diagonal, z and p live in shared memory; x, r, p and Ap live in registers
-// of the owning thread. Neighbours inside the range are read from shared
-// memory, the others from the global copies of z and p (L2). An iteration is
-// the same recurrence as k_matvec/k_update in vx_pcg.cu (src/solver.rs:1833-1911)
-// with two grid barriers:
-//   matvec phase  p = z + beta p_old, Ap, block partial of p.Ap   -> barrier A
-//   update phase  alpha, x, r, z = D^-1 r, partials of r.z, r.r   -> barrier B
-// Every block sums the partials in the same fixed order, so all blocks take
-// the same alpha, beta and stop decisions. The barriers spin a bounded number
-// of times; when the bound is hit the kernel records VX_TIMEOUT and every
-// block leaves its loop at its next barrier.
+// diagonal and the pair (z, p_old) live in shared memory as float4 + float2
+// records, so a neighbour costs two vector loads; x, r, p and Ap live in
+// registers of the owning thread. Neighbours outside the range are read from
+// the global copy of (z, p_old), which every block republishes once per
+// iteration. An iteration is the same recurrence as k_matvec/k_update in
+// vx_pcg.cu (src/solver.rs:1833-1911) with two grid-wide reductions:
+//   matvec phase  p = z + beta p_old, Ap, block partial of p.Ap   -> reduction A
+//   update phase  alpha, x, r, z = D^-1 r, partials of r.z, r.r   -> reduction B
+// A reduction is also the grid barrier: each block stores its partials and
+// adds one to an arrival counter; a block passes once the counter shows every
+// block's arrival, and sums the partials in block order, so all blocks take
+// the same alpha, beta and stop decisions. The waits are bounded; when a
+// bound is hit the kernel records VX_TIMEOUT and every block leaves its loop
+// at its next reduction.
 #include <cstdlib>
 
 #include "vx_device.cuh"
@@ -26,7 +29,7 @@ namespace vx {
 namespace {
 
 constexpr int kPThreads = 512;
-constexpr int kFloatsPerRev = 30;  // 18 K + 6 D + 3 z + 3 p in shared memory
+constexpr int kFloatsPerRev = 30;  // 18 K + 6 D + (z, p_old) 6 in shared memory
 
 struct PersistArgs {
     uint32_t n;
@@ -40,87 +43,87 @@ struct PersistArgs {
     const double* src;         // right-hand side in FP64
     const double* scale_from;  // |src|; r0 = src / |src|
     float* x;                  // correction [3][n]
-    float* zg;                 // global z [3][n]
-    float* pg;                 // global p [3][n]
+    float4* zp4;               // published (z.x, z.y, z.z, p_old.x) [n]
+    float2* zp2;               // published (p_old.y, p_old.z) [n]
     double* part;              // [3][G] partials: p.Ap, r.z, r.r
-    unsigned* bar;             // [2] arrival count, generation
-    int32_t* err;              // barrier timeout flag
+    unsigned long long* count;  // arrivals at the grid reductions so far
+    int32_t* err;               // a wait ran out
     PcgScalars* sc;
     double tolerance;
     uint32_t max_iterations;
     unsigned long long spin_limit;
 };
 
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Block-wide sum of NV values, published as this block's partials, then the
+// grid-wide totals once all G blocks have arrived at reduction number `seq`
+// (the arrival counter only grows: reduction seq is complete at seq * G). One
+// warp sums the partials in block order, so every block obtains the same bits.
+// Returns false (in every thread) when a wait ran out here or in another block.
 template <int NV>
-__device__ __forceinline__ void reduce_block(double (&v)[NV], double (*sh)[32]) {
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[NV], const PersistArgs& a,
+                                           unsigned long long seq, double (*sh)[32], double* tot, int* s_ok,
+                                           double (&out)[NV]) {
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5, G = gridDim.x;
 #pragma unroll
     for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
     }
-    __syncthreads();
+    __syncthreads();  // also orders every thread's global stores before the release below
     if (warp == 0) {
+        double b[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) v[k] = warp_sum(lane < nw ? sh[k][lane] : 0.0);
-    }
-    __syncthreads();
-}
-
-// Sum of G partials in a fixed order; the result reaches every thread.
-template <int NV>
-__device__ __forceinline__ void grid_totals(const double* part, unsigned G, const int (&slot)[NV],
-                                            double (*sh)[32], double* tot, double (&out)[NV]) {
-    double v[NV];
+        for (int k = 0; k < NV; ++k) b[k] = warp_sum(lane < nw ? sh[k][lane] : 0.0);
+        int ok = 1;
+        if (lane == 0) {
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        v[k] = 0.0;
-        for (unsigned b = threadIdx.x; b < G; b += blockDim.x) v[k] += __ldcg(part + (size_t)slot[k] * G + b);
-    }
-    reduce_block<NV>(v, sh);
-    if (threadIdx.x == 0) {
+            for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
+            __threadfence();
+            red_release_add(a.count, 1ull);
+            const unsigned long long target = seq * G;
+            unsigned long long spins = 0;
+            while (ld_acquire(a.count) < target) {
+                if (++spins >= a.spin_limit || ((spins & 63) == 0 && *(volatile int32_t*)a.err)) {
+                    ok = 0;
+                    break;
+                }
+            }
+            if (!ok) atomicExch(a.err, 1);
+            else if (*(volatile int32_t*)a.err) ok = 0;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __threadfence();
+        double t[NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) tot[k] = v[k];
+        for (int k = 0; k < NV; ++k) t[k] = 0.0;
+        if (ok) {
+            for (unsigned blk = lane; blk < G; blk += 32) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) t[k] += __ldcg(a.part + (size_t)slot[k] * G + blk);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = warp_sum(t[k]);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) tot[k] = t[k];
+            *s_ok = ok;
+        }
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < NV; ++k) out[k] = tot[k];
-}
-
-// Generation barrier over all blocks of a cooperative launch with a bounded
-// wait. Returns false (in every thread of the block) once any block has timed
-// out, so the caller leaves its loop.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int32_t* err, unsigned long long spin_limit) {
-    __shared__ int32_t s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned* gen = bar + 1;
-        const unsigned g0 = *gen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u) + 1u;
-        int32_t ok = 1;
-        if (arrived == gridDim.x) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned long long spins = 0;
-            while (*gen == g0) {
-                if (++spins > spin_limit) {
-                    atomicExch(err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(40);
-            }
-        }
-        __threadfence();
-        if (*(volatile int32_t*)err) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
+    return *s_ok != 0;
 }
 
 struct F3 {
@@ -130,55 +133,35 @@ __device__ __forceinline__ F3 smul(const Sym<float>& s, F3 v) {
     return {s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
             s.xz * v.x + s.yz * v.y + s.zz * v.z};
 }
-// Inverse of a symmetric positive block by its adjugate, scaled by the largest
-// diagonal entry so the FP32 cofactors stay far from overflow.
-__device__ __forceinline__ Sym<float> sym_inverse(const Sym<float>& d) {
-    const float s = fmaxf(fmaxf(d.xx, d.yy), d.zz);
-    const float is = 1.0f / s;
-    const float xx = d.xx * is, yy = d.yy * is, zz = d.zz * is, xy = d.xy * is, xz = d.xz * is, yz = d.yz * is;
-    const float c00 = yy * zz - yz * yz, c01 = xz * yz - xy * zz, c02 = xy * yz - xz * yy;
-    const float c11 = xx * zz - xz * xz, c12 = xy * xz - xx * yz, c22 = xx * yy - xy * xy;
-    const float inv = is / (xx * c00 + xy * c01 + xz * c02);
-    return {c00 * inv, c11 * inv, c22 * inv, c01 * inv, c02 * inv, c12 * inv};
-}
-__device__ __forceinline__ Sym<float> ssym(const float* base, uint32_t cap, uint32_t li) {
-    return {base[li], base[cap + li], base[2 * cap + li], base[3 * cap + li], base[4 * cap + li], base[5 * cap + li]};
-}
-__device__ __forceinline__ F3 s3(const float* base, uint32_t cap, uint32_t li) {
-    return {base[li], base[cap + li], base[2 * cap + li]};
-}
-__device__ __forceinline__ void w3(float* base, uint32_t cap, uint32_t li, F3 v) {
-    base[li] = v.x;
-    base[cap + li] = v.y;
-    base[2 * cap + li] = v.z;
-}
+__device__ __forceinline__ Sym<float> sym_of(float4 a, float2 b) { return {a.x, a.y, a.z, a.w, b.x, b.y}; }
 
 template <int R>
 __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) {
-    extern __shared__ float smem[];
+    extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
     __shared__ double tot[3];
-    const uint32_t n = a.n, cap = a.cap, T = blockDim.x, G = gridDim.x;
-    float* sK = smem;             // [18][cap]: axis a component c at (6a + c) * cap
-    float* sD = sK + 18 * cap;    // [6][cap]
-    float* sz = sD + 6 * cap;     // [3][cap]
-    float* sp = sz + 3 * cap;     // [3][cap]
+    __shared__ int s_ok;
+    const uint32_t n = a.n, cap = a.cap, T = blockDim.x;
+    float4* sK4 = smem4;                                   // [3][cap] owned bonds (xx, yy, zz, xy)
+    float4* sD4 = sK4 + 3 * cap;                           // [cap]
+    float4* sZP4 = sD4 + cap;                              // [cap] (z, p_old.x)
+    float2* sK2 = reinterpret_cast<float2*>(sZP4 + cap);   // [3][cap] (xz, yz)
+    float2* sD2 = sK2 + 3 * cap;                           // [cap]
+    float2* sZP2 = sD2 + cap;                              // [cap] (p_old.y, p_old.z)
     const uint32_t lo = blockIdx.x * cap;
     const uint32_t cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
 
     // stiffness and diagonal of the range into shared memory
     for (uint32_t li = threadIdx.x; li < cnt; li += T) {
-        const uint32_t i = lo + li;
+        const size_t i = lo + li;
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-            Sym<float> k = load_sym(a.K + (size_t)ax * 6 * n, n, i);
-            float* b = sK + (size_t)6 * ax * cap;
-            b[li] = k.xx, b[cap + li] = k.yy, b[2 * cap + li] = k.zz;
-            b[3 * cap + li] = k.xy, b[4 * cap + li] = k.xz, b[5 * cap + li] = k.yz;
+            const float* kb = a.K + (size_t)ax * 6 * n;
+            sK4[ax * cap + li] = __ldg(reinterpret_cast<const float4*>(kb) + i);
+            sK2[ax * cap + li] = __ldg(reinterpret_cast<const float2*>(kb + 4 * (size_t)n) + i);
         }
-        Sym<float> d = load_sym(a.D, n, i);
-        sD[li] = d.xx, sD[cap + li] = d.yy, sD[2 * cap + li] = d.zz;
-        sD[3 * cap + li] = d.xy, sD[4 * cap + li] = d.xz, sD[5 * cap + li] = d.yz;
+        sD4[li] = __ldg(reinterpret_cast<const float4*>(a.D) + i);
+        sD2[li] = __ldg(reinterpret_cast<const float2*>(a.D + 4 * (size_t)n) + i);
     }
 
     float x[R][3], r[R][3], p[R][3], ap[R][3];
@@ -191,36 +174,30 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const uint32_t li = threadIdx.x + k * T;
-        x[k][0] = x[k][1] = x[k][2] = 0.f;
-        p[k][0] = p[k][1] = p[k][2] = 0.f;
-        ap[k][0] = ap[k][1] = ap[k][2] = 0.f;
-        r[k][0] = r[k][1] = r[k][2] = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = ap[k][c] = r[k][c] = 0.f;
         if (li < cnt) {
             const size_t i = lo + li;
             F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale), (float)(a.src[2 * (size_t)n + i] * scale)};
             F3 z = smul(load_sym(a.Dinv, n, i), rr);
             r[k][0] = rr.x, r[k][1] = rr.y, r[k][2] = rr.z;
-            w3(sz, cap, li, z);
-            w3(sp, cap, li, F3{0.f, 0.f, 0.f});
-            a.zg[i] = z.x, a.zg[n + i] = z.y, a.zg[2 * (size_t)n + i] = z.z;
-            a.pg[i] = 0.f, a.pg[n + i] = 0.f, a.pg[2 * (size_t)n + i] = 0.f;
+            const float4 q4 = make_float4(z.x, z.y, z.z, 0.f);
+            const float2 q2 = make_float2(0.f, 0.f);
+            sZP4[li] = q4, sZP2[li] = q2;
+            a.zp4[i] = q4, a.zp2[i] = q2;
             acc[0] += (double)rr.x * z.x + (double)rr.y * z.y + (double)rr.z * z.z;
             acc[1] += (double)rr.x * rr.x + (double)rr.y * rr.y + (double)rr.z * rr.z;
         }
     }
-    reduce_block<2>(acc, red);
-    if (threadIdx.x == 0) {
-        a.part[(size_t)1 * G + blockIdx.x] = acc[0];
-        a.part[(size_t)2 * G + blockIdx.x] = acc[1];
-    }
-    bool alive = grid_barrier(a.bar, a.err, a.spin_limit);
-    double t2[2] = {0.0, 0.0};
+    unsigned long long seq = 1;
     const int su[2] = {1, 2};
-    if (alive) grid_totals<2>(a.part, G, su, red, tot, t2);
+    const int sm[1] = {0};
+    double t2[2];
+    bool alive = grid_reduce<2>(acc, su, a, seq++, red, tot, &s_ok, t2);
     const double initial = sqrt(t2[1]);
     double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
     uint32_t its = 0;
-    int32_t status = VX_OK;
+    int32_t status = alive ? VX_OK : VX_TIMEOUT;
     bool done = !alive;
     if (alive) {
         if (!isfinite(t2[0]) || !isfinite(t2[1])) {
@@ -237,7 +214,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     while (!done) {
         const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
         // ---- matvec phase: p = z + beta p_old, Ap = D p - P sum K p_nbr ----
-        double pap = 0.0;
+        double pap[1] = {0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
@@ -250,9 +227,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 nb[3 + ax] = __ldg(a.rev + (size_t)ax * n + i);
             }
             const uint8_t fl = __ldg(a.flags + i);
-            F3 zi = s3(sz, cap, li), po = s3(sp, cap, li);
-            F3 pi = {fmaf(beta, po.x, zi.x), fmaf(beta, po.y, zi.y), fmaf(beta, po.z, zi.z)};
-            F3 y = smul(ssym(sD, cap, li), pi);
+            const float4 o4 = sZP4[li];
+            const float2 o2 = sZP2[li];
+            const F3 pi = {fmaf(beta, o4.w, o4.x), fmaf(beta, o2.x, o4.y), fmaf(beta, o2.y, o4.z)};
+            F3 y = smul(sym_of(sD4[li], sD2[li]), pi);
             F3 s = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
@@ -262,17 +240,24 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 const int ax = t < 3 ? t : t - 3;
                 const uint32_t lj = j - lo;
                 const bool inb = lj < cnt;
-                const uint32_t ls = inb ? lj : li;  // always a valid shared-memory slot
-                F3 zj = s3(sz, cap, ls), pj = s3(sp, cap, ls);
-                Sym<float> Kb = ssym(sK + (size_t)6 * ax * cap, cap, t < 3 ? li : ls);
-                if (!inb) {
-                    zj = {__ldcg(a.zg + j), __ldcg(a.zg + n + j), __ldcg(a.zg + 2 * (size_t)n + j)};
-                    pj = {__ldcg(a.pg + j), __ldcg(a.pg + n + j), __ldcg(a.pg + 2 * (size_t)n + j)};
-                    if (t >= 3) Kb = load_sym(a.K + (size_t)ax * 6 * n, n, j);
+                float4 q4;
+                float2 q2;
+                Sym<float> Kb;
+                if (inb) {
+                    q4 = sZP4[lj], q2 = sZP2[lj];
+                } else {
+                    q4 = __ldcg(a.zp4 + j), q2 = __ldcg(a.zp2 + j);
+                }
+                if (t < 3) {
+                    Kb = sym_of(sK4[ax * cap + li], sK2[ax * cap + li]);
+                } else if (inb) {
+                    Kb = sym_of(sK4[ax * cap + lj], sK2[ax * cap + lj]);
+                } else {
+                    Kb = load_sym(a.K + (size_t)ax * 6 * n, n, j);
                 }
                 const float m = ok ? 1.f : 0.f;
-                F3 pn = {m * fmaf(beta, pj.x, zj.x), m * fmaf(beta, pj.y, zj.y), m * fmaf(beta, pj.z, zj.z)};
-                F3 kv = smul(Kb, pn);
+                const F3 pn = {m * fmaf(beta, q4.w, q4.x), m * fmaf(beta, q2.x, q4.y), m * fmaf(beta, q2.y, q4.z)};
+                const F3 kv = smul(Kb, pn);
                 s.x += kv.x, s.y += kv.y, s.z += kv.z;
             }
             if (fl & 1) y.x -= s.x;
@@ -280,27 +265,13 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             if (fl & 4) y.z -= s.z;
             p[k][0] = pi.x, p[k][1] = pi.y, p[k][2] = pi.z;
             ap[k][0] = y.x, ap[k][1] = y.y, ap[k][2] = y.z;
-            pap += (double)pi.x * y.x + (double)pi.y * y.y + (double)pi.z * y.z;
+            pap[0] += (double)pi.x * y.x + (double)pi.y * y.y + (double)pi.z * y.z;
         }
-        double v1[1] = {pap};
-        reduce_block<1>(v1, red);
-        if (threadIdx.x == 0) a.part[blockIdx.x] = v1[0];
-        if (!grid_barrier(a.bar, a.err, a.spin_limit)) {
+        double t1[1];
+        if (!grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1)) {
             status = VX_TIMEOUT;
             break;
         }
-        // every block has read the old directions: publish the new ones
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
-            const size_t i = lo + li;
-            w3(sp, cap, li, F3{p[k][0], p[k][1], p[k][2]});
-            a.pg[i] = p[k][0], a.pg[n + i] = p[k][1], a.pg[2 * (size_t)n + i] = p[k][2];
-        }
-        double t1[1];
-        const int sm[1] = {0};
-        grid_totals<1>(a.part, G, sm, red, tot, t1);
         const double pap_all = t1[0];
         if (!isfinite(pap_all) || pap_all <= 1e-30) {
             its += 1;  // the matvec happened (src/solver.rs:1861-1866)
@@ -308,7 +279,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             break;
         }
         const float alpha = (float)(rz / pap_all);
-        // ---- update phase ----
+        // ---- update phase; every block has read the old (z, p_old): publish the new ----
         double au[2] = {0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -320,24 +291,20 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 x[k][c] = fmaf(alpha, p[k][c], x[k][c]);
                 r[k][c] = fmaf(-alpha, ap[k][c], r[k][c]);
             }
-            F3 rr = {r[k][0], r[k][1], r[k][2]};
-            F3 z = smul(sym_inverse(ssym(sD, cap, li)), rr);
-            w3(sz, cap, li, z);
-            a.zg[i] = z.x, a.zg[n + i] = z.y, a.zg[2 * (size_t)n + i] = z.z;
+            const F3 rr = {r[k][0], r[k][1], r[k][2]};
+            const F3 z = smul(load_sym(a.Dinv, n, i), rr);
+            const float4 q4 = make_float4(z.x, z.y, z.z, p[k][0]);
+            const float2 q2 = make_float2(p[k][1], p[k][2]);
+            sZP4[li] = q4, sZP2[li] = q2;
+            a.zp4[i] = q4, a.zp2[i] = q2;
             au[0] += (double)rr.x * z.x + (double)rr.y * z.y + (double)rr.z * z.z;
             au[1] += (double)rr.x * rr.x + (double)rr.y * rr.y + (double)rr.z * rr.z;
         }
-        reduce_block<2>(au, red);
-        if (threadIdx.x == 0) {
-            a.part[(size_t)1 * G + blockIdx.x] = au[0];
-            a.part[(size_t)2 * G + blockIdx.x] = au[1];
-        }
-        if (!grid_barrier(a.bar, a.err, a.spin_limit)) {
+        double tu[2];
+        if (!grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu)) {
             status = VX_TIMEOUT;
             break;
         }
-        double tu[2];
-        grid_totals<2>(a.part, G, su, red, tot, tu);
         its += 1;
         residual = sqrt(tu[1]) / initial;
         if (!isfinite(tu[0]) || !isfinite(tu[1])) {
@@ -421,15 +388,15 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     a.src = s->r64;
     a.scale_from = &s->sc->r64_norm;
     a.x = s->x32;
-    a.zg = s->z32;
-    a.pg = s->p32[0];
+    a.zp4 = reinterpret_cast<float4*>(s->zp32);
+    a.zp2 = reinterpret_cast<float2*>(s->zp32 + 4 * (size_t)s->n);
     a.part = s->partials;
-    a.bar = s->barrier;
+    a.count = reinterpret_cast<unsigned long long*>(s->barrier);
     a.err = reinterpret_cast<int32_t*>(s->barrier + 2);
     a.sc = s->sc32;
     a.tolerance = tolerance;
     a.max_iterations = max_iterations;
-    a.spin_limit = 20000000ull;  // ~1-2 s of waiting at one barrier
+    a.spin_limit = 4000000ull;  // ~1-2 s of polling at one reduction
     // VXCOROT_BARRIER_SPINS lowers the bound so a test can make the wait run out
     if (const char* v = std::getenv("VXCOROT_BARRIER_SPINS")) {
         unsigned long long lim = std::strtoull(v, nullptr, 10);
