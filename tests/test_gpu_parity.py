@@ -273,6 +273,23 @@ def test_persistent_inner_solve_matches_streaming_and_oracle(ctx, edge):
     assert rel(out[N.KERNEL_PERSISTENT], out[N.KERNEL_STREAMING]) < 2e-5
 
 
+@pytest.mark.parametrize("edge", [48, 64])
+def test_persistent_kernels_agree_at_full_grid(ctx, edge):
+    """All 148 blocks busy (R = 2 at 48^3, R = 4 at 64^3): both inner kernels
+    reach the FP64 target and agree over three passes."""
+    s = S.mixed_block(edge, seed=3)
+    out = {}
+    for kernel in (N.KERNEL_STREAMING, N.KERNEL_PERSISTENT):
+        d = N.DeviceScene(ctx, s)
+        for _ in range(3):
+            d.fit_rotations()
+            st = d.corotational_pass(1e-3, 1e-8, 20000, precision=N.PRECISION_MIXED, kernel=kernel)
+            assert st["converged"] == 1 and st["true_residual"] <= 1e-8, (kernel, st)
+        out[kernel] = d.positions() - s.position
+        d.close()
+    assert rel(out[N.KERNEL_PERSISTENT], out[N.KERNEL_STREAMING]) < 2e-5
+
+
 def test_persistent_solve_on_wood_cube_meets_fp64_target(ctx):
     s = S.wood_cube()
     d = N.DeviceScene(ctx, s)

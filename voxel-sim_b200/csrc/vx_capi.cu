@@ -84,6 +84,8 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->bond_count = A.take<uint32_t>(1);
     s->barrier = A.take<unsigned>(4);
     s->zp32 = A.take<float>(6 * m);
+    s->nbcode = A.take<uint32_t>(3 * m);
+    s->nbcode_bad = A.take<uint32_t>(1);
 }
 
 uint64_t scene_bytes(uint32_t n, uint32_t material_count) {

@@ -126,6 +126,8 @@ struct vx_scene {
     uint32_t* bond_count;         // bonds assembled by the last pass
     unsigned* barrier;            // [4] persistent kernel: u64 arrival count, error flag, pad
     float* zp32;                  // [6n] persistent kernel's published (z, p_old): float4[n] then float2[n]
+    uint32_t* nbcode;             // [3][n] neighbour deltas j - i as int16 pairs (0 = none): own x|y, own z|rev x, rev y|z
+    uint32_t* nbcode_bad;         // [1] neighbour entries a delta cannot encode
 
     // host mirrors
     double* h_stage = nullptr;       // pinned staging of host copies [4n doubles]
@@ -150,6 +152,7 @@ struct vx_scene {
     bool persist_ok = false;
     unsigned persist_G = 0, persist_cap = 0, persist_R = 0;
     size_t persist_smem = 0;
+    int nbcode_state = 0;         // 0 = not yet read back, 1 = all deltas encoded, 2 = some did not fit
     uint32_t active = 0;          // REVs with a free axis (cached per target set)
     bool active_cached = false;
     bool assembled = false;

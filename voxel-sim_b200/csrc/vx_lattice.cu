@@ -45,12 +45,44 @@ __global__ void k_reverse(uint32_t n, const uint32_t* __restrict__ nbr, uint32_t
     rev[a * n + j] = i;
 }
 
+// Neighbour deltas for the persistent kernel, which keeps them in shared
+// memory: entry t of REV i (own x, y, z, then reverse x, y, z) is j - i as an
+// int16, 0 for no neighbour, packed two per word. Entries that do not fit
+// (|j - i| > 32767, j == i or j >= n) are counted in *bad; the persistent
+// kernel is then not used for the scene.
+__global__ void k_neighbor_codes(uint32_t n, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ rev,
+                                 uint32_t* __restrict__ code, uint32_t* __restrict__ bad) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t d16[6];
+    uint32_t miss = 0;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+        const uint32_t j = t < 3 ? nbr[(size_t)t * n + i] : rev[(size_t)(t - 3) * n + i];
+        d16[t] = 0;
+        if (j == VX_EMPTY_U32) continue;
+        const long long d = (long long)j - (long long)i;
+        if (j >= n || d == 0 || d < -32768 || d > 32767) {
+            miss += 1;
+            continue;
+        }
+        d16[t] = (uint32_t)(uint16_t)(int16_t)d;
+    }
+#pragma unroll
+    for (int w = 0; w < 3; ++w) code[(size_t)w * n + i] = d16[2 * w] | (d16[2 * w + 1] << 16);
+    if (miss) atomicAdd(bad, miss);
+}
+
 cudaError_t launch_reverse_neighbors(vx_scene* s) {
     size_t m = 3 * (size_t)s->n;
+    s->persist_checked = false;  // the on-chip plan depends on the deltas
+    s->nbcode_state = 0;
     if (m == 0) return cudaSuccess;
     unsigned g = (unsigned)((m + 255) / 256);
     k_fill_u32<<<g, 256, 0, s->stream>>>(s->rev, m, VX_EMPTY_U32);
     k_reverse<<<g, 256, 0, s->stream>>>(s->n, s->nbr, s->rev);
+    cudaMemsetAsync(s->nbcode_bad, 0, sizeof(uint32_t), s->stream);
+    k_neighbor_codes<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->nbr, s->rev, s->nbcode, s->nbcode_bad);
     return cudaGetLastError();
 }
 

@@ -1,23 +1,27 @@
 // vx_persistent.cu — the FP32 inner PCG solve as one persistent kernel whose
 // working set stays on chip.
 //
-// When a scene is small enough (up to ~1,900 REVs per SM), one cooperative
+// When a scene is small enough (up to ~2,000 REVs per SM), one cooperative
 // block of 512 threads per SM owns a contiguous range of REVs for the whole
-// inner solve. Its REVs' bond stiffness (three owned bonds), projected
-// diagonal and the pair (z, p_old) live in shared memory as float4 + float2
-// records, so a neighbour costs two vector loads; x, r, p and Ap live in
-// registers of the owning thread. Neighbours outside the range are read from
-// the global copy of (z, p_old), which every block republishes once per
-// iteration. An iteration is the same recurrence as k_matvec/k_update in
-// vx_pcg.cu (src/solver.rs:1833-1911) with two grid-wide reductions:
+// inner solve. Shared memory holds, per REV of the range, the stiffness of its
+// three owned bonds, the pair (z, p_old) as float4 + float2 records, its six
+// neighbour deltas as int16 and its free-axis flags, so an in-range neighbour
+// costs two vector loads from shared memory and no index load. x, r, p and Ap
+// live in registers of the owning thread; the diagonal block and its inverse
+// are read from L2 (issued before the grid wait when registers allow).
+// Neighbours outside the range are read from the global copy of (z, p_old),
+// which every block republishes once per iteration. An iteration is the
+// recurrence of k_matvec/k_update in vx_pcg.cu (src/solver.rs:1833-1911) with
+// two grid-wide reductions:
 //   matvec phase  p = z + beta p_old, Ap, block partial of p.Ap   -> reduction A
 //   update phase  alpha, x, r, z = D^-1 r, partials of r.z, r.r   -> reduction B
-// A reduction is also the grid barrier: each block stores its partials and
-// adds one to an arrival counter; a block passes once the counter shows every
-// block's arrival, and sums the partials in block order, so all blocks take
-// the same alpha, beta and stop decisions. The waits are bounded; when a
-// bound is hit the kernel records VX_TIMEOUT and every block leaves its loop
-// at its next reduction.
+// A reduction is also the grid barrier: a block stores its partial, adds one
+// to an arrival counter with release semantics and polls the counter with
+// acquire loads until every block has arrived; then one warp sums the
+// partials in block order, so all blocks take the same alpha, beta and stop
+// decisions. The per-REV dot products are formed in FP32 and summed in FP64.
+// The waits are bounded; when a bound is hit the kernel records VX_TIMEOUT
+// and every block leaves its loop at its next reduction.
 #include <cstdlib>
 
 #include "vx_device.cuh"
@@ -29,7 +33,9 @@ namespace vx {
 namespace {
 
 constexpr int kPThreads = 512;
-constexpr int kFloatsPerRev = 30;  // 18 K + 6 D + (z, p_old) 6 in shared memory
+// shared memory per REV: K float4[3] + float2[3], (z, p_old) float4 + float2,
+// three delta words and one flag byte
+constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 1;
 
 struct PersistArgs {
     uint32_t n;
@@ -38,14 +44,13 @@ struct PersistArgs {
     const float* D;
     const float* K;
     const float* Dinv;
-    const uint32_t* nbr;
-    const uint32_t* rev;
-    const double* src;         // right-hand side in FP64
-    const double* scale_from;  // |src|; r0 = src / |src|
-    float* x;                  // correction [3][n]
-    float4* zp4;               // published (z.x, z.y, z.z, p_old.x) [n]
-    float2* zp2;               // published (p_old.y, p_old.z) [n]
-    double* part;              // [3][G] partials: p.Ap, r.z, r.r
+    const uint32_t* code;       // [3][n] neighbour deltas
+    const double* src;          // right-hand side in FP64
+    const double* scale_from;   // |src|; r0 = src / |src|
+    float* x;                   // correction [3][n]
+    float4* zp4;                // published (z.x, z.y, z.z, p_old.x) [n]
+    float2* zp2;                // published (p_old.y, p_old.z) [n]
+    double* part;               // [3][G] partials: p.Ap, r.z, r.r
     unsigned long long* count;  // arrivals at the grid reductions so far
     int32_t* err;               // a wait ran out
     PcgScalars* sc;
@@ -65,9 +70,12 @@ __device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned 
 
 // Block-wide sum of NV values, published as this block's partials, then the
 // grid-wide totals once all G blocks have arrived at reduction number `seq`
-// (the arrival counter only grows: reduction seq is complete at seq * G). One
-// warp sums the partials in block order, so every block obtains the same bits.
-// Returns false (in every thread) when a wait ran out here or in another block.
+// (the arrival counter only grows: reduction seq is complete at seq * G).
+// The __syncthreads before the release makes every thread's earlier global
+// stores part of what the release publishes; the acquire by lane 0, then
+// __syncwarp and the final __syncthreads, order every thread's later loads
+// after the other blocks' released stores. Returns false (in every thread)
+// when a wait ran out here or in another block.
 template <int NV>
 __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[NV], const PersistArgs& a,
                                            unsigned long long seq, double (*sh)[32], double* tot, int* s_ok,
@@ -79,7 +87,7 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
 #pragma unroll
         for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
     }
-    __syncthreads();  // also orders every thread's global stores before the release below
+    __syncthreads();
     if (warp == 0) {
         double b[NV];
 #pragma unroll
@@ -88,7 +96,6 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
         if (lane == 0) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
-            __threadfence();
             red_release_add(a.count, 1ull);
             const unsigned long long target = seq * G;
             unsigned long long spins = 0;
@@ -102,7 +109,7 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
             else if (*(volatile int32_t*)a.err) ok = 0;
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
-        __threadfence();
+        __syncwarp();
         double t[NV];
 #pragma unroll
         for (int k = 0; k < NV; ++k) t[k] = 0.0;
@@ -134,24 +141,28 @@ __device__ __forceinline__ F3 smul(const Sym<float>& s, F3 v) {
             s.xz * v.x + s.yz * v.y + s.zz * v.z};
 }
 __device__ __forceinline__ Sym<float> sym_of(float4 a, float2 b) { return {a.x, a.y, a.z, a.w, b.x, b.y}; }
+__device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+// R REVs per thread. With R <= 2 the diagonal block and its inverse are loaded
+// into registers before each grid wait, so their L2 latency overlaps the wait;
+// at R = 4 the registers are not there and they are loaded where used.
 template <int R>
 __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) {
+    constexpr bool kPrefetch = R <= 2;
     extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
     __shared__ double tot[3];
     __shared__ int s_ok;
     const uint32_t n = a.n, cap = a.cap, T = blockDim.x;
-    float4* sK4 = smem4;                                   // [3][cap] owned bonds (xx, yy, zz, xy)
-    float4* sD4 = sK4 + 3 * cap;                           // [cap]
-    float4* sZP4 = sD4 + cap;                              // [cap] (z, p_old.x)
-    float2* sK2 = reinterpret_cast<float2*>(sZP4 + cap);   // [3][cap] (xz, yz)
-    float2* sD2 = sK2 + 3 * cap;                           // [cap]
-    float2* sZP2 = sD2 + cap;                              // [cap] (p_old.y, p_old.z)
+    float4* sK4 = smem4;                                       // [3][cap] owned bonds (xx, yy, zz, xy)
+    float4* sZP4 = sK4 + 3 * cap;                              // [cap] (z, p_old.x)
+    float2* sK2 = reinterpret_cast<float2*>(sZP4 + cap);       // [3][cap] (xz, yz)
+    float2* sZP2 = sK2 + 3 * cap;                              // [cap] (p_old.y, p_old.z)
+    uint32_t* sNB = reinterpret_cast<uint32_t*>(sZP2 + cap);   // [3][cap] neighbour deltas
+    uint8_t* sFL = reinterpret_cast<uint8_t*>(sNB + 3 * cap);  // [cap] free-axis flags
     const uint32_t lo = blockIdx.x * cap;
     const uint32_t cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
 
-    // stiffness and diagonal of the range into shared memory
     for (uint32_t li = threadIdx.x; li < cnt; li += T) {
         const size_t i = lo + li;
 #pragma unroll
@@ -159,12 +170,13 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             const float* kb = a.K + (size_t)ax * 6 * n;
             sK4[ax * cap + li] = __ldg(reinterpret_cast<const float4*>(kb) + i);
             sK2[ax * cap + li] = __ldg(reinterpret_cast<const float2*>(kb + 4 * (size_t)n) + i);
+            sNB[ax * cap + li] = __ldg(a.code + (size_t)ax * n + i);
         }
-        sD4[li] = __ldg(reinterpret_cast<const float4*>(a.D) + i);
-        sD2[li] = __ldg(reinterpret_cast<const float2*>(a.D + 4 * (size_t)n) + i);
+        sFL[li] = __ldg(a.flags + i);
     }
 
     float x[R][3], r[R][3], p[R][3], ap[R][3];
+    Sym<float> dreg[kPrefetch ? R : 1], ireg[kPrefetch ? R : 1];
     double scale = 1.0;
     {
         double rn = *a.scale_from;
@@ -178,15 +190,17 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
         for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = ap[k][c] = r[k][c] = 0.f;
         if (li < cnt) {
             const size_t i = lo + li;
-            F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale), (float)(a.src[2 * (size_t)n + i] * scale)};
-            F3 z = smul(load_sym(a.Dinv, n, i), rr);
+            const F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale),
+                           (float)(a.src[2 * (size_t)n + i] * scale)};
+            const F3 z = smul(load_sym(a.Dinv, n, i), rr);
             r[k][0] = rr.x, r[k][1] = rr.y, r[k][2] = rr.z;
             const float4 q4 = make_float4(z.x, z.y, z.z, 0.f);
             const float2 q2 = make_float2(0.f, 0.f);
             sZP4[li] = q4, sZP2[li] = q2;
             a.zp4[i] = q4, a.zp2[i] = q2;
-            acc[0] += (double)rr.x * z.x + (double)rr.y * z.y + (double)rr.z * z.z;
-            acc[1] += (double)rr.x * rr.x + (double)rr.y * rr.y + (double)rr.z * rr.z;
+            acc[0] += (double)dot3(rr, z);
+            acc[1] += (double)dot3(rr, rr);
+            if constexpr (kPrefetch) dreg[k] = load_sym(a.D, n, i);
         }
     }
     unsigned long long seq = 1;
@@ -220,23 +234,26 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             const uint32_t li = threadIdx.x + k * T;
             if (li >= cnt) continue;
             const uint32_t i = lo + li;
-            uint32_t nb[6];
+            int32_t dl[6];
 #pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-                nb[ax] = __ldg(a.nbr + (size_t)ax * n + i);
-                nb[3 + ax] = __ldg(a.rev + (size_t)ax * n + i);
+            for (int w = 0; w < 3; ++w) {
+                const uint32_t c = sNB[w * cap + li];
+                dl[2 * w] = (int32_t)(int16_t)(c & 0xffffu);
+                dl[2 * w + 1] = (int32_t)(int16_t)(c >> 16);
             }
-            const uint8_t fl = __ldg(a.flags + i);
+            const uint8_t fl = sFL[li];
             const float4 o4 = sZP4[li];
             const float2 o2 = sZP2[li];
             const F3 pi = {fmaf(beta, o4.w, o4.x), fmaf(beta, o2.x, o4.y), fmaf(beta, o2.y, o4.z)};
-            F3 y = smul(sym_of(sD4[li], sD2[li]), pi);
+            Sym<float> Dm;
+            if constexpr (kPrefetch) Dm = dreg[k];
+            else Dm = load_sym(a.D, n, i);
+            F3 y = smul(Dm, pi);
             F3 s = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
-                const uint32_t jraw = nb[t];
-                const bool ok = jraw != VX_EMPTY_U32;
-                const uint32_t j = ok ? jraw : i;
+                const bool ok = dl[t] != 0;
+                const uint32_t j = (uint32_t)((int32_t)i + dl[t]);
                 const int ax = t < 3 ? t : t - 3;
                 const uint32_t lj = j - lo;
                 const bool inb = lj < cnt;
@@ -265,7 +282,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             if (fl & 4) y.z -= s.z;
             p[k][0] = pi.x, p[k][1] = pi.y, p[k][2] = pi.z;
             ap[k][0] = y.x, ap[k][1] = y.y, ap[k][2] = y.z;
-            pap[0] += (double)pi.x * y.x + (double)pi.y * y.y + (double)pi.z * y.z;
+            pap[0] += (double)dot3(pi, y);
+        }
+        if constexpr (kPrefetch) {
+#pragma unroll
+            for (int k = 0; k < R; ++k) {  // in flight during the wait below
+                const uint32_t li = threadIdx.x + k * T;
+                if (li < cnt) ireg[k] = load_sym(a.Dinv, n, lo + li);
+            }
         }
         double t1[1];
         if (!grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1)) {
@@ -292,13 +316,17 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 r[k][c] = fmaf(-alpha, ap[k][c], r[k][c]);
             }
             const F3 rr = {r[k][0], r[k][1], r[k][2]};
-            const F3 z = smul(load_sym(a.Dinv, n, i), rr);
+            Sym<float> Di;
+            if constexpr (kPrefetch) Di = ireg[k];
+            else Di = load_sym(a.Dinv, n, i);
+            const F3 z = smul(Di, rr);
             const float4 q4 = make_float4(z.x, z.y, z.z, p[k][0]);
             const float2 q2 = make_float2(p[k][1], p[k][2]);
             sZP4[li] = q4, sZP2[li] = q2;
             a.zp4[i] = q4, a.zp2[i] = q2;
-            au[0] += (double)rr.x * z.x + (double)rr.y * z.y + (double)rr.z * z.z;
-            au[1] += (double)rr.x * rr.x + (double)rr.y * rr.y + (double)rr.z * rr.z;
+            au[0] += (double)dot3(rr, z);
+            au[1] += (double)dot3(rr, rr);
+            if constexpr (kPrefetch) dreg[k] = load_sym(a.D, n, i);  // in flight during the wait below
         }
         double tu[2];
         if (!grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu)) {
@@ -354,6 +382,14 @@ bool persistent_plan(vx_scene* s) {
     s->persist_checked = true;
     s->persist_ok = false;
     if (s->n == 0) return false;
+    if (s->nbcode_state == 0) {  // once per topology: did every neighbour delta fit?
+        uint32_t bad = 0;
+        if (cudaMemcpyAsync(&bad, s->nbcode_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            return false;
+        s->nbcode_state = bad == 0 ? 1 : 2;
+    }
+    if (s->nbcode_state != 1) return false;
     int dev = s->device, max_smem = 0, coop = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -364,7 +400,7 @@ bool persistent_plan(vx_scene* s) {
     if (G == 0) G = 1;
     unsigned cap = (s->n + G - 1) / G;
     unsigned R = (cap + kPThreads - 1) / kPThreads;
-    size_t smem = (size_t)kFloatsPerRev * cap * sizeof(float);
+    size_t smem = ((size_t)kBytesPerRev * cap + 15) & ~size_t(15);
     if (R > 4 || smem + 4096 > (size_t)max_smem) return false;
     s->persist_G = G;
     s->persist_cap = cap;
@@ -383,8 +419,7 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     a.D = s->d32;
     a.K = s->bonds.k32;
     a.Dinv = s->dinv32;
-    a.nbr = s->nbr;
-    a.rev = s->rev;
+    a.code = s->nbcode;
     a.src = s->r64;
     a.scale_from = &s->sc->r64_norm;
     a.x = s->x32;
