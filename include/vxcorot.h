@@ -267,6 +267,55 @@ int32_t vx_bond_stress(vx_scene* scene, float* ratio, float* force, uint32_t* ne
                        uint32_t cap, uint32_t* near_count);
 
 /*
+ * ---- the fixed step on the device ----
+ *
+ * One call of solver::step_with_axis_targets_and_loads (src/solver.rs:438-700)
+ * restricted to the elastic path, for every substep:
+ *   - the explicit prediction (:495-517): free REVs gain gravity * h of
+ *     velocity, targeted axes get zero velocity, x += v h, then targeted axes
+ *     are set to their targets; the result is the predicted position;
+ *   - the rotation fit, then up to corotation_iterations passes (assembly,
+ *     solve, x += dx), re-fitting between passes and stopping early when the
+ *     largest angle change is <= corotation_tolerance and the pass residual is
+ *     <= pass.tolerance (:546-570);
+ *   - the velocity update (:667-681): targeted axes (x - previous) / h, free
+ *     axes drift + (x - predicted) / h.
+ * Kinematic REVs do not move. The targets, loads (applied_loads: persistent
+ * force + acceleration * mass + per-step loads) and masses are the scene's
+ * current ones. Tools, contacts, thermal transport and the fracture commit are
+ * outside this path. pass.h is ignored (h = fixed_dt / substeps).
+ */
+typedef struct vx_step_params {
+    double fixed_dt;                 /* s (SceneConfig::fixed_dt) */
+    uint32_t substeps;               /* >= 1 */
+    uint32_t corotation_iterations;  /* passes per substep, >= 1 */
+    double corotation_tolerance;     /* rad */
+    double gravity[3];               /* m/s^2 */
+    vx_pass_params pass;             /* solve of every pass; reuse_preconditioner applies from
+                                        the second pass of a substep on, as the reference's CPU path */
+} vx_step_params;
+
+typedef struct vx_step_stats {
+    uint32_t passes;                 /* passes run, all substeps */
+    uint32_t pcg_iterations;         /* PCG (inner) iterations, all passes */
+    double residual;                 /* residual of the last pass (Scene::solver_residual) */
+    double max_angle;                /* largest angle change of the last fit, rad */
+    int32_t converged;               /* every pass reached its tolerance */
+} vx_step_stats;
+
+int32_t vx_scene_step(vx_scene* scene, const vx_step_params* params, vx_step_stats* out);
+/* Velocities, m/s, AoS n x 3 like positions. */
+int32_t vx_scene_set_velocities(vx_scene* scene, const double* xyz);
+int32_t vx_scene_get_velocities(vx_scene* scene, double* xyz);
+/*
+ * Sets (op 0) or adds to (op 1) the velocity of count REVs: index[count],
+ * value[3 * count]. Axes that are currently targeted keep zero velocity, as
+ * set_velocity and apply_impulse do (src/solver.rs:207-255).
+ */
+int32_t vx_scene_update_velocities(vx_scene* scene, uint32_t count, const uint32_t* index,
+                                   const double* value, int32_t op);
+
+/*
  * ---- scene pool: many scenes resident in one arena, solved together ----
  *
  * Batched and served forms (no counterpart in the reference, which steps one

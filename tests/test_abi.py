@@ -38,15 +38,17 @@ def test_struct_layouts_match_header(tmp_path):
 #include <stddef.h>
 #include "{ROOT}/include/vxcorot.h"
 int main(void) {{
-  printf("%zu %zu %zu %zu %zu\\n", sizeof(vx_material), sizeof(vx_scene_desc), sizeof(vx_pass_params),
-         sizeof(vx_pass_stats), offsetof(vx_scene_desc, neighbor));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(vx_material), sizeof(vx_scene_desc), sizeof(vx_pass_params),
+         sizeof(vx_pass_stats), offsetof(vx_scene_desc, neighbor), sizeof(vx_step_params),
+         offsetof(vx_step_params, pass), sizeof(vx_step_stats));
   return 0;
 }}''')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(N.VxMaterial), C.sizeof(N.VxSceneDesc), C.sizeof(N.VxPassParams), C.sizeof(N.VxPassStats),
-            N.VxSceneDesc.neighbor.offset]
+            N.VxSceneDesc.neighbor.offset, C.sizeof(N.VxStepParams), N.VxStepParams.pass_.offset,
+            C.sizeof(N.VxStepStats)]
     assert got == want
 
 
@@ -73,3 +75,5 @@ def test_null_handles_are_rejected(lib):
     assert lib.vx_corotational_pass(None, None, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_set_positions(None, None) == N.VX_BAD_INPUT
     assert lib.vx_ctx_create(0, None) == N.VX_BAD_INPUT
+    assert lib.vx_scene_step(None, None, None) == N.VX_BAD_INPUT
+    assert lib.vx_scene_update_velocities(None, 0, None, None, 0) == N.VX_BAD_INPUT

@@ -71,6 +71,9 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->p32[0] = A.take<float>(3 * m);
     s->p32[1] = A.take<float>(3 * m);
     s->ap32 = A.take<float>(3 * m);
+    s->vel = A.take<double>(3 * m);
+    s->prev = A.take<double>(3 * m);
+    s->drift = A.take<double>(3 * m);
     s->save_pos = A.take<double>(3 * m);
     s->save_rot = A.take<double4>(m);
     s->out_ratio = A.take<float>(3 * m);
@@ -454,6 +457,61 @@ int32_t vx_scene_set_targets(vx_scene* s, const uint8_t* mask, const double* xyz
     VX_TRY(launch_flags(s), "flags");
     VX_TRY(cudaStreamSynchronize(s->stream), "upload");
     s->active_cached = false;
+    return VX_OK;
+}
+int32_t vx_scene_set_velocities(vx_scene* s, const double* xyz) {
+    VX_CHECK_SCENE(s, xyz);
+    for (size_t t = 0; t < 3 * (size_t)s->n; ++t)
+        if (!std::isfinite(xyz[t])) {
+            set_error("vx_scene_set_velocities: non-finite value at %zu", t);
+            return VX_NONFINITE;
+        }
+    return upload_vec3(s, s->vel, xyz);
+}
+int32_t vx_scene_get_velocities(vx_scene* s, double* xyz) {
+    VX_CHECK_SCENE(s, xyz);
+    return download_vec3(s, xyz, s->vel);
+}
+int32_t vx_scene_update_velocities(vx_scene* s, uint32_t count, const uint32_t* index, const double* value,
+                                   int32_t op) {
+    clear_error();
+    if (!s || (count && (!index || !value)) || (op != 0 && op != 1)) {
+        set_error("vx_scene_update_velocities: bad argument");
+        return VX_BAD_INPUT;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        if (index[k] >= s->n) {
+            set_error("vx_scene_update_velocities: index %u out of range", index[k]);
+            return VX_BAD_INPUT;
+        }
+        for (int a = 0; a < 3; ++a)
+            if (!std::isfinite(value[3 * (size_t)k + a])) {
+                set_error("vx_scene_update_velocities: non-finite value for REV %u", index[k]);
+                return VX_NONFINITE;
+            }
+    }
+    if (count == 0) return VX_OK;
+    cudaSetDevice(s->device);
+    // values and indices travel through the pinned stage (3 + 1 doubles per
+    // entry, at most n entries at a time) into the FP64 z and p vectors, which
+    // are free between passes
+    for (uint32_t base = 0; base < count;) {
+        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, (size_t)s->n);
+        VX_TRY(cudaStreamSynchronize(s->stream), "velocity update");
+        double* vals = s->h_stage;
+        uint32_t* idx = reinterpret_cast<uint32_t*>(s->h_stage + 3 * (size_t)chunk);
+        std::memcpy(vals, value + 3 * (size_t)base, 3 * (size_t)chunk * sizeof(double));
+        std::memcpy(idx, index + base, (size_t)chunk * sizeof(uint32_t));
+        double* d_vals = s->z64;
+        uint32_t* d_idx = reinterpret_cast<uint32_t*>(s->p64[0]);
+        VX_TRY(cudaMemcpyAsync(d_vals, vals, 3 * (size_t)chunk * sizeof(double), cudaMemcpyHostToDevice, s->stream),
+               "velocity update");
+        VX_TRY(cudaMemcpyAsync(d_idx, idx, (size_t)chunk * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream),
+               "velocity update");
+        VX_TRY(launch_velocity_update(s, chunk, d_idx, d_vals, op), "velocity update");
+        base += chunk;
+    }
+    VX_TRY(cudaStreamSynchronize(s->stream), "velocity update");
     return VX_OK;
 }
 int32_t vx_scene_set_loads(vx_scene* s, const double* xyz) {

@@ -113,6 +113,9 @@ struct vx_scene {
     float* z32;
     float* p32[2];
     float* ap32;
+    double* vel;                  // [3][n] velocity, m/s (Voxel::velocity)
+    double* prev;                 // [3][n] positions at the start of the substep (Scene::previous)
+    double* drift;                // [3][n] predicted velocity of the substep (drift_velocity)
     double* save_pos;             // [3][n] checkpoint
     double4* save_rot;            // [n]
     float* out_ratio;             // [3n] bond stress outputs

@@ -66,6 +66,27 @@ class VxPassStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class VxStepParams(C.Structure):
+    _fields_ = [("fixed_dt", C.c_double), ("substeps", C.c_uint32), ("corotation_iterations", C.c_uint32),
+                ("corotation_tolerance", C.c_double), ("gravity", C.c_double * 3), ("pass_", VxPassParams)]
+
+
+class VxStepStats(C.Structure):
+    _fields_ = [("passes", C.c_uint32), ("pcg_iterations", C.c_uint32), ("residual", C.c_double),
+                ("max_angle", C.c_double), ("converged", C.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def step_params(fixed_dt, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5, gravity=(0.0, 0.0, 0.0),
+                tolerance=1e-5, max_iterations=10000, precision=PRECISION_FP64, reuse=False, inner_tolerance=0.0,
+                max_outer=0, kernel=KERNEL_AUTO) -> VxStepParams:
+    return VxStepParams(fixed_dt, substeps, corotation_iterations, corotation_tolerance, (C.c_double * 3)(*gravity),
+                        VxPassParams(fixed_dt / substeps, tolerance, max_iterations, precision, int(reuse),
+                                     inner_tolerance, max_outer, kernel))
+
+
 _lib = None
 
 
@@ -109,6 +130,10 @@ def load(path: Path | None = None):
     L.vx_scene_stream.restype = C.c_void_p
     L.vx_scene_stream.argtypes = [C.c_void_p]
     L.vx_scene_kernel_times.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_uint64, f64p]
+    L.vx_scene_step.argtypes = [C.c_void_p, C.POINTER(VxStepParams), C.POINTER(VxStepStats)]
+    L.vx_scene_set_velocities.argtypes = [C.c_void_p, f64p]
+    L.vx_scene_get_velocities.argtypes = [C.c_void_p, f64p]
+    L.vx_scene_update_velocities.argtypes = [C.c_void_p, C.c_uint32, u32p, f64p, C.c_int32]
     for name in header_symbols():
         getattr(L, name)  # every declared entry point is exported
     _lib = L
@@ -289,6 +314,28 @@ class DeviceScene:
         d = st.as_dict()
         d["status"] = status
         return d
+
+    def step(self, params: VxStepParams, allow=(VX_NOT_CONVERGED,)):
+        st = VxStepStats()
+        status = check(load().vx_scene_step(self.h, C.byref(params), C.byref(st)), allow=allow)
+        d = st.as_dict()
+        d["status"] = status
+        return d
+
+    def set_velocities(self, v):
+        v = self._vec(v)
+        check(load().vx_scene_set_velocities(self.h, _p(v, C.c_double)))
+
+    def velocities(self) -> np.ndarray:
+        out = np.zeros(3 * self.n, np.float64)
+        check(load().vx_scene_get_velocities(self.h, _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def update_velocities(self, index, values, add=False):
+        idx = np.ascontiguousarray(index, np.uint32).reshape(-1)
+        val = np.ascontiguousarray(values, np.float64).reshape(-1)
+        check(load().vx_scene_update_velocities(self.h, len(idx), _p(idx, C.c_uint32), _p(val, C.c_double),
+                                                1 if add else 0))
 
     def bond_stress(self, with_force=True, with_ratio=True, cap=None):
         m = 3 * self.n
