@@ -314,6 +314,16 @@ int32_t vx_scene_get_velocities(vx_scene* scene, double* xyz);
  */
 int32_t vx_scene_update_velocities(vx_scene* scene, uint32_t count, const uint32_t* index,
                                    const double* value, int32_t op);
+/*
+ * Indexed access to one per-REV vector field (VX_FIELD_POSITION or
+ * VX_FIELD_VELOCITY) of count REVs: index[count], xyz[3 * count]. Writes
+ * store the given values on every axis, with no target handling; they serve
+ * host calls that change a few REVs (fix_voxel_axes, apply_impulse).
+ */
+enum { VX_FIELD_POSITION = 0, VX_FIELD_VELOCITY = 1 };
+int32_t vx_scene_read_revs(vx_scene* scene, int32_t field, uint32_t count, const uint32_t* index, double* xyz);
+int32_t vx_scene_write_revs(vx_scene* scene, int32_t field, uint32_t count, const uint32_t* index,
+                            const double* xyz);
 
 /*
  * ---- scene pool: many scenes resident in one arena, solved together ----

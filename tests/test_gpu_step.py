@@ -94,3 +94,39 @@ def test_velocity_set_and_impulse_keep_targeted_axes_at_zero(ctx):
     with pytest.raises(N.VxError):
         d.update_velocities([s.n], [[0.0, 0.0, 0.0]])
     d.close()
+
+
+@pytest.mark.parametrize("edge", [1, 3])
+def test_odd_rev_counts(ctx, edge):
+    """Scenes with an odd REV count (1 and 27): the FP32 stiffness arrays keep
+    every axis on a 16-byte boundary, and passes and steps match the oracle."""
+    s = S.wood_cube(edge) if edge > 1 else S.from_cells(np.zeros((1, 3), np.int32), 1, S.M.table(),
+                                                          anisotropy=1.0)
+    assert s.n % 2 == 1
+    if edge == 1:
+        h, m = 0.01, float(s.mass[0])
+        s.loads[:] = [[3.0 * m, 2.0 * m, 0.0]]
+        d = N.DeviceScene(ctx, s)
+        p = N.step_params(h, substeps=1, corotation_iterations=1, tolerance=1e-5, max_iterations=1)
+        st = d.step(p)
+        assert st["status"] == N.VX_OK
+        assert np.allclose(d.velocities()[0], [0.03, 0.02, 0.0], rtol=0, atol=1e-12)
+        d.close()
+        return
+    top = s.target_mask == 7
+    s.position[top] = s.target[top]  # targeted REVs on their targets, as after a prediction
+    o = O.OracleScene(s)
+    o.fit_rotations()
+    o.assemble(1e-3, predicted=s.position)
+    o.factor_block_jacobi()
+    ref, _, _ = o.pcg(20000, 1e-14)
+    for precision, kernel in ((N.PRECISION_FP64, N.KERNEL_AUTO), (N.PRECISION_MIXED, N.KERNEL_STREAMING),
+                              (N.PRECISION_MIXED, N.KERNEL_PERSISTENT)):
+        d = N.DeviceScene(ctx, s)
+        d.fit_rotations()
+        d.set_predicted(s.position)
+        st = d.corotational_pass(1e-3, 1e-12 if precision == N.PRECISION_FP64 else 1e-8, 20000,
+                                 precision=precision, kernel=kernel)
+        assert st["converged"] == 1, (precision, kernel, st)
+        assert rel(d.positions() - s.position, ref.reshape(-1, 3)) < (1e-9 if precision == N.PRECISION_FP64 else 1e-6)
+        d.close()

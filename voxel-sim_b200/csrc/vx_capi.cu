@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "vx_kernels.h"
+#include "vx_layout.cuh"
 
 namespace vx {
 
@@ -49,7 +50,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->bond_a = A.take<float4>(3 * m);
     s->bond_b = A.take<float4>(3 * m);
     s->bonds.k64 = A.take<double>(18 * m);
-    s->bonds.k32 = A.take<float>(18 * m);
+    s->bonds.k32 = A.take<float>(18 * (size_t)kstride32((uint32_t)m));
     s->bonds.mat_k = A.take<double>(18 * m);
     s->bonds.frame_q = A.take<double4>(3 * m);
     s->bonds.force = A.take<double>(9 * m);
@@ -513,6 +514,63 @@ int32_t vx_scene_update_velocities(vx_scene* s, uint32_t count, const uint32_t* 
     }
     VX_TRY(cudaStreamSynchronize(s->stream), "velocity update");
     return VX_OK;
+}
+// Indexed reads and writes of a per-REV vector field, staged in chunks of at
+// most n entries through the pinned stage and the FP64 z / p solver vectors
+// (free between passes).
+static int32_t indexed_field(vx_scene* s, int32_t field, uint32_t count, const uint32_t* index, double* xyz,
+                             bool write, const char* who) {
+    clear_error();
+    if (!s || (count && (!index || !xyz)) || (field != VX_FIELD_POSITION && field != VX_FIELD_VELOCITY)) {
+        set_error("%s: bad argument", who);
+        return VX_BAD_INPUT;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        if (index[k] >= s->n) {
+            set_error("%s: index %u out of range", who, index[k]);
+            return VX_BAD_INPUT;
+        }
+        if (write)
+            for (int a = 0; a < 3; ++a)
+                if (!std::isfinite(xyz[3 * (size_t)k + a])) {
+                    set_error("%s: non-finite value for REV %u", who, index[k]);
+                    return VX_NONFINITE;
+                }
+    }
+    if (count == 0) return VX_OK;
+    cudaSetDevice(s->device);
+    double* dev_field = field == VX_FIELD_POSITION ? s->pos : s->vel;
+    for (uint32_t base = 0; base < count;) {
+        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, (size_t)s->n);
+        VX_TRY(cudaStreamSynchronize(s->stream), who);
+        double* vals = s->h_stage;
+        uint32_t* idx = reinterpret_cast<uint32_t*>(s->h_stage + 3 * (size_t)chunk);
+        std::memcpy(idx, index + base, (size_t)chunk * sizeof(uint32_t));
+        double* d_vals = s->z64;
+        uint32_t* d_idx = reinterpret_cast<uint32_t*>(s->p64[0]);
+        VX_TRY(cudaMemcpyAsync(d_idx, idx, (size_t)chunk * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream), who);
+        if (write) {
+            std::memcpy(vals, xyz + 3 * (size_t)base, 3 * (size_t)chunk * sizeof(double));
+            VX_TRY(cudaMemcpyAsync(d_vals, vals, 3 * (size_t)chunk * sizeof(double), cudaMemcpyHostToDevice,
+                                   s->stream), who);
+            VX_TRY(launch_scatter3(s, chunk, d_idx, d_vals, dev_field), who);
+        } else {
+            VX_TRY(launch_gather3(s, chunk, d_idx, dev_field, d_vals), who);
+            VX_TRY(cudaMemcpyAsync(vals, d_vals, 3 * (size_t)chunk * sizeof(double), cudaMemcpyDeviceToHost,
+                                   s->stream), who);
+            VX_TRY(cudaStreamSynchronize(s->stream), who);
+            std::memcpy(xyz + 3 * (size_t)base, vals, 3 * (size_t)chunk * sizeof(double));
+        }
+        base += chunk;
+    }
+    VX_TRY(cudaStreamSynchronize(s->stream), who);
+    return VX_OK;
+}
+int32_t vx_scene_read_revs(vx_scene* s, int32_t field, uint32_t count, const uint32_t* index, double* xyz) {
+    return indexed_field(s, field, count, index, xyz, false, "vx_scene_read_revs");
+}
+int32_t vx_scene_write_revs(vx_scene* s, int32_t field, uint32_t count, const uint32_t* index, const double* xyz) {
+    return indexed_field(s, field, count, index, const_cast<double*>(xyz), true, "vx_scene_write_revs");
 }
 int32_t vx_scene_set_loads(vx_scene* s, const double* xyz) {
     VX_CHECK_SCENE(s, xyz);

@@ -140,7 +140,8 @@ __global__ void k_assemble_bonds(SceneView s, BondArrays b, uint32_t* __restrict
     unsigned ballot = __ballot_sync(__activemask(), st == 2);
     if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot) atomicAdd(assembled, __popc(ballot));
     store_sym(b.k64 + (size_t)a * 6 * n, n, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
-    store_sym(b.k32 + (size_t)a * 6 * n, n, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
+    const uint32_t kn = kstride32(n);
+    store_sym(b.k32 + (size_t)a * 6 * kn, kn, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
     b.force[e] = force.x;
     b.force[m3n + e] = force.y;
     b.force[2 * m3n + e] = force.z;

@@ -38,7 +38,7 @@ struct PcgScalars {
 // Per-bond storage of the last assembly (SoA, bond e = axis * n + i).
 struct BondArrays {
     double* k64;        // [18][n]  world K (sym6) per axis, 0 if not assembled
-    float* k32;         // [18][n]
+    float* k32;         // [3][6][kstride32(n)]: FP32 copy, axis-padded to 16 bytes
     double* mat_k;      // [6][3n]  undamaged local K (sym6) for stress
     double4* frame_q;   // [3n]     bond frame quaternion (slerp midpoint)
     double* force;      // [3][3n]  K (x_j - x_i - rest) of assembled bonds

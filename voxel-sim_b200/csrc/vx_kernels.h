@@ -51,6 +51,9 @@ cudaError_t launch_predict(vx_scene* s, const double* gravity, double h);
 cudaError_t launch_velocity(vx_scene* s, double h);
 cudaError_t launch_velocity_update(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
                                    int32_t op);
+cudaError_t launch_gather3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* field, double* d_out);
+cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
+                            double* field);
 // bond stress / ratio / force
 cudaError_t launch_bond_stress(vx_scene* s, float* d_ratio, float* d_force, uint32_t* d_near, uint32_t cap);
 

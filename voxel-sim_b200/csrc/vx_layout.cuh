@@ -5,14 +5,21 @@
 // warp's loads are contiguous:
 //   FP32: float4[n] (xx, yy, zz, xy) followed by float2[n] (xz, yz)  -> 6n floats
 //   FP64: double2[n] (xx, yy), double2[n] (zz, xy), double2[n] (xz, yz) -> 6n doubles
-// Per-axis bond stiffness uses one such array per axis at base + axis * 6n.
+// Per-axis bond stiffness uses one such array per axis. In FP64 the axes sit
+// at base + axis * 6n; in FP32 at base + axis * 6 * kstride32(n), n rounded up
+// to a multiple of 4, so every axis starts on a 16-byte boundary (a float4
+// load at 24 n bytes would be misaligned for odd n).
 #pragma once
 
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
 
 namespace vx {
+
+// REV stride of the per-axis FP32 stiffness arrays.
+__host__ __device__ constexpr uint32_t kstride32(uint32_t n) { return (n + 3u) & ~3u; }
 
 template <typename T>
 struct Sym {

@@ -231,6 +231,7 @@ __global__ void k_accumulate(uint32_t n, double* __restrict__ x64, const float* 
 static IterArgs<double> args64(vx_scene* s, int ping) {
     IterArgs<double> a;
     a.n = s->n;
+    a.kn = s->n;
     a.flags = s->flags;
     a.D = s->d64;
     a.K = s->bonds.k64;
@@ -253,6 +254,7 @@ static IterArgs<double> args64(vx_scene* s, int ping) {
 static IterArgs<float> args32(vx_scene* s, int ping) {
     IterArgs<float> a;
     a.n = s->n;
+    a.kn = kstride32(s->n);
     a.flags = s->flags;
     a.D = s->d32;
     a.K = s->bonds.k32;

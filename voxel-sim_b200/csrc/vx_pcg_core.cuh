@@ -12,6 +12,7 @@ namespace vx {
 template <typename T>
 struct IterArgs {
     uint32_t n;
+    uint32_t kn;      // REV stride of the per-axis K arrays (n in FP64, kstride32(n) in FP32)
     const uint8_t* flags;
     const T* D;       // projected diagonal (sym layout)
     const T* K;       // per-axis bond K (3 sym layouts), zero when not assembled
@@ -110,7 +111,7 @@ __device__ __forceinline__ V3<T> apply_row(const IterArgs<T>& a, uint32_t i, V3<
     const Sym<T> D = load_sym(a.D, n, i);
     Sym<T> Ko[3];
 #pragma unroll
-    for (int ax = 0; ax < 3; ++ax) Ko[ax] = load_sym(a.K + ax * 6 * n, n, i);
+    for (int ax = 0; ax < 3; ++ax) Ko[ax] = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, i);
     uint32_t jj[6];
 #pragma unroll
     for (int s = 0; s < 6; ++s) jj[s] = nb[s] == VX_EMPTY_U32 ? i : nb[s];
@@ -119,7 +120,7 @@ __device__ __forceinline__ V3<T> apply_row(const IterArgs<T>& a, uint32_t i, V3<
     for (int s = 0; s < 6; ++s) vj[s] = get(jj[s]);
     Sym<T> Kr[3];
 #pragma unroll
-    for (int ax = 0; ax < 3; ++ax) Kr[ax] = load_sym(a.K + ax * 6 * n, n, jj[3 + ax]);
+    for (int ax = 0; ax < 3; ++ax) Kr[ax] = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, jj[3 + ax]);
     V3<T> y = mul(D, vi);
     V3<T> s = {T(0), T(0), T(0)};
 #pragma unroll

@@ -40,6 +40,7 @@ constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 1;
 struct PersistArgs {
     uint32_t n;
     uint32_t cap;  // REVs per block (contiguous range)
+    uint32_t kn;   // REV stride of the per-axis K arrays
     const uint8_t* flags;
     const float* D;
     const float* K;
@@ -167,9 +168,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
         const size_t i = lo + li;
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-            const float* kb = a.K + (size_t)ax * 6 * n;
+            const float* kb = a.K + (size_t)ax * 6 * a.kn;
             sK4[ax * cap + li] = __ldg(reinterpret_cast<const float4*>(kb) + i);
-            sK2[ax * cap + li] = __ldg(reinterpret_cast<const float2*>(kb + 4 * (size_t)n) + i);
+            sK2[ax * cap + li] = __ldg(reinterpret_cast<const float2*>(kb + 4 * (size_t)a.kn) + i);
             sNB[ax * cap + li] = __ldg(a.code + (size_t)ax * n + i);
         }
         sFL[li] = __ldg(a.flags + i);
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 } else if (inb) {
                     Kb = sym_of(sK4[ax * cap + lj], sK2[ax * cap + lj]);
                 } else {
-                    Kb = load_sym(a.K + (size_t)ax * 6 * n, n, j);
+                    Kb = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
                 }
                 const float m = ok ? 1.f : 0.f;
                 const F3 pn = {m * fmaf(beta, q4.w, q4.x), m * fmaf(beta, q2.x, q4.y), m * fmaf(beta, q2.y, q4.z)};
@@ -415,6 +416,7 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     PersistArgs a;
     a.n = s->n;
     a.cap = s->persist_cap;
+    a.kn = kstride32(s->n);
     a.flags = s->flags;
     a.D = s->d32;
     a.K = s->bonds.k32;

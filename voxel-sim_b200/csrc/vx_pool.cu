@@ -360,6 +360,7 @@ PoolArgs pool_args(vx_pool* p, const vx_pass_params* prm) {
 IterArgs<float> pool_args32(vx_scene* s, int ping) {
     IterArgs<float> a{};
     a.n = s->n;
+    a.kn = kstride32(s->n);
     a.flags = s->flags;
     a.D = s->d32;
     a.K = s->bonds.k32;
@@ -379,6 +380,7 @@ IterArgs<float> pool_args32(vx_scene* s, int ping) {
 IterArgs<double> pool_args64(vx_scene* s) {
     IterArgs<double> a{};
     a.n = s->n;
+    a.kn = s->n;
     a.flags = s->flags;
     a.D = s->d64;
     a.K = s->bonds.k64;

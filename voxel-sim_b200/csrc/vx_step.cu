@@ -75,6 +75,38 @@ __global__ void k_velocity_update(uint32_t n, uint32_t count, const uint32_t* __
     }
 }
 
+// Indexed gather / scatter of a [3][n] field (AoS values, 3 per entry).
+__global__ void k_gather3(uint32_t n, uint32_t count, const uint32_t* __restrict__ index,
+                          const double* __restrict__ field, double* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t i = index[k];
+    if (i >= n) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[3 * (size_t)k + a] = field[(size_t)a * n + i];
+}
+__global__ void k_scatter3(uint32_t n, uint32_t count, const uint32_t* __restrict__ index,
+                           const double* __restrict__ value, double* __restrict__ field) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t i = index[k];
+    if (i >= n) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) field[(size_t)a * n + i] = value[3 * (size_t)k + a];
+}
+
+cudaError_t launch_gather3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* field, double* d_out) {
+    if (count == 0) return cudaSuccess;
+    k_gather3<<<(count + 255) / 256, 256, 0, s->stream>>>(s->n, count, d_index, field, d_out);
+    return cudaGetLastError();
+}
+cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
+                            double* field) {
+    if (count == 0) return cudaSuccess;
+    k_scatter3<<<(count + 255) / 256, 256, 0, s->stream>>>(s->n, count, d_index, d_value, field);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_predict(vx_scene* s, const double* gravity, double h) {
     if (s->n == 0) return cudaSuccess;
     k_predict<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->pos, s->vel, s->prev, s->drift, s->pred, s->kin,
