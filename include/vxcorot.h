@@ -355,10 +355,20 @@ int32_t vx_pool_get_rotations(vx_pool* pool, uint32_t slot, double* xyzw);
 int32_t vx_pool_set_targets(vx_pool* pool, uint32_t slot, const uint8_t* mask, const double* xyz);
 int32_t vx_pool_set_loads(vx_pool* pool, uint32_t slot, const double* xyz);
 int32_t vx_pool_set_predicted(vx_pool* pool, uint32_t slot, const double* xyz);
+/* Velocities of one slot's REVs (zero when the scene is added). */
+int32_t vx_pool_set_velocities(vx_pool* pool, uint32_t slot, const double* xyz);
+int32_t vx_pool_get_velocities(vx_pool* pool, uint32_t slot, double* xyz);
 int32_t vx_pool_fit_rotations(vx_pool* pool, const uint8_t* enabled, double* out_max_angle);
 int32_t vx_pool_pass(vx_pool* pool, const uint8_t* enabled, const vx_pass_params* params, vx_pass_stats* out);
 int32_t vx_pool_bond_stress(vx_pool* pool, uint32_t slot, float* ratio, float* force, uint32_t* near,
                             uint32_t cap, uint32_t* near_count);
+/*
+ * vx_scene_step for every selected slot together (params.pass.precision must
+ * be VX_PRECISION_MIXED). A slot that meets the early-exit rule leaves the
+ * remaining passes of its substep while the others continue; each slot's
+ * result is the same whichever other slots share the call. out[max_slots].
+ */
+int32_t vx_pool_step(vx_pool* pool, const uint8_t* enabled, const vx_step_params* params, vx_step_stats* out);
 int32_t vx_pool_checkpoint(vx_pool* pool, int32_t op);
 void* vx_pool_stream(vx_pool* pool);
 

@@ -132,3 +132,58 @@ def test_pool_bond_stress_matches_single_scene(ctx):
     assert np.all(np.abs(g["ratio"][live] - p["ratio"][live]) <= 1e-5 * np.maximum(g["ratio"][live], 1e-3))
     d.close()
     pool.close()
+
+
+def step_params():
+    return N.step_params(1e-3, substeps=2, corotation_iterations=3, corotation_tolerance=1e-6,
+                         gravity=(0.0, 0.0, -9.81), tolerance=TOL, max_iterations=CAP,
+                         precision=N.PRECISION_MIXED)
+
+
+def test_pool_step_matches_single_scene_steps(ctx):
+    """vx_pool_step against vx_scene_step on each scene (both reach 1e-8 in
+    every pass, so they agree to the solve error), over three steps."""
+    sc = scenes()
+    pool = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)
+    slots = [pool.add(s) for s in sc]
+    p = step_params()
+    for _ in range(3):
+        status, stats = pool.step(p)
+        assert status == N.VX_OK
+        for k in slots:
+            assert stats[k]["converged"] == 1 and stats[k]["residual"] <= TOL, stats[k]
+    for s, k in zip(sc, slots):
+        d = N.DeviceScene(ctx, s)
+        for _ in range(3):
+            assert d.step(p)["status"] == N.VX_OK
+        x0 = s.position
+        assert rel(pool.positions(k) - x0, d.positions() - x0) < 1e-5
+        # velocities are (x - predicted) / h: a position difference within the
+        # bar above, divided by the substep h = 0.5 ms
+        v_bar = 1e-5 * np.linalg.norm(d.positions() - x0) / 5e-4
+        assert np.linalg.norm(pool.velocities(k) - d.velocities()) <= v_bar
+        d.close()
+    pool.close()
+
+
+def test_pool_step_is_bit_identical_alone_and_in_a_mix(ctx):
+    """A scene stepped alone in a pool and the same scene stepped together
+    with others (admitted at a different slot and tile range) end with the
+    same bits after three steps, velocities included."""
+    sc = scenes()
+    target = sc[2]
+    p = step_params()
+    alone = N.DevicePool(ctx, target.n + 4096, 4)
+    ka = alone.add(target)
+    mixed = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)
+    others = [mixed.add(s) for s in sc[:2]]
+    km = mixed.add(target)
+    mixed.add(sc[3])
+    for _ in range(3):
+        assert alone.step(p)[0] == N.VX_OK
+        assert mixed.step(p)[0] == N.VX_OK
+    assert np.array_equal(alone.positions(ka), mixed.positions(km))
+    assert np.array_equal(alone.velocities(ka), mixed.velocities(km))
+    assert others
+    alone.close()
+    mixed.close()

@@ -723,6 +723,7 @@ int32_t vx_pool_add(vx_pool* p, const vx_scene_desc* d, uint32_t* out_slot) {
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->pred + c * C + base, pos.data() + c * m, m * 8, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->loads + c * C + base, 0, m * 8, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->vel + c * C + base, 0, m * 8, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->nbr + c * C + base, nbr.data() + c * m, m * 4, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
@@ -832,6 +833,21 @@ int32_t vx_pool_get_positions(vx_pool* p, uint32_t slot, double* xyz) {
     int32_t r = slot_ok(p, slot, xyz, __func__);
     if (r != VX_OK) return r;
     return slot_vec(p, slot, p->s.pos, xyz, false);
+}
+int32_t vx_pool_set_velocities(vx_pool* p, uint32_t slot, const double* xyz) {
+    int32_t r = slot_ok(p, slot, xyz, __func__);
+    if (r != VX_OK) return r;
+    for (size_t t = 0; t < 3 * (size_t)p->rev_n[slot]; ++t)
+        if (!std::isfinite(xyz[t])) {
+            set_error("vx_pool_set_velocities: non-finite value at %zu", t);
+            return VX_NONFINITE;
+        }
+    return slot_vec(p, slot, p->s.vel, const_cast<double*>(xyz), true);
+}
+int32_t vx_pool_get_velocities(vx_pool* p, uint32_t slot, double* xyz) {
+    int32_t r = slot_ok(p, slot, xyz, __func__);
+    if (r != VX_OK) return r;
+    return slot_vec(p, slot, p->s.vel, xyz, false);
 }
 int32_t vx_pool_set_loads(vx_pool* p, uint32_t slot, const double* xyz) {
     int32_t r = slot_ok(p, slot, xyz, __func__);
@@ -979,6 +995,85 @@ int32_t vx_pool_bond_stress(vx_pool* p, uint32_t slot, float* ratio, float* forc
     }
     if (near_count) *near_count = kept;
     return VX_OK;
+}
+
+
+// The fixed step of vx_scene_step for every selected slot together: each
+// substep predicts the selected slots, fits, runs up to
+// corotation_iterations pool passes (a slot leaves the remaining passes of
+// the substep once its angle change and pass residual are within tolerance,
+// src/solver.rs:561-570) and updates the velocities.
+int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* prm, vx_step_stats* out) {
+    clear_error();
+    if (!p || !prm) {
+        set_error("vx_pool_step: null argument");
+        return VX_BAD_INPUT;
+    }
+    if (!(prm->fixed_dt > 0.0) || !std::isfinite(prm->fixed_dt) || prm->substeps == 0 ||
+        prm->corotation_iterations == 0 || !std::isfinite(prm->gravity[0]) || !std::isfinite(prm->gravity[1]) ||
+        !std::isfinite(prm->gravity[2])) {
+        set_error("vx_pool_step: invalid fixed_dt=%g, substeps=%u, corotation_iterations=%u or gravity",
+                  prm->fixed_dt, prm->substeps, prm->corotation_iterations);
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(p->s.device);
+    const uint32_t S = p->slots;
+    const double h = prm->fixed_dt / (double)prm->substeps;
+    std::vector<uint8_t> on(S), active(S);
+    for (uint32_t k = 0; k < S; ++k) on[k] = p->used[k] && (!enabled || enabled[k]);
+    std::vector<vx_step_stats> st(S);
+    for (uint32_t k = 0; k < S; ++k) st[k].converged = 1;
+    std::vector<vx_pass_stats> ps(S);
+    std::vector<double> angle(S, 0.0);
+    int32_t worst = VX_OK;
+    std::vector<uint8_t> sel;
+    for (uint32_t sub = 0; sub < prm->substeps; ++sub) {
+        int32_t r = pool_select(p, on.data(), sel);
+        if (r != VX_OK) return r;
+        VX_POOL_TRY(launch_predict(&p->s, prm->gravity, h), "pool prediction");
+        r = vx_pool_fit_rotations(p, on.data(), angle.data());
+        if (r != VX_OK) return r;
+        for (uint32_t k = 0; k < S; ++k) {
+            active[k] = on[k];
+            if (on[k]) st[k].max_angle = angle[k];
+        }
+        for (uint32_t pass = 0; pass < prm->corotation_iterations; ++pass) {
+            vx_pass_params pp = prm->pass;
+            pp.h = h;
+            pp.reuse_preconditioner = prm->pass.reuse_preconditioner && pass > 0;
+            r = vx_pool_pass(p, active.data(), &pp, ps.data());
+            if (r == VX_CUDA_ERROR || r == VX_OOM || r == VX_BAD_INPUT || r == VX_TIMEOUT) return r;
+            for (uint32_t k = 0; k < S; ++k) {
+                if (!active[k]) continue;
+                st[k].passes += 1;
+                st[k].pcg_iterations += ps[k].iterations;
+                st[k].residual = ps[k].residual;
+                if (!ps[k].converged) {
+                    st[k].converged = 0;
+                    if (worst == VX_OK) worst = VX_NOT_CONVERGED;
+                }
+            }
+            if (pass + 1 == prm->corotation_iterations) break;
+            r = vx_pool_fit_rotations(p, active.data(), angle.data());
+            if (r != VX_OK) return r;
+            bool any = false;
+            for (uint32_t k = 0; k < S; ++k) {
+                if (!active[k]) continue;
+                st[k].max_angle = angle[k];
+                if (angle[k] <= prm->corotation_tolerance && st[k].residual <= prm->pass.tolerance) active[k] = 0;
+                any = any || active[k];
+            }
+            if (!any) break;
+        }
+        r = pool_select(p, on.data(), sel);
+        if (r != VX_OK) return r;
+        VX_POOL_TRY(launch_velocity(&p->s, h), "pool velocity update");
+        VX_POOL_TRY(cudaStreamSynchronize(p->s.stream), "pool step");
+    }
+    if (out)
+        for (uint32_t k = 0; k < S; ++k) out[k] = on[k] ? st[k] : vx_step_stats{};
+    if (worst == VX_NOT_CONVERGED) set_error("vx_pool_step: a scene's pass did not reach its tolerance");
+    return worst;
 }
 
 }  // extern "C"

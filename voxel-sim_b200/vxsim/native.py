@@ -406,12 +406,13 @@ def _bind_pool(L):
     L.vx_pool_add.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), C.POINTER(C.c_uint32)]
     L.vx_pool_remove.argtypes = [C.c_void_p, C.c_uint32]
     for name in ("vx_pool_set_positions", "vx_pool_get_positions", "vx_pool_get_rotations", "vx_pool_set_loads",
-                 "vx_pool_set_predicted"):
+                 "vx_pool_set_predicted", "vx_pool_set_velocities", "vx_pool_get_velocities"):
         getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, f64p]
     L.vx_pool_set_targets.argtypes = [C.c_void_p, C.c_uint32, u8p, f64p]
     L.vx_pool_fit_rotations.argtypes = [C.c_void_p, u8p, f64p]
     L.vx_pool_pass.argtypes = [C.c_void_p, u8p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
     L.vx_pool_bond_stress.argtypes = [C.c_void_p, C.c_uint32, f32p, f32p, u32p, C.c_uint32, u32p]
+    L.vx_pool_step.argtypes = [C.c_void_p, u8p, C.POINTER(VxStepParams), C.POINTER(VxStepStats)]
     L.vx_pool_checkpoint.argtypes = [C.c_void_p, C.c_int32]
     L.vx_pool_stream.restype = C.c_void_p
     L.vx_pool_stream.argtypes = [C.c_void_p]
@@ -492,6 +493,22 @@ class DevicePool:
     def set_predicted(self, slot, x=None):
         x = None if x is None else self._v(x)
         check(load().vx_pool_set_predicted(self.h, slot, _p(x, C.c_double)))
+
+    def set_velocities(self, slot, v):
+        x = self._v(v)
+        check(load().vx_pool_set_velocities(self.h, slot, _p(x, C.c_double)))
+
+    def velocities(self, slot) -> np.ndarray:
+        out = np.zeros(3 * self.n[slot], np.float64)
+        check(load().vx_pool_get_velocities(self.h, slot, _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def step(self, params: "VxStepParams", enabled=None, allow=(VX_NOT_CONVERGED,)):
+        """vx_pool_step: one fixed step of every selected slot; per-slot stats."""
+        m = self._mask(enabled)
+        stats = (VxStepStats * self.slots)()
+        status = check(load().vx_pool_step(self.h, _p(m, C.c_uint8), C.byref(params), stats), allow=allow)
+        return status, [stats[k].as_dict() for k in range(self.slots)]
 
     def _mask(self, enabled):
         if enabled is None:
