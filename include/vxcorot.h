@@ -353,6 +353,13 @@ int32_t vx_pool_set_positions(vx_pool* pool, uint32_t slot, const double* xyz);
 int32_t vx_pool_get_positions(vx_pool* pool, uint32_t slot, double* xyz);
 int32_t vx_pool_get_rotations(vx_pool* pool, uint32_t slot, double* xyzw);
 int32_t vx_pool_set_targets(vx_pool* pool, uint32_t slot, const uint8_t* mask, const double* xyz);
+/*
+ * Moving targets: REVs whose target mask also has VX_TARGET_MOVING set get
+ * their targeted axes advanced by delta[3 * slot + a] for every selected slot
+ * (a prescribed-displacement tool that moves each step). delta[3 * max_slots].
+ */
+#define VX_TARGET_MOVING 8u
+int32_t vx_pool_advance_targets(vx_pool* pool, const uint8_t* enabled, const double* delta);
 int32_t vx_pool_set_loads(vx_pool* pool, uint32_t slot, const double* xyz);
 int32_t vx_pool_set_predicted(vx_pool* pool, uint32_t slot, const double* xyz);
 /* Velocities of one slot's REVs (zero when the scene is added). */
@@ -370,6 +377,76 @@ int32_t vx_pool_bond_stress(vx_pool* pool, uint32_t slot, float* ratio, float* f
  */
 int32_t vx_pool_step(vx_pool* pool, const uint8_t* enabled, const vx_step_params* params, vx_step_stats* out);
 int32_t vx_pool_checkpoint(vx_pool* pool, int32_t op);
+
+/*
+ * ---- served form: a request loop that keeps scenes resident ----
+ *
+ * No counterpart in the reference. A vx_server owns a host thread, a CUDA
+ * stream and one pool. vx_server_submit copies a scene and queues it; at every
+ * round boundary the thread admits queued scenes in arrival order while a slot
+ * and a tile range of the pool are free (admission by memory footprint; the
+ * pool's capacity is the HBM budget), then advances every resident scene's
+ * moving targets by target_velocity * fixed_dt and runs one fixed step of all
+ * resident scenes together (vx_pool_step), so requests that arrive while
+ * others are stepping share the device with them (continuous batching). A
+ * scene leaves after plan.steps steps; its result and final positions wait for
+ * vx_server_wait. Each scene's result is the one it gets alone: pool slots
+ * keep per-scene scalars. Latency of a scene-step is the time of the round it
+ * stepped in.
+ */
+typedef struct vx_server vx_server;
+
+typedef struct vx_server_config {
+    uint64_t max_revs;            /* pool capacity in REVs; 0 = hbm_fraction of the device memory */
+    double hbm_fraction;          /* budget used when max_revs == 0 (for example 0.8) */
+    uint32_t max_slots;           /* resident scenes at most */
+    vx_step_params step;          /* the step every scene runs (pass.precision VX_PRECISION_MIXED) */
+} vx_server_config;
+
+typedef struct vx_request_plan {
+    uint32_t steps;               /* fixed steps to run, >= 1 */
+    double target_velocity[3];    /* m/s of the targets marked VX_TARGET_MOVING (a driven tool) */
+} vx_request_plan;
+
+typedef struct vx_request_result {
+    int32_t status;               /* VX_OK; VX_NOT_CONVERGED if a pass missed its tolerance; other
+                                     codes when the request failed */
+    uint32_t n;                   /* REVs */
+    uint32_t steps_done;
+    uint32_t passes;              /* corotational passes run */
+    uint64_t pcg_iterations;
+    double worst_residual;        /* largest pass residual over all steps */
+    double queued_s;              /* submission to admission */
+    double run_s;                 /* admission to completion */
+} vx_request_result;
+
+typedef struct vx_server_stats {
+    uint64_t submitted, completed, failed;
+    uint32_t resident, queued;
+    uint64_t rounds;              /* batched steps run */
+    uint64_t scene_steps;
+    uint64_t solves;              /* corotational passes, each solved to its tolerance */
+    double elapsed_s;             /* since creation */
+    double busy_s;                /* inside batched steps */
+    double p50_step_ms, p99_step_ms, max_step_ms;  /* per scene-step latency */
+    uint64_t pool_revs;           /* pool capacity */
+    uint64_t pool_bytes;          /* device bytes of the pool */
+} vx_server_stats;
+
+int32_t vx_server_create(vx_ctx* ctx, const vx_server_config* config, vx_server** out_server);
+/* mask[n] / xyz[3n] are the scene's targets (VX_TARGET_MOVING marks moving ones), or NULL. */
+int32_t vx_server_submit(vx_server* server, const vx_scene_desc* desc, const uint8_t* target_mask,
+                         const double* target, const vx_request_plan* plan, uint64_t* out_ticket);
+/*
+ * Waits up to timeout_s for a request. Returns VX_TIMEOUT while it is still
+ * queued or running; once it has finished, fills out (and positions[3n] when
+ * not NULL), releases the request and returns VX_OK.
+ */
+int32_t vx_server_wait(vx_server* server, uint64_t ticket, double timeout_s, vx_request_result* out,
+                       double* positions);
+int32_t vx_server_get_stats(vx_server* server, vx_server_stats* out);
+/* Stops after the current round; queued and resident requests are dropped. */
+int32_t vx_server_destroy(vx_server* server);
 void* vx_pool_stream(vx_pool* pool);
 
 /* ---- state checkpoint and measurement hooks (no counterpart in the reference) ---- */

@@ -48,6 +48,7 @@ cudaError_t launch_assembly(vx_scene* s, double h, bool reuse_preconditioner);
 cudaError_t launch_apply_correction(vx_scene* s);
 // substep prediction and velocity update of the fixed step (vx_step.cu)
 cudaError_t launch_predict(vx_scene* s, const double* gravity, double h);
+cudaError_t launch_advance_targets(vx_scene* s, const double* d_delta);
 cudaError_t launch_velocity(vx_scene* s, double h);
 cudaError_t launch_velocity_update(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
                                    int32_t op);

@@ -998,6 +998,36 @@ int32_t vx_pool_bond_stress(vx_pool* p, uint32_t slot, float* ratio, float* forc
 }
 
 
+int32_t vx_pool_advance_targets(vx_pool* p, const uint8_t* enabled, const double* delta) {
+    clear_error();
+    if (!p || !delta) {
+        set_error("vx_pool_advance_targets: null argument");
+        return VX_BAD_INPUT;
+    }
+    for (size_t t = 0; t < 3 * (size_t)p->slots; ++t)
+        if (!std::isfinite(delta[t])) {
+            set_error("vx_pool_advance_targets: non-finite delta at %zu", t);
+            return VX_NONFINITE;
+        }
+    if (p->slots > p->s.n) {  // the staging below holds 3 doubles per REV of capacity
+        set_error("vx_pool_advance_targets: pool has more slots (%u) than REVs (%u)", p->slots, p->s.n);
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(p->s.device);
+    std::vector<uint8_t> on;
+    int32_t r = pool_select(p, enabled, on);
+    if (r != VX_OK) return r;
+    vx_scene* s = &p->s;
+    // the FP64 z vector (3 x capacity doubles, free between passes) holds the deltas
+    VX_POOL_TRY(cudaStreamSynchronize(s->stream), "advance targets");
+    std::memcpy(s->h_stage, delta, 3 * (size_t)p->slots * sizeof(double));
+    VX_POOL_TRY(cudaMemcpyAsync(s->z64, s->h_stage, 3 * (size_t)p->slots * sizeof(double), cudaMemcpyHostToDevice,
+                                s->stream), "advance targets");
+    VX_POOL_TRY(launch_advance_targets(s, s->z64), "advance targets");
+    VX_POOL_TRY(cudaStreamSynchronize(s->stream), "advance targets");
+    return VX_OK;
+}
+
 // The fixed step of vx_scene_step for every selected slot together: each
 // substep predicts the selected slots, fits, runs up to
 // corotation_iterations pool passes (a slot leaves the remaining passes of

@@ -107,6 +107,28 @@ cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index
     return cudaGetLastError();
 }
 
+// Targets that move (mask bit VX_TARGET_MOVING) advance by their slot's delta
+// on their targeted axes; delta[3 * slot + a].
+__global__ void k_advance_targets(uint32_t n, const uint8_t* __restrict__ tmask, double* __restrict__ target,
+                                  const double* __restrict__ delta, const uint8_t* __restrict__ tile_on,
+                                  const uint32_t* __restrict__ tile_scene) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !tile_active(tile_on, i)) return;
+    const uint8_t tm = tmask[i];
+    if (!(tm & VX_TARGET_MOVING)) return;
+    const uint32_t slot = tile_scene ? tile_scene[i >> 8] : 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if ((tm >> a) & 1) target[(size_t)a * n + i] += delta[3 * (size_t)slot + a];
+}
+
+cudaError_t launch_advance_targets(vx_scene* s, const double* d_delta) {
+    if (s->n == 0) return cudaSuccess;
+    k_advance_targets<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->tmask, s->target, d_delta, s->tile_on,
+                                                                 s->tile_scene);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_predict(vx_scene* s, const double* gravity, double h) {
     if (s->n == 0) return cudaSuccess;
     k_predict<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->pos, s->vel, s->prev, s->drift, s->pred, s->kin,

@@ -79,6 +79,35 @@ class VxStepStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class VxServerConfig(C.Structure):
+    _fields_ = [("max_revs", C.c_uint64), ("hbm_fraction", C.c_double), ("max_slots", C.c_uint32),
+                ("step", VxStepParams)]
+
+
+class VxRequestPlan(C.Structure):
+    _fields_ = [("steps", C.c_uint32), ("target_velocity", C.c_double * 3)]
+
+
+class VxRequestResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("n", C.c_uint32), ("steps_done", C.c_uint32), ("passes", C.c_uint32),
+                ("pcg_iterations", C.c_uint64), ("worst_residual", C.c_double), ("queued_s", C.c_double),
+                ("run_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VxServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("resident", C.c_uint32), ("queued", C.c_uint32), ("rounds", C.c_uint64),
+                ("scene_steps", C.c_uint64), ("solves", C.c_uint64), ("elapsed_s", C.c_double),
+                ("busy_s", C.c_double), ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double),
+                ("max_step_ms", C.c_double), ("pool_revs", C.c_uint64), ("pool_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def step_params(fixed_dt, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5, gravity=(0.0, 0.0, 0.0),
                 tolerance=1e-5, max_iterations=10000, precision=PRECISION_FP64, reuse=False, inner_tolerance=0.0,
                 max_outer=0, kernel=KERNEL_AUTO) -> VxStepParams:
@@ -131,6 +160,12 @@ def load(path: Path | None = None):
     L.vx_scene_stream.argtypes = [C.c_void_p]
     L.vx_scene_kernel_times.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_uint64, f64p]
     L.vx_scene_step.argtypes = [C.c_void_p, C.POINTER(VxStepParams), C.POINTER(VxStepStats)]
+    L.vx_server_create.argtypes = [C.c_void_p, C.POINTER(VxServerConfig), C.POINTER(C.c_void_p)]
+    L.vx_server_submit.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), u8p, f64p, C.POINTER(VxRequestPlan),
+                                   C.POINTER(C.c_uint64)]
+    L.vx_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_double, C.POINTER(VxRequestResult), f64p]
+    L.vx_server_get_stats.argtypes = [C.c_void_p, C.POINTER(VxServerStats)]
+    L.vx_server_destroy.argtypes = [C.c_void_p]
     L.vx_scene_set_velocities.argtypes = [C.c_void_p, f64p]
     L.vx_scene_get_velocities.argtypes = [C.c_void_p, f64p]
     L.vx_scene_update_velocities.argtypes = [C.c_void_p, C.c_uint32, u32p, f64p, C.c_int32]
@@ -554,3 +589,60 @@ class DevicePool:
     @property
     def stream_ptr(self):
         return int(load().vx_pool_stream(self.h) or 0)
+
+
+class Server:
+    """The served form (vx_server): a native thread keeps scenes resident in one
+    pool, admits submissions at round boundaries and steps all resident scenes
+    together."""
+
+    def __init__(self, ctx: Context, step: VxStepParams, max_slots: int = 64, max_revs: int = 0,
+                 hbm_fraction: float = 0.8):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        cfg = VxServerConfig(max_revs, hbm_fraction, max_slots, step)
+        check(load().vx_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
+        self.n = {}
+
+    def submit(self, scene, steps: int, target_velocity=(0.0, 0.0, 0.0), moving=None) -> int:
+        """Queues a scene for `steps` fixed steps. `moving` (bool per REV) marks
+        targeted REVs whose targets advance at target_velocity (m/s)."""
+        keep = {}
+        desc = scene_desc(scene, keep)
+        mask = np.ascontiguousarray(scene.target_mask, np.uint8).copy()
+        if moving is not None:
+            mask[np.asarray(moving, bool)] |= 8
+        tgt = np.ascontiguousarray(scene.target, np.float64).reshape(-1)
+        plan = VxRequestPlan(steps, (C.c_double * 3)(*target_velocity))
+        ticket = C.c_uint64()
+        check(load().vx_server_submit(self.h, C.byref(desc), _p(mask, C.c_uint8), _p(tgt, C.c_double),
+                                      C.byref(plan), C.byref(ticket)))
+        self.n[ticket.value] = scene.n
+        return ticket.value
+
+    def wait(self, ticket: int, timeout: float = 600.0):
+        """(result dict, final positions) once the request has finished, else None."""
+        res = VxRequestResult()
+        pos = np.zeros(3 * self.n[ticket], np.float64)
+        st = load().vx_server_wait(self.h, ticket, timeout, C.byref(res), _p(pos, C.c_double))
+        if st == VX_TIMEOUT:
+            return None
+        check(st)
+        self.n.pop(ticket, None)
+        return res.as_dict(), pos.reshape(-1, 3)
+
+    def stats(self) -> dict:
+        out = VxServerStats()
+        check(load().vx_server_get_stats(self.h, C.byref(out)))
+        return out.as_dict()
+
+    def close(self):
+        if self.h:
+            load().vx_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
