@@ -431,6 +431,8 @@ typedef struct vx_server_stats {
     double p50_step_ms, p99_step_ms, max_step_ms;  /* per scene-step latency */
     uint64_t pool_revs;           /* pool capacity */
     uint64_t pool_bytes;          /* device bytes of the pool */
+    double worst_residual;        /* largest pass residual of any scene-step so far */
+    uint64_t not_converged;       /* scene-steps with a pass that missed its tolerance */
 } vx_server_stats;
 
 int32_t vx_server_create(vx_ctx* ctx, const vx_server_config* config, vx_server** out_server);

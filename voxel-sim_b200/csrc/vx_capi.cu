@@ -134,8 +134,9 @@ static int32_t download_vec3(vx_scene* s, double* dst, const double* src) {
 }
 
 // Allocates a scene's arena (n REVs, material_count materials), its stream and
-// pinned host buffers, and clears the arena.
-int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_count) {
+// pinned host buffers (a stage of 4 doubles per REV, for at most stage_revs
+// REVs when that is not 0), and clears the arena.
+int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_count, size_t stage_revs) {
     s->ctx = ctx;
     s->device = ctx->device;
     s->sm_count = ctx->sm_count > 0 ? ctx->sm_count : 1;
@@ -150,7 +151,10 @@ int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_coun
     s->arena.used = 0;
     carve(s, s->arena, n, material_count);
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMallocHost(&s->h_stage, 4 * (size_t)(n ? n : 1) * sizeof(double));
+    size_t stage = n ? n : 1;
+    if (stage_revs && stage_revs < stage) stage = stage_revs;
+    s->stage_revs = stage;
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_stage, 4 * stage * sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_sc, sizeof(PcgScalars));
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_done, 2 * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev[0], cudaEventDisableTiming);
@@ -331,7 +335,7 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
     cudaSetDevice(ctx->device);
     vx_scene* s = new (std::nothrow) vx_scene();
     if (!s) return VX_OOM;
-    int32_t ar = scene_alloc(s, ctx, n, d->material_count);
+    int32_t ar = scene_alloc(s, ctx, n, d->material_count, 0);
     if (ar != VX_OK) {
         delete s;
         return ar;
@@ -497,7 +501,7 @@ int32_t vx_scene_update_velocities(vx_scene* s, uint32_t count, const uint32_t* 
     // entry, at most n entries at a time) into the FP64 z and p vectors, which
     // are free between passes
     for (uint32_t base = 0; base < count;) {
-        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, (size_t)s->n);
+        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, s->stage_revs);
         VX_TRY(cudaStreamSynchronize(s->stream), "velocity update");
         double* vals = s->h_stage;
         uint32_t* idx = reinterpret_cast<uint32_t*>(s->h_stage + 3 * (size_t)chunk);
@@ -541,7 +545,7 @@ static int32_t indexed_field(vx_scene* s, int32_t field, uint32_t count, const u
     cudaSetDevice(s->device);
     double* dev_field = field == VX_FIELD_POSITION ? s->pos : s->vel;
     for (uint32_t base = 0; base < count;) {
-        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, (size_t)s->n);
+        const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, s->stage_revs);
         VX_TRY(cudaStreamSynchronize(s->stream), who);
         double* vals = s->h_stage;
         uint32_t* idx = reinterpret_cast<uint32_t*>(s->h_stage + 3 * (size_t)chunk);

@@ -133,7 +133,8 @@ struct vx_scene {
     uint32_t* nbcode_bad;         // [1] neighbour entries a delta cannot encode
 
     // host mirrors
-    double* h_stage = nullptr;       // pinned staging of host copies [4n doubles]
+    double* h_stage = nullptr;       // pinned staging of host copies [4 * stage_revs doubles]
+    size_t stage_revs = 0;           // n for a single scene; capped for pools
     vx::PcgScalars* h_sc = nullptr;  // pinned
     int32_t* h_done = nullptr;       // pinned [2]
     cudaEvent_t ev[2] = {nullptr, nullptr};

@@ -82,7 +82,10 @@ struct vx_pool {
 
 namespace vx {
 
-int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_count);
+int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_count, size_t stage_revs);
+
+// Pinned staging of a pool, in REVs: per-slot copies go through it in chunks.
+constexpr size_t kPoolStageRevs = size_t(4) << 20;
 void scene_release(vx_scene* s);
 
 namespace {
@@ -539,7 +542,12 @@ int32_t vx_pool_create(vx_ctx* ctx, uint64_t max_revs, uint32_t max_slots, vx_po
     cudaSetDevice(ctx->device);
     vx_pool* p = new (std::nothrow) vx_pool();
     if (!p) return VX_OOM;
-    int32_t r = scene_alloc(&p->s, ctx, (uint32_t)cap, VX_POOL_MATERIALS * max_slots);
+    if ((size_t)max_slots * 3 > 4 * kPoolStageRevs) {
+        set_error("vx_pool_create: %u slots exceed the staging of per-slot scalars", max_slots);
+        delete p;
+        return VX_BAD_INPUT;
+    }
+    int32_t r = scene_alloc(&p->s, ctx, (uint32_t)cap, VX_POOL_MATERIALS * max_slots, kPoolStageRevs);
     if (r != VX_OK) {
         delete p;
         return r;
@@ -798,19 +806,23 @@ static int32_t slot_vec(vx_pool* p, uint32_t slot, double* dev, double* host, bo
     const size_t C = s->n, base = (size_t)p->first[slot] * 256, n = p->rev_n[slot];
     double* stage = s->h_stage;
     cudaError_t e = cudaStreamSynchronize(s->stream);
-    if (upload) {
-        for (size_t i = 0; i < n; ++i)
-            for (int c = 0; c < 3; ++c) stage[c * n + i] = host[3 * i + c];
-        for (int c = 0; c < 3 && e == cudaSuccess; ++c)
-            e = cudaMemcpyAsync(dev + c * C + base, stage + c * n, n * 8, cudaMemcpyHostToDevice, s->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-    } else {
-        for (int c = 0; c < 3 && e == cudaSuccess; ++c)
-            e = cudaMemcpyAsync(stage + c * n, dev + c * C + base, n * 8, cudaMemcpyDeviceToHost, s->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        if (e == cudaSuccess)
-            for (size_t i = 0; i < n; ++i)
-                for (int c = 0; c < 3; ++c) host[3 * i + c] = stage[c * n + i];
+    // chunks of at most stage_revs REVs (AoS host <-> SoA device)
+    for (size_t lo = 0; lo < n && e == cudaSuccess; lo += s->stage_revs) {
+        const size_t m = std::min(s->stage_revs, n - lo);
+        if (upload) {
+            for (size_t i = 0; i < m; ++i)
+                for (int c = 0; c < 3; ++c) stage[c * m + i] = host[3 * (lo + i) + c];
+            for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+                e = cudaMemcpyAsync(dev + c * C + base + lo, stage + c * m, m * 8, cudaMemcpyHostToDevice, s->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        } else {
+            for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+                e = cudaMemcpyAsync(stage + c * m, dev + c * C + base + lo, m * 8, cudaMemcpyDeviceToHost, s->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+            if (e == cudaSuccess)
+                for (size_t i = 0; i < m; ++i)
+                    for (int c = 0; c < 3; ++c) host[3 * (lo + i) + c] = stage[c * m + i];
+        }
     }
     if (e != cudaSuccess) {
         set_error("pool copy failed: %s", cudaGetErrorString(e));

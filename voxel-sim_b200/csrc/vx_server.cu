@@ -83,7 +83,8 @@ struct vx_server {
     uint64_t next_ticket = 1;
     // statistics (under mu)
     uint64_t submitted = 0, completed = 0, failed = 0, rounds = 0, scene_steps = 0, solves = 0;
-    double busy_s = 0.0;
+    double busy_s = 0.0, worst_residual = 0.0;
+    uint64_t not_converged = 0;
     std::vector<float> latency_ms;
     Clock::time_point start = Clock::now();
 
@@ -200,7 +201,11 @@ void vx_server::run() {
                 r->res.passes += st[k].passes;
                 r->res.pcg_iterations += st[k].pcg_iterations;
                 r->res.worst_residual = std::max(r->res.worst_residual, st[k].residual);
-                if (!st[k].converged) r->res.status = VX_NOT_CONVERGED;
+                if (!st[k].converged) {
+                    r->res.status = VX_NOT_CONVERGED;
+                    ++not_converged;
+                }
+                worst_residual = std::max(worst_residual, st[k].residual);
                 ++scene_steps;
                 solves += st[k].passes;
                 latency_ms.push_back(ms);
@@ -366,6 +371,8 @@ int32_t vx_server_get_stats(vx_server* s, vx_server_stats* out) {
     }
     o.pool_revs = s->pool_revs;
     o.pool_bytes = s->pool_bytes;
+    o.worst_residual = s->worst_residual;
+    o.not_converged = s->not_converged;
     *out = o;
     return VX_OK;
 }

@@ -102,7 +102,8 @@ class VxServerStats(C.Structure):
                 ("resident", C.c_uint32), ("queued", C.c_uint32), ("rounds", C.c_uint64),
                 ("scene_steps", C.c_uint64), ("solves", C.c_uint64), ("elapsed_s", C.c_double),
                 ("busy_s", C.c_double), ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double),
-                ("max_step_ms", C.c_double), ("pool_revs", C.c_uint64), ("pool_bytes", C.c_uint64)]
+                ("max_step_ms", C.c_double), ("pool_revs", C.c_uint64), ("pool_bytes", C.c_uint64),
+                ("worst_residual", C.c_double), ("not_converged", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
