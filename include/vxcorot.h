@@ -267,6 +267,49 @@ int32_t vx_bond_stress(vx_scene* scene, float* ratio, float* force, uint32_t* ne
                        uint32_t cap, uint32_t* near_count);
 
 /*
+ * ---- fracture on the device ----
+ *
+ * FractureConfig fields read by fracture::update (src/fracture.rs:12-43; the
+ * reference's defaults are 35, 0.005, 1000, 3, 0.5, 0.9).
+ */
+typedef struct vx_fracture_config {
+    double damage_rate;
+    double energy_release;
+    double fatigue_cycles;
+    double fatigue_exponent;
+    double fatigue_threshold;
+    double plastic_heat_fraction;
+} vx_fracture_config;
+
+/* Energy of a fracture stage, J, summed over bonds (fracture::Dissipation). */
+typedef struct vx_dissipation {
+    double plastic_heat;
+    double stored_plastic;
+    double surface_work;
+    double damage_heat;
+    double released;
+} vx_dissipation;
+
+/*
+ * The fracture stage of a substep (src/solver.rs:600-665): fracture::update
+ * (src/fracture.rs:210-292) on every bond of the last assembly that still has
+ * a neighbour and a free owner, with the frame and undamaged stiffness of that
+ * assembly, the current positions and the bond's limits. It runs the plastic
+ * return map, fatigue, damage and the energy split, stores the bond state
+ * (plastic strain, damage, equivalent plastic strain, plastic work, fatigue
+ * state) and breaks bonds whose damage reaches 1 (neighbor = VX_EMPTY, then the
+ * reverse table is rebuilt). dt is the substep. out (or NULL) receives the
+ * summed dissipation (a fixed-order reduction, the same bits every run);
+ * out_broken (or NULL) the number of bonds broken by this call.
+ */
+int32_t vx_fracture_commit(vx_scene* scene, double dt, const vx_fracture_config* config, vx_dissipation* out,
+                           uint32_t* out_broken);
+/* Per-bond fracture state, axis-major: plastic_strain[9n] ((axis*n+i)*3+c), damage[3n],
+   equivalent_plastic_strain[3n], fatigue_damage[3n]; any may be NULL. */
+int32_t vx_scene_get_bond_state(vx_scene* scene, float* plastic_strain, float* damage,
+                                float* equivalent_plastic_strain, float* fatigue_damage);
+
+/*
  * ---- the fixed step on the device ----
  *
  * One call of solver::step_with_axis_targets_and_loads (src/solver.rs:438-700)
@@ -293,6 +336,8 @@ typedef struct vx_step_params {
     double gravity[3];               /* m/s^2 */
     vx_pass_params pass;             /* solve of every pass; reuse_preconditioner applies from
                                         the second pass of a substep on, as the reference's CPU path */
+    int32_t fracture;                /* 1: the fracture stage after the passes of every substep */
+    vx_fracture_config fracture_config;
 } vx_step_params;
 
 typedef struct vx_step_stats {
@@ -301,6 +346,8 @@ typedef struct vx_step_stats {
     double residual;                 /* residual of the last pass (Scene::solver_residual) */
     double max_angle;                /* largest angle change of the last fit, rad */
     int32_t converged;               /* every pass reached its tolerance */
+    uint32_t broken;                 /* bonds broken by the fracture stages */
+    vx_dissipation dissipation;      /* summed over the fracture stages */
 } vx_step_stats;
 
 int32_t vx_scene_step(vx_scene* scene, const vx_step_params* params, vx_step_stats* out);

@@ -41,8 +41,8 @@ int main(void) {{
   printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(vx_material), sizeof(vx_scene_desc), sizeof(vx_pass_params),
          sizeof(vx_pass_stats), offsetof(vx_scene_desc, neighbor), sizeof(vx_step_params),
          offsetof(vx_step_params, pass), sizeof(vx_step_stats));
-  printf("%zu %zu %zu %zu\\n", sizeof(vx_server_config), sizeof(vx_request_plan), sizeof(vx_request_result),
-         sizeof(vx_server_stats));
+  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(vx_server_config), sizeof(vx_request_plan), sizeof(vx_request_result),
+         sizeof(vx_server_stats), sizeof(vx_fracture_config), sizeof(vx_dissipation));
   return 0;
 }}''')
     exe = tmp_path / "layout"
@@ -51,7 +51,8 @@ int main(void) {{
     want = [C.sizeof(N.VxMaterial), C.sizeof(N.VxSceneDesc), C.sizeof(N.VxPassParams), C.sizeof(N.VxPassStats),
             N.VxSceneDesc.neighbor.offset, C.sizeof(N.VxStepParams), N.VxStepParams.pass_.offset,
             C.sizeof(N.VxStepStats), C.sizeof(N.VxServerConfig), C.sizeof(N.VxRequestPlan),
-            C.sizeof(N.VxRequestResult), C.sizeof(N.VxServerStats)]
+            C.sizeof(N.VxRequestResult), C.sizeof(N.VxServerStats), C.sizeof(N.VxFractureConfig),
+            C.sizeof(N.VxDissipation)]
     assert got == want
 
 

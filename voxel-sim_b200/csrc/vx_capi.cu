@@ -49,6 +49,11 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->rev = A.take<uint32_t>(3 * m);
     s->bond_a = A.take<float4>(3 * m);
     s->bond_b = A.take<float4>(3 * m);
+    s->bond_c = A.take<float4>(3 * m);
+    s->bond_d = A.take<float>(3 * m);
+    s->frac_partials = A.take<double>(5 * 3 * (size_t)blocks);
+    s->frac_totals = A.take<double>(8);
+    s->frac_counter = A.take<uint32_t>(2);
     s->bonds.k64 = A.take<double>(18 * m);
     s->bonds.k32 = A.take<float>(18 * (size_t)kstride32((uint32_t)m));
     s->bonds.mat_k = A.take<double>(18 * m);
@@ -188,6 +193,29 @@ void scene_release(vx_scene* s) {
     s->h_stage = nullptr;
     s->arena.base = nullptr;
     s->stream = nullptr;
+}
+
+// Shared by the single-scene and pool steps: one fracture stage, then the
+// reverse table and neighbour deltas when a bond broke.
+int32_t fracture_stage(vx_scene* s, double dt, const vx_fracture_config* cfg, vx_dissipation* out,
+                       uint32_t* out_broken) {
+    if (!s->assembled) {
+        set_error("vx_fracture_commit: no corotational pass has assembled the bonds yet");
+        return VX_BAD_INPUT;
+    }
+    VX_TRY(launch_fracture_commit(s, dt, cfg), "fracture launch");
+    double tot[8];
+    uint32_t cnt[2];
+    VX_TRY(cudaMemcpyAsync(tot, s->frac_totals, sizeof tot, cudaMemcpyDeviceToHost, s->stream), "fracture");
+    VX_TRY(cudaMemcpyAsync(cnt, s->frac_counter, sizeof cnt, cudaMemcpyDeviceToHost, s->stream), "fracture");
+    VX_TRY(cudaStreamSynchronize(s->stream), "fracture");
+    if (cnt[1]) {
+        VX_TRY(launch_reverse_neighbors(s), "reverse neighbours");
+        VX_TRY(cudaStreamSynchronize(s->stream), "reverse neighbours");
+    }
+    if (out) *out = vx_dissipation{tot[0], tot[1], tot[2], tot[3], tot[4]};
+    if (out_broken) *out_broken = cnt[1];
+    return VX_OK;
 }
 
 }  // namespace vx
@@ -725,6 +753,42 @@ int32_t vx_bond_stress(vx_scene* s, float* ratio, float* force, uint32_t* near, 
         for (size_t k = 0; k < tmp.size() && k < cap; ++k) near[k] = tmp[k];
     }
     if (near_count) *near_count = count;
+    return VX_OK;
+}
+
+int32_t vx_fracture_commit(vx_scene* s, double dt, const vx_fracture_config* cfg, vx_dissipation* out,
+                           uint32_t* out_broken) {
+    clear_error();
+    if (!s || !cfg) {
+        set_error("vx_fracture_commit: null argument");
+        return VX_BAD_INPUT;
+    }
+    if (!(dt > 0.0) || !std::isfinite(dt)) {
+        set_error("vx_fracture_commit: invalid dt=%g", dt);
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(s->device);
+    return fracture_stage(s, dt, cfg, out, out_broken);
+}
+
+int32_t vx_scene_get_bond_state(vx_scene* s, float* plastic, float* damage, float* eqp, float* fatigue) {
+    clear_error();
+    if (!s) return VX_BAD_INPUT;
+    cudaSetDevice(s->device);
+    const size_t m = 3 * (size_t)s->n;
+    std::vector<float4> a(m), b(m), c(m);
+    if (m) {
+        VX_TRY(cudaMemcpyAsync(a.data(), s->bond_a, m * sizeof(float4), cudaMemcpyDeviceToHost, s->stream), "bonds");
+        VX_TRY(cudaMemcpyAsync(b.data(), s->bond_b, m * sizeof(float4), cudaMemcpyDeviceToHost, s->stream), "bonds");
+        VX_TRY(cudaMemcpyAsync(c.data(), s->bond_c, m * sizeof(float4), cudaMemcpyDeviceToHost, s->stream), "bonds");
+        VX_TRY(cudaStreamSynchronize(s->stream), "bonds");
+    }
+    for (size_t e = 0; e < m; ++e) {
+        if (plastic) plastic[3 * e] = b[e].x, plastic[3 * e + 1] = b[e].y, plastic[3 * e + 2] = b[e].z;
+        if (damage) damage[e] = a[e].w;
+        if (eqp) eqp[e] = b[e].w;
+        if (fatigue) fatigue[e] = c[e].y;
+    }
     return VX_OK;
 }
 

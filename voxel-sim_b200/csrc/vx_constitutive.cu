@@ -11,6 +11,7 @@
 #include "vx_device.cuh"
 #include "vx_kernels.h"
 #include "vx_layout.cuh"
+#include "vx_reduce.cuh"
 
 namespace vx {
 
@@ -349,6 +350,131 @@ cudaError_t launch_bond_stress(vx_scene* s, float* d_ratio, float* d_force, uint
     if (m == 0) return cudaGetLastError();
     k_bond_stress<<<(unsigned)((m + 255) / 256), 256, 0, s->stream>>>(view_of(s), s->bonds, d_ratio, d_force,
                                                                        d_near, cap, s->near_count);
+    return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Fracture stage (src/solver.rs:600-665 with fracture::update, src/fracture.rs:
+// 186-292), in FP64 on the bond state the reference keeps in f32.
+struct FractureCfg {
+    double damage_rate, energy_release, fatigue_cycles, fatigue_exponent, fatigue_threshold, plastic_heat_fraction;
+};
+
+__device__ __forceinline__ double bond_energy(v3 u, const sym6& K, double damage) {  // energy, :186-188
+    return fmax(0.5 * (1.0 - damage) * dot(u, mul(K, u)), 0.0);
+}
+
+__global__ void k_fracture_commit(SceneView s, BondArrays b, float4* __restrict__ bond_a, float4* __restrict__ bond_b,
+                                  float4* __restrict__ bond_c, float* __restrict__ bond_d, uint32_t* __restrict__ nbr,
+                                  double dt, FractureCfg c, double* __restrict__ partials, uint32_t* __restrict__ counter,
+                                  double* __restrict__ totals) {
+    const uint32_t n = s.n;
+    const size_t m3n = 3 * (size_t)n;
+    const size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // plastic heat, stored plastic, surface work, damage heat, released
+    if (e < m3n) {
+        const int a = (int)(e / n);
+        const uint32_t i = (uint32_t)(e - (size_t)a * n);
+        const uint32_t j = nbr[e];
+        if (tile_active(s.tile_on, i) && b.state[e] != 0 && j != VX_EMPTY_U32 && !s.kin[i]) {
+            const double4 q = b.frame_q[e];
+            const m3 F = basis(a, quat{q.x, q.y, q.z, q.w});
+            sym6 K;
+#pragma unroll
+            for (int t = 0; t < 6; ++t) K.s[t] = b.mat_k[t * m3n + e];
+            const Limits l = bond_limits(s, i, j, F.c[0]);
+            const v3 xi = load3(s.pos, n, i), xj = load3(s.pos, n, j);
+            float4 ba = bond_a[e], bb = bond_b[e], bc = bond_c[e];
+            const v3 u_total = mul_t(F, xj - xi) - thermal_rest(s, i, j, F) - mk(ba.x, ba.y, ba.z);
+            v3 plastic = mk(bb.x, bb.y, bb.z);
+            double eqp = bb.w, damage = ba.w, work = bc.x, fatigue = bc.y, prev = bc.z, reversal = bc.w;
+            double increment = bond_d[e];
+            const double old_damage = damage;
+            v3 u = u_total - plastic * kCell;
+            const double before = bond_energy(u, K, old_damage);
+            if (l.ductility > 1e-5) {  // return map, :226-243
+                const v3 ku0 = mul(K, u);
+                const v3 trial = mk(ku0.x / kArea, ku0.y / kArea, ku0.z / kArea);
+                const double equivalent = sqrt(dot(trial, trial));
+                const double yield_now = l.yield_stress + l.hardening * eqp;
+                if (equivalent > yield_now) {
+                    const v3 dir = mk(trial.x / equivalent * kArea, trial.y / equivalent * kArea,
+                                      trial.z / equivalent * kArea);
+                    v3 cd = mul(inverse(K), dir);
+                    cd = mk(cd.x / kCell, cd.y / kCell, cd.z / kCell);
+                    const double modulus = 1.0 / fmax(sqrt(dot(cd, cd)), 1e-20);
+                    const double dep = (equivalent - yield_now) / (modulus + l.hardening) * l.ductility;
+                    plastic = plastic + normalize_or_zero(cd) * dep;
+                    eqp += dep;
+                    u = u_total - plastic * kCell;
+                    const double lost = fmax(before - bond_energy(u, K, old_damage), 0.0);
+                    work += lost;
+                    v[0] = lost * c.plastic_heat_fraction;
+                    v[1] = lost - v[0];
+                }
+            }
+            const v3 ku = mul(K, u);  // failure after the return map, :244-254
+            const v3 stress = mk(ku.x / kArea, ku.y / kArea, ku.z / kArea);
+            const double normal_limit = stress.x >= 0.0 ? l.tension : l.compression;
+            const double r0 = stress.x / fmax(normal_limit, 1.0);
+            const double sh = fmax(l.shear, 1.0);
+            const double ratio = sqrt(r0 * r0 + (stress.y * stress.y + stress.z * stress.z) / (sh * sh));
+            const double ax = fabs(stress.x), ay = fabs(stress.y), az = fabs(stress.z);
+            const double principal = ax >= fmax(ay, az) ? stress.x : (ay >= az ? stress.y : stress.z);
+            const double signed_ratio = copysign(ratio, principal);  // fatigue, :190-207
+            const double delta = signed_ratio - prev;
+            if (fabs(delta) > 1e-6) {
+                if (increment * delta < 0.0) {
+                    const double amplitude = fabs(prev - reversal) * 0.5;
+                    if (amplitude > c.fatigue_threshold) {
+                        const double level = fmin((amplitude - c.fatigue_threshold) / (1.0 - c.fatigue_threshold), 1.0);
+                        fatigue = fmin(fatigue + 0.5 * pow(level, c.fatigue_exponent) / c.fatigue_cycles, 1.0);
+                    }
+                    reversal = prev;
+                }
+                increment = delta;
+            }
+            prev = signed_ratio;
+            if (ratio >= 1.0) {  // damage, :265-277
+                if (l.ductility <= 1e-5) damage = 1.0;
+                else damage = fmin(damage + c.damage_rate * dt * fmin(ratio, 10.0), 1.0);
+            }
+            if (l.ductility > 1e-5 && eqp >= fmax(l.plastic_failure, 1e-6)) damage = fmin(damage + c.damage_rate * dt, 1.0);
+            if (fatigue >= 1.0) damage = 1.0;
+            const double lost = fmax(bond_energy(u, K, old_damage) - bond_energy(u, K, damage), 0.0);  // :280-288
+            const double budget = l.fracture_energy * kArea * (damage - old_damage);
+            v[2] = fmin(lost, budget);
+            const double available = lost - v[2];
+            v[4] = available * c.energy_release;
+            v[3] = available - v[4];
+            bond_a[e] = make_float4(ba.x, ba.y, ba.z, (float)damage);
+            bond_b[e] = make_float4((float)plastic.x, (float)plastic.y, (float)plastic.z, (float)eqp);
+            bond_c[e] = make_float4((float)work, (float)fatigue, (float)prev, (float)reversal);
+            bond_d[e] = (float)increment;
+            if (damage >= 1.0) {
+                nbr[e] = VX_EMPTY_U32;
+                atomicAdd(counter + 1, 1u);
+            }
+        }
+    }
+    if (grid_sum<5>(v, partials, counter) && threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 5; ++k) totals[k] = v[k];
+    }
+}
+
+cudaError_t launch_fracture_commit(vx_scene* s, double dt, const vx_fracture_config* cfg) {
+    const size_t m = 3 * (size_t)s->n;
+    cudaError_t e = cudaMemsetAsync(s->frac_counter, 0, 2 * sizeof(uint32_t), s->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->frac_totals, 0, 8 * sizeof(double), s->stream);
+    if (e != cudaSuccess || m == 0) return e;
+    FractureCfg c{cfg->damage_rate, cfg->energy_release, cfg->fatigue_cycles, cfg->fatigue_exponent,
+                  cfg->fatigue_threshold, cfg->plastic_heat_fraction};
+    const unsigned grid = (unsigned)((m + kThreads - 1) / kThreads);
+    k_fracture_commit<<<grid, kThreads, 0, s->stream>>>(view_of(s), s->bonds, s->bond_a, s->bond_b, s->bond_c,
+                                                        s->bond_d, s->nbr, dt, c, s->frac_partials, s->frac_counter,
+                                                        s->frac_totals);
     return cudaGetLastError();
 }
 

@@ -92,6 +92,11 @@ struct vx_scene {
     uint32_t* rev;                // [3][n]
     float4* bond_a;               // [3n] formation xyz, damage
     float4* bond_b;               // [3n] plastic xyz, equivalent plastic strain
+    float4* bond_c;               // [3n] plastic work, fatigue damage, previous / reversal stress ratio
+    float* bond_d;                // [3n] loading increment (fatigue)
+    double* frac_partials;        // [5 * 3 * blocks] block partials of the dissipation
+    double* frac_totals;          // [8] dissipation totals of the last fracture stage
+    uint32_t* frac_counter;       // [2] last-block ticket, bonds broken
 
     vx::BondArrays bonds;
 

@@ -55,6 +55,11 @@ cudaError_t launch_velocity_update(vx_scene* s, uint32_t count, const uint32_t* 
 cudaError_t launch_gather3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* field, double* d_out);
 cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
                             double* field);
+// fracture stage: fracture::update on every bond of the last assembly (dt = substep)
+cudaError_t launch_fracture_commit(vx_scene* s, double dt, const vx_fracture_config* cfg);
+// fracture stage plus the reverse-table rebuild when bonds broke (vx_capi.cu)
+int32_t fracture_stage(vx_scene* s, double dt, const vx_fracture_config* cfg, vx_dissipation* out,
+                       uint32_t* out_broken);
 // bond stress / ratio / force
 cudaError_t launch_bond_stress(vx_scene* s, float* d_ratio, float* d_force, uint32_t* d_near, uint32_t cap);
 

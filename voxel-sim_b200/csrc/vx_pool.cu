@@ -732,6 +732,8 @@ int32_t vx_pool_add(vx_pool* p, const vx_scene_desc* d, uint32_t* out_slot) {
             e = cudaMemcpyAsync(s->pred + c * C + base, pos.data() + c * m, m * 8, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->loads + c * C + base, 0, m * 8, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->vel + c * C + base, 0, m * 8, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->bond_c + c * C + base, 0, m * sizeof(float4), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->bond_d + c * C + base, 0, m * sizeof(float), st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->nbr + c * C + base, nbr.data() + c * m, m * 4, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
@@ -1109,6 +1111,14 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
         }
         r = pool_select(p, on.data(), sel);
         if (r != VX_OK) return r;
+        if (prm->fracture) {  // one stage over every selected slot; totals are pool-wide
+            vx_dissipation d{};
+            uint32_t broken = 0;
+            r = fracture_stage(&p->s, h, &prm->fracture_config, &d, &broken);
+            if (r != VX_OK) return r;
+            for (uint32_t k = 0; k < S; ++k)
+                if (on[k]) st[k].broken += broken;
+        }
         VX_POOL_TRY(launch_velocity(&p->s, h), "pool velocity update");
         VX_POOL_TRY(cudaStreamSynchronize(p->s.stream), "pool step");
     }

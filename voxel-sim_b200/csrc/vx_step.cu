@@ -205,6 +205,18 @@ extern "C" int32_t vx_scene_step(vx_scene* s, const vx_step_params* p, vx_step_s
             st.max_angle = angle;
             if (angle <= p->corotation_tolerance && st.residual <= p->pass.tolerance) break;
         }
+        if (p->fracture) {
+            vx_dissipation d{};
+            uint32_t broken = 0;
+            r = fracture_stage(s, h, &p->fracture_config, &d, &broken);
+            if (r != VX_OK) return r;
+            st.broken += broken;
+            st.dissipation.plastic_heat += d.plastic_heat;
+            st.dissipation.stored_plastic += d.stored_plastic;
+            st.dissipation.surface_work += d.surface_work;
+            st.dissipation.damage_heat += d.damage_heat;
+            st.dissipation.released += d.released;
+        }
         e = launch_velocity(s, h);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) {

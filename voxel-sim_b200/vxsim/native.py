@@ -66,17 +66,42 @@ class VxPassStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class VxFractureConfig(C.Structure):
+    _fields_ = [("damage_rate", C.c_double), ("energy_release", C.c_double), ("fatigue_cycles", C.c_double),
+                ("fatigue_exponent", C.c_double), ("fatigue_threshold", C.c_double),
+                ("plastic_heat_fraction", C.c_double)]
+
+
+def fracture_config(damage_rate=35.0, energy_release=0.005, fatigue_cycles=1000.0, fatigue_exponent=3.0,
+                    fatigue_threshold=0.5, plastic_heat_fraction=0.9) -> VxFractureConfig:
+    """FractureConfig::default (src/fracture.rs:27-42)."""
+    return VxFractureConfig(damage_rate, energy_release, fatigue_cycles, fatigue_exponent, fatigue_threshold,
+                            plastic_heat_fraction)
+
+
+class VxDissipation(C.Structure):
+    _fields_ = [("plastic_heat", C.c_double), ("stored_plastic", C.c_double), ("surface_work", C.c_double),
+                ("damage_heat", C.c_double), ("released", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class VxStepParams(C.Structure):
     _fields_ = [("fixed_dt", C.c_double), ("substeps", C.c_uint32), ("corotation_iterations", C.c_uint32),
-                ("corotation_tolerance", C.c_double), ("gravity", C.c_double * 3), ("pass_", VxPassParams)]
+                ("corotation_tolerance", C.c_double), ("gravity", C.c_double * 3), ("pass_", VxPassParams),
+                ("fracture", C.c_int32), ("fracture_config", VxFractureConfig)]
 
 
 class VxStepStats(C.Structure):
     _fields_ = [("passes", C.c_uint32), ("pcg_iterations", C.c_uint32), ("residual", C.c_double),
-                ("max_angle", C.c_double), ("converged", C.c_int32)]
+                ("max_angle", C.c_double), ("converged", C.c_int32), ("broken", C.c_uint32),
+                ("dissipation", VxDissipation)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["dissipation"] = self.dissipation.as_dict()
+        return d
 
 
 class VxServerConfig(C.Structure):
@@ -111,10 +136,11 @@ class VxServerStats(C.Structure):
 
 def step_params(fixed_dt, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5, gravity=(0.0, 0.0, 0.0),
                 tolerance=1e-5, max_iterations=10000, precision=PRECISION_FP64, reuse=False, inner_tolerance=0.0,
-                max_outer=0, kernel=KERNEL_AUTO) -> VxStepParams:
+                max_outer=0, kernel=KERNEL_AUTO, fracture=False, fracture_cfg=None) -> VxStepParams:
     return VxStepParams(fixed_dt, substeps, corotation_iterations, corotation_tolerance, (C.c_double * 3)(*gravity),
                         VxPassParams(fixed_dt / substeps, tolerance, max_iterations, precision, int(reuse),
-                                     inner_tolerance, max_outer, kernel))
+                                     inner_tolerance, max_outer, kernel),
+                        int(fracture), fracture_cfg or fracture_config())
 
 
 _lib = None
@@ -161,6 +187,9 @@ def load(path: Path | None = None):
     L.vx_scene_stream.argtypes = [C.c_void_p]
     L.vx_scene_kernel_times.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, C.c_void_p, C.c_uint64, f64p]
     L.vx_scene_step.argtypes = [C.c_void_p, C.POINTER(VxStepParams), C.POINTER(VxStepStats)]
+    L.vx_fracture_commit.argtypes = [C.c_void_p, C.c_double, C.POINTER(VxFractureConfig), C.POINTER(VxDissipation),
+                                     C.POINTER(C.c_uint32)]
+    L.vx_scene_get_bond_state.argtypes = [C.c_void_p, f32p, f32p, f32p, f32p]
     L.vx_server_create.argtypes = [C.c_void_p, C.POINTER(VxServerConfig), C.POINTER(C.c_void_p)]
     L.vx_server_submit.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), u8p, f64p, C.POINTER(VxRequestPlan),
                                    C.POINTER(C.c_uint64)]
@@ -357,6 +386,20 @@ class DeviceScene:
         d = st.as_dict()
         d["status"] = status
         return d
+
+    def fracture_commit(self, dt, cfg=None):
+        d, broken = VxDissipation(), C.c_uint32()
+        check(load().vx_fracture_commit(self.h, dt, C.byref(cfg or fracture_config()), C.byref(d), C.byref(broken)))
+        return d.as_dict(), broken.value
+
+    def bond_state(self):
+        m = 3 * self.n
+        pl, dm, ep, fa = (np.zeros(3 * m, np.float32), np.zeros(m, np.float32), np.zeros(m, np.float32),
+                          np.zeros(m, np.float32))
+        check(load().vx_scene_get_bond_state(self.h, _p(pl, C.c_float), _p(dm, C.c_float), _p(ep, C.c_float),
+                                             _p(fa, C.c_float)))
+        return dict(plastic=pl.reshape(3, -1, 3), damage=dm.reshape(3, -1), eq_plastic=ep.reshape(3, -1),
+                    fatigue=fa.reshape(3, -1))
 
     def set_velocities(self, v):
         v = self._vec(v)
