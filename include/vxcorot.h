@@ -304,6 +304,13 @@ typedef struct vx_dissipation {
  */
 int32_t vx_fracture_commit(vx_scene* scene, double dt, const vx_fracture_config* config, vx_dissipation* out,
                            uint32_t* out_broken);
+/*
+ * rebuild_clusters (src/solver.rs:828-858) on the device: connected components
+ * of the bond graph. clusters[n] (or NULL) receives each REV's cluster id,
+ * numbered as the reference numbers them (in order of each component's first
+ * non-kinematic REV), VX_EMPTY for kinematic REVs; out_count the cluster count.
+ */
+int32_t vx_scene_rebuild_clusters(vx_scene* scene, uint32_t* clusters, uint32_t* out_count);
 /* Per-bond fracture state, axis-major: plastic_strain[9n] ((axis*n+i)*3+c), damage[3n],
    equivalent_plastic_strain[3n], fatigue_damage[3n]; any may be NULL. */
 int32_t vx_scene_get_bond_state(vx_scene* scene, float* plastic_strain, float* damage,

@@ -409,3 +409,14 @@ class OracleStepper:
 
     def last_forces(self):
         return self.last_force.reshape(3, self.o.n, 3)
+
+
+def rebuild_clusters(neighbor, kinematic):
+    """vxo_rebuild_clusters: (clusters[n], cluster_count)."""
+    nb = np.ascontiguousarray(neighbor, np.uint32).reshape(-1)
+    kin = np.ascontiguousarray(kinematic, np.uint8)
+    n = len(kin)
+    out = np.zeros(max(n, 1), np.uint32)
+    lib().vxo_rebuild_clusters.restype = C.c_uint32
+    cnt = lib().vxo_rebuild_clusters(n, ptr(nb, C.c_uint32), ptr(kin, C.c_uint8), ptr(out, C.c_uint32))
+    return out[:n].copy(), int(cnt)

@@ -1364,3 +1364,42 @@ int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d) {
     free(factor);
     return 0;
 }
+
+/* ---- rebuild_clusters (src/solver.rs:828-858) ---------------------------- */
+static uint32_t cluster_root(uint32_t* parent, uint32_t i) {
+    while (parent[i] != i) {
+        parent[i] = parent[parent[i]];
+        i = parent[i];
+    }
+    return i;
+}
+
+uint32_t vxo_rebuild_clusters(uint32_t n, const uint32_t* neighbor, const uint8_t* kinematic, uint32_t* clusters) {
+    uint32_t* parent = (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t));
+    uint32_t* ids = (uint32_t*)malloc((n ? n : 1) * sizeof(uint32_t));
+    for (uint32_t i = 0; i < n; ++i) {
+        parent[i] = i;
+        ids[i] = VX_EMPTY;
+    }
+    for (int a = 0; a < 3; ++a)
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t j = neighbor[(size_t)a * n + i];
+            if (j == VX_EMPTY) continue;
+            uint32_t ra = cluster_root(parent, i), rc = cluster_root(parent, j);
+            parent[rc] = ra;
+        }
+    /* the HashMap of the reference hands out ids in first-seen order */
+    uint32_t count = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (kinematic[i]) {
+            clusters[i] = VX_EMPTY;
+            continue;
+        }
+        uint32_t r = cluster_root(parent, i);
+        if (ids[r] == VX_EMPTY) ids[r] = count++;
+        clusters[i] = ids[r];
+    }
+    free(parent);
+    free(ids);
+    return count;
+}

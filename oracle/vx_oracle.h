@@ -182,6 +182,11 @@ typedef struct vxo_dynamics {
 
 int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d);
 
+/* rebuild_clusters (src/solver.rs:828-858): union-find over every bond with a
+   neighbour; non-kinematic REVs get ids in the order their components first
+   appear by REV index, kinematic REVs VX_EMPTY. Returns cluster_count. */
+uint32_t vxo_rebuild_clusters(uint32_t n, const uint32_t* neighbor, const uint8_t* kinematic, uint32_t* clusters);
+
 #ifdef __cplusplus
 }
 #endif

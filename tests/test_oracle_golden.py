@@ -388,3 +388,54 @@ def test_topology_matches_dense_lattice_rule():
     O.lib().vxo_build_topology(O.ptr(np.ascontiguousarray(cells, np.int32), O.C.c_int32),
                                O.ptr(kin, O.C.c_uint8), len(cells), O.ptr(nbr_c, O.C.c_uint32))
     assert np.array_equal(nbr_py.reshape(-1), nbr_c)
+
+
+def test_cluster_numbering_follows_the_reference_test():
+    """connecting_adjacent_revs_rebuilds_topology_and_accepts_either_order
+    (src/scene.rs:2082-2103): a fixed and a free iron REV are not bonded (one
+    cluster); once released there are two; bonded, one again."""
+    empty = np.full(6, 0xFFFFFFFF, np.uint32)
+    cl, cnt = O.rebuild_clusters(empty, np.array([1, 0], np.uint8))
+    assert cnt == 1 and list(cl) == [0xFFFFFFFF, 0]
+    cl, cnt = O.rebuild_clusters(empty, np.array([0, 0], np.uint8))
+    assert cnt == 2 and list(cl) == [0, 1]
+    bonded = empty.copy()
+    bonded[0] = 1  # bonds[0][0].neighbor = 1
+    cl, cnt = O.rebuild_clusters(bonded, np.array([0, 0], np.uint8))
+    assert cnt == 1 and list(cl) == [0, 0]
+
+
+def test_cluster_ids_agree_with_a_breadth_first_restatement():
+    """On a lattice with 60% of its bonds removed, the union-find numbering
+    equals components found by breadth-first search, numbered by first
+    non-kinematic REV."""
+    rng = np.random.default_rng(3)
+    s = S.wood_cube(8)
+    nb = s.neighbor.copy()
+    nb[rng.random(nb.shape) < 0.6] = 0xFFFFFFFF
+    n = s.n
+    adj = [[] for _ in range(n)]
+    for a in range(3):
+        for i in range(n):
+            j = int(nb[a, i])
+            if j != 0xFFFFFFFF:
+                adj[i].append(j)
+                adj[j].append(i)
+    comp = [-1] * n
+    for i in range(n):
+        if comp[i] < 0:
+            comp[i], todo = i, [i]
+            while todo:
+                x = todo.pop()
+                for y in adj[x]:
+                    if comp[y] < 0:
+                        comp[y] = i
+                        todo.append(y)
+    ids, want = {}, []
+    for i in range(n):
+        if s.kinematic[i]:
+            want.append(0xFFFFFFFF)
+        else:
+            want.append(ids.setdefault(comp[i], len(ids)))
+    cl, cnt = O.rebuild_clusters(nb, s.kinematic)
+    assert list(cl) == want and cnt == len(ids) and cnt > 5

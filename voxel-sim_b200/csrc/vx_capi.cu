@@ -54,6 +54,13 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->frac_partials = A.take<double>(5 * 3 * (size_t)blocks);
     s->frac_totals = A.take<double>(8);
     s->frac_counter = A.take<uint32_t>(2);
+    s->clusters = A.take<uint32_t>(m);
+    s->cl_parent = A.take<uint32_t>(m);
+    s->cl_root = A.take<uint32_t>(m);
+    s->cl_first = A.take<uint32_t>(m);
+    s->cl_scan = A.take<uint32_t>(m);
+    s->cl_bsum = A.take<uint32_t>(m / 1024 + 2);
+    s->cl_err = A.take<uint32_t>(1);
     s->bonds.k64 = A.take<double>(18 * m);
     s->bonds.k32 = A.take<float>(18 * (size_t)kstride32((uint32_t)m));
     s->bonds.mat_k = A.take<double>(18 * m);

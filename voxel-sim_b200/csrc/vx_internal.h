@@ -97,6 +97,13 @@ struct vx_scene {
     double* frac_partials;        // [5 * 3 * blocks] block partials of the dissipation
     double* frac_totals;          // [8] dissipation totals of the last fracture stage
     uint32_t* frac_counter;       // [2] last-block ticket, bonds broken
+    uint32_t* clusters;           // [n] cluster id per REV (VX_EMPTY for kinematic REVs)
+    uint32_t* cl_parent;          // [n] union-find parents
+    uint32_t* cl_root;            // [n] component root (smallest REV)
+    uint32_t* cl_first;           // [n] per root: first non-kinematic REV
+    uint32_t* cl_scan;            // [n] exclusive scan of first-REV flags within a scan block
+    uint32_t* cl_bsum;            // [n / 1024 + 2] scan-block totals, then the cluster count
+    uint32_t* cl_err;             // [1] a union exceeded its retry bound
 
     vx::BondArrays bonds;
 

@@ -55,6 +55,9 @@ cudaError_t launch_velocity_update(vx_scene* s, uint32_t count, const uint32_t* 
 cudaError_t launch_gather3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* field, double* d_out);
 cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
                             double* field);
+// connected components of the bond graph with the reference's cluster numbering (vx_clusters.cu)
+cudaError_t launch_rebuild_clusters(vx_scene* s);
+uint32_t cluster_scan_blocks(uint32_t n);
 // fracture stage: fracture::update on every bond of the last assembly (dt = substep)
 cudaError_t launch_fracture_commit(vx_scene* s, double dt, const vx_fracture_config* cfg);
 // fracture stage plus the reverse-table rebuild when bonds broke (vx_capi.cu)

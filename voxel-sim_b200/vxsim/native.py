@@ -190,6 +190,7 @@ def load(path: Path | None = None):
     L.vx_fracture_commit.argtypes = [C.c_void_p, C.c_double, C.POINTER(VxFractureConfig), C.POINTER(VxDissipation),
                                      C.POINTER(C.c_uint32)]
     L.vx_scene_get_bond_state.argtypes = [C.c_void_p, f32p, f32p, f32p, f32p]
+    L.vx_scene_rebuild_clusters.argtypes = [C.c_void_p, u32p, C.POINTER(C.c_uint32)]
     L.vx_server_create.argtypes = [C.c_void_p, C.POINTER(VxServerConfig), C.POINTER(C.c_void_p)]
     L.vx_server_submit.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), u8p, f64p, C.POINTER(VxRequestPlan),
                                    C.POINTER(C.c_uint64)]
@@ -391,6 +392,13 @@ class DeviceScene:
         d, broken = VxDissipation(), C.c_uint32()
         check(load().vx_fracture_commit(self.h, dt, C.byref(cfg or fracture_config()), C.byref(d), C.byref(broken)))
         return d.as_dict(), broken.value
+
+    def rebuild_clusters(self):
+        """(clusters[n], cluster_count) as rebuild_clusters numbers them."""
+        out = np.zeros(max(self.n, 1), np.uint32)
+        cnt = C.c_uint32()
+        check(load().vx_scene_rebuild_clusters(self.h, _p(out, C.c_uint32), C.byref(cnt)))
+        return out[:self.n].copy(), cnt.value
 
     def bond_state(self):
         m = 3 * self.n
