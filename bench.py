@@ -208,6 +208,20 @@ def reference_arm(args):
     return 0
 
 
+def combine_ranks(ms, dof_iters, solves, dist=None, device="cpu"):
+    """Whole-job figures of the replica run: the device time is the maximum over
+    ranks (every rank's timed region ends at a barrier), the work the sum. Each
+    rank takes the same two collectives in the same order."""
+    if dist is None:
+        return ms, dof_iters, solves
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w = torch.tensor([dof_iters, solves], device=device, dtype=torch.float64)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(w[0].item()), float(w[1].item())
+
+
 def our_arm(args):
     import torch
     from vxsim import native as N
@@ -287,15 +301,8 @@ def our_arm(args):
 
     # aggregate: max device time over ranks, summed work
     dof_iters = float(free_dof) * total_it
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        w_ = torch.tensor([dof_iters, float(passes * args.steps)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(w_, op=dist.ReduceOp.SUM)
-        job_ms = float(t.item())
-        job_dof_iters, job_solves = float(w_[0].item()), float(w_[1].item())
-    else:
-        job_ms, job_dof_iters, job_solves = total_ms, dof_iters, float(passes * args.steps)
+    job_ms, job_dof_iters, job_solves = combine_ranks(total_ms, dof_iters, float(passes * args.steps),
+                                                      dist, "cuda")
     value = job_dof_iters / (job_ms / 1000.0)
 
     # kernel roofline, CUDA events on the scene stream (cold: L2 flushed before the launch)
