@@ -272,6 +272,10 @@ def our_arm(args):
         launches += 1
         return it, launches, worst
 
+    # one step assembles the system, the autotuner picks the inner-solve launch
+    # configuration from it, then the warm-up steps run with that choice
+    step()
+    tuning = ds.autotune(precision)
     for _ in range(args.warmup):
         step()
 
@@ -402,6 +406,9 @@ def our_arm(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": total_launch,
+            "tuning": {"kernel": "persistent" if tuning["kernel"] == N.KERNEL_PERSISTENT else "streaming",
+                       "blocks_per_sm": tuning["blocks_per_sm"], "us_per_iteration": tuning["us_per_iteration"],
+                       "candidates_us": [round(c[2], 2) for c in tuning["candidates"]]},
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -522,6 +522,29 @@ void* vx_scene_stream(vx_scene* scene);
  * out_us[2] = its time per iteration (one launch of out_us[3] iterations),
  * else both are 0. out_us has four entries.
  */
+/*
+ * Autotuner (no counterpart in the reference). After a pass has assembled the
+ * scene, times a 64-iteration inner solve of the given precision for every
+ * candidate launch configuration and keeps the fastest for the scene's later
+ * passes (VX_KERNEL_AUTO follows it): the streaming kernels with a register
+ * budget of 3, 4 or 5 blocks of 256 threads per SM, and for MIXED the
+ * persistent kernel when the scene fits. With cache_path (or NULL), a choice
+ * found there for this GPU, precision and scene size (log2 of the REV count)
+ * is applied without timing, and a new choice is stored. Positions and bond
+ * state are not changed; the solver's work vectors are.
+ */
+typedef struct vx_tune_result {
+    int32_t kernel;               /* VX_KERNEL_STREAMING or VX_KERNEL_PERSISTENT */
+    int32_t blocks_per_sm;        /* register budget of the streaming kernels */
+    double us_per_iteration;      /* of the chosen configuration */
+    int32_t from_cache;           /* 1: read from cache_path, nothing timed */
+    uint32_t candidates;          /* timed configurations (at most 8) */
+    int32_t candidate_kernel[8];
+    int32_t candidate_blocks[8];
+    double candidate_us[8];
+} vx_tune_result;
+int32_t vx_scene_autotune(vx_scene* scene, int32_t precision, const char* cache_path, vx_tune_result* out);
+
 int32_t vx_scene_kernel_times(vx_scene* scene, int32_t precision, uint32_t reps, void* flush,
                               uint64_t flush_bytes, double* out_us);
 

@@ -43,6 +43,7 @@ int main(void) {{
          offsetof(vx_step_params, pass), sizeof(vx_step_stats));
   printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(vx_server_config), sizeof(vx_request_plan), sizeof(vx_request_result),
          sizeof(vx_server_stats), sizeof(vx_fracture_config), sizeof(vx_dissipation));
+  printf("%zu\\n", sizeof(vx_tune_result));
   return 0;
 }}''')
     exe = tmp_path / "layout"
@@ -52,7 +53,7 @@ int main(void) {{
             N.VxSceneDesc.neighbor.offset, C.sizeof(N.VxStepParams), N.VxStepParams.pass_.offset,
             C.sizeof(N.VxStepStats), C.sizeof(N.VxServerConfig), C.sizeof(N.VxRequestPlan),
             C.sizeof(N.VxRequestResult), C.sizeof(N.VxServerStats), C.sizeof(N.VxFractureConfig),
-            C.sizeof(N.VxDissipation)]
+            C.sizeof(N.VxDissipation), C.sizeof(N.VxTuneResult)]
     assert got == want
 
 

@@ -821,6 +821,99 @@ int32_t vx_scene_checkpoint(vx_scene* s, int32_t op) {
 
 void* vx_scene_stream(vx_scene* s) { return s ? (void*)s->stream : nullptr; }
 
+// One cache line per choice: "<gpu> <sms> <precision> <log2 n> <kernel> <blocks> <us>".
+static std::string tune_key(vx_scene* s, int32_t precision) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, s->device);
+    std::string name = prop.name;
+    for (char& c : name)
+        if (c == ' ' || c == '\t') c = '_';
+    int bucket = 0;
+    for (uint32_t v = s->n; v > 1; v >>= 1) ++bucket;
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s %d %d %d", name.c_str(), s->sm_count, precision, bucket);
+    return buf;
+}
+
+int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path, vx_tune_result* out) {
+    clear_error();
+    if (!s || !out || (precision != VX_PRECISION_FP64 && precision != VX_PRECISION_MIXED)) {
+        set_error("vx_scene_autotune: bad argument");
+        return VX_BAD_INPUT;
+    }
+    if (!s->assembled || s->n == 0) {
+        set_error("vx_scene_autotune: run a pass first (the tuner times the assembled system)");
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(s->device);
+    std::memset(out, 0, sizeof *out);
+    const std::string key = tune_key(s, precision);
+    std::vector<std::string> lines;
+    if (cache_path) {
+        if (FILE* f = std::fopen(cache_path, "r")) {
+            char line[512];
+            while (std::fgets(line, sizeof line, f)) {
+                std::string l(line);
+                while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+                if (l.empty()) continue;
+                if (l.compare(0, key.size() + 1, key + " ") == 0) {
+                    int kernel = 0, blocks = 0;
+                    double us = 0.0;
+                    if (std::sscanf(l.c_str() + key.size() + 1, "%d %d %lf", &kernel, &blocks, &us) == 3 &&
+                        (kernel == VX_KERNEL_STREAMING || (kernel == VX_KERNEL_PERSISTENT && persistent_plan(s))) &&
+                        blocks >= 3 && blocks <= 5) {
+                        std::fclose(f);
+                        apply_tuning(s, kernel, blocks);
+                        out->kernel = kernel;
+                        out->blocks_per_sm = blocks;
+                        out->us_per_iteration = us;
+                        out->from_cache = 1;
+                        return VX_OK;
+                    }
+                    continue;  // a stale entry for this key is dropped
+                }
+                lines.push_back(l);
+            }
+            std::fclose(f);
+        }
+    }
+    struct Cand {
+        int32_t kernel;
+        int blocks;
+    };
+    std::vector<Cand> cands = {{VX_KERNEL_STREAMING, 3}, {VX_KERNEL_STREAMING, 4}, {VX_KERNEL_STREAMING, 5}};
+    if (precision == VX_PRECISION_MIXED && persistent_plan(s)) cands.push_back({VX_KERNEL_PERSISTENT, 4});
+    const int old_blocks = s->pcg_minb;
+    int best = -1;
+    for (size_t k = 0; k < cands.size(); ++k) {
+        double us = 0.0;
+        int32_t r = time_candidate(s, precision, cands[k].kernel, cands[k].blocks, &us);
+        if (r != VX_OK) {
+            apply_tuning(s, -1, old_blocks);
+            return r;
+        }
+        out->candidate_kernel[k] = cands[k].kernel;
+        out->candidate_blocks[k] = cands[k].blocks;
+        out->candidate_us[k] = us;
+        out->candidates = (uint32_t)(k + 1);
+        if (best < 0 || us < out->candidate_us[best]) best = (int)k;
+    }
+    apply_tuning(s, cands[best].kernel, cands[best].blocks);
+    out->kernel = cands[best].kernel;
+    out->blocks_per_sm = cands[best].blocks;
+    out->us_per_iteration = out->candidate_us[best];
+    if (cache_path) {
+        if (FILE* f = std::fopen(cache_path, "w")) {
+            for (const std::string& l : lines) std::fprintf(f, "%s\n", l.c_str());
+            std::fprintf(f, "%s %d %d %.3f\n", key.c_str(), out->kernel, out->blocks_per_sm, out->us_per_iteration);
+            std::fclose(f);
+        } else {
+            set_error("vx_scene_autotune: cannot write %s (the choice is applied, not stored)", cache_path);
+        }
+    }
+    return VX_OK;
+}
+
 int32_t vx_scene_kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush, uint64_t flush_bytes,
                               double* out_us) {
     clear_error();

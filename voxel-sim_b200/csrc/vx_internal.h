@@ -162,6 +162,8 @@ struct vx_scene {
     uint32_t launches = 0;        // kernels launched by the current pass
     int sm_count = 148;           // SMs of the scene's GPU
     unsigned grid32 = 0;          // grid of the FP32 / FP64 PCG kernels (0 = not yet chosen)
+    int pcg_minb = 4;             // register budget of the streaming kernels: blocks per SM (3, 4 or 5)
+    int tuned_kernel = -1;        // inner kernel chosen by the autotuner (-1 = none)
     unsigned grid64 = 0;
     // persistent (on-chip) inner solve plan
     bool persist_checked = false;

@@ -75,6 +75,9 @@ bool persistent_plan(vx_scene* s);
 int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations);
 // |b - A x64| / |b| with the FP64 operator (device scalars updated)
 int32_t true_residual(vx_scene* s, double* out);
+// autotuning: time one candidate (microseconds per inner iteration) and apply a choice (vx_pcg.cu)
+int32_t time_candidate(vx_scene* s, int32_t precision, int32_t kernel, int mb, double* us);
+void apply_tuning(vx_scene* s, int32_t kernel, int mb);
 // CUDA-event timing of the matvec and update kernels (microseconds per launch)
 int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush, uint64_t flush_bytes,
                      double* out_us);

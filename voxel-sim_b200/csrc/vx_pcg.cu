@@ -86,13 +86,13 @@ __global__ void __launch_bounds__(kThreads) k_init(IterArgs<T> a, const double* 
 
 // Iteration k (PAR = k & 1): convergence test of iteration k-1, beta, then
 // p_new = z + beta p_old and Ap = A p_new with p.Ap partials.
-// The PCG kernels are latency-bound gathers: four 256-thread blocks per SM
-// (64 registers a thread) keep twice the loads in flight of the register
-// count the compiler picks unbounded (79 in k_matvec<float>, 126 in
-// k_update<double>); on the 160^3 lattice the FP32 matvec runs 2.1x faster.
-constexpr int kPcgMinBlocks = 4;
-template <typename T, int PAR>
-__global__ void __launch_bounds__(kThreads, kPcgMinBlocks) k_matvec(IterArgs<T> a) {
+// The PCG kernels are latency-bound gathers; MB 256-thread blocks per SM is
+// the register budget the compiler must meet (MB 4: 64 registers a thread).
+// Unbounded it picks 79 in k_matvec<float> and 126 in k_update<double>, which
+// halves the loads in flight: on the 160^3 lattice the FP32 matvec runs 2.1x
+// faster at MB 4. The autotuner (vx_scene_autotune) picks MB per scene.
+template <typename T, int PAR, int MB>
+__global__ void __launch_bounds__(kThreads, MB) k_matvec(IterArgs<T> a) {
     __shared__ int32_t s_done;
     const unsigned G = gridDim.x;
     if (threadIdx.x == 0) s_done = *(volatile int32_t*)&a.sc->done;
@@ -155,8 +155,8 @@ __global__ void __launch_bounds__(kThreads, kPcgMinBlocks) k_matvec(IterArgs<T> 
 
 // Iteration k: alpha = rz_k / p.Ap, x += alpha p, r -= alpha Ap, z = D^-1 r with
 // r.z and r.r partials; p.Ap <= 1e-30 stops like the reference (src/solver.rs:1864-1866).
-template <typename T, int PAR>
-__global__ void __launch_bounds__(kThreads, kPcgMinBlocks) k_update(IterArgs<T> a) {
+template <typename T, int PAR, int MB>
+__global__ void __launch_bounds__(kThreads, MB) k_update(IterArgs<T> a) {
     __shared__ int32_t s_done;
     const unsigned G = gridDim.x;
     if (threadIdx.x == 0) s_done = *(volatile int32_t*)&a.sc->done;
@@ -279,15 +279,31 @@ static IterArgs<float> args32(vx_scene* s, int ping) {
     return a;
 }
 
+// The instantiations of the streaming kernels for one register budget.
+template <typename T>
+struct StreamKernels {
+    void (*matvec[2])(IterArgs<T>);
+    void (*update[2])(IterArgs<T>);
+};
+template <typename T>
+static StreamKernels<T> stream_kernels(int mb) {
+    switch (mb) {
+        case 3: return {{k_matvec<T, 0, 3>, k_matvec<T, 1, 3>}, {k_update<T, 0, 3>, k_update<T, 1, 3>}};
+        case 5: return {{k_matvec<T, 0, 5>, k_matvec<T, 1, 5>}, {k_update<T, 0, 5>, k_update<T, 1, 5>}};
+        default: return {{k_matvec<T, 0, 4>, k_matvec<T, 1, 4>}, {k_update<T, 0, 4>, k_update<T, 1, 4>}};
+    }
+}
+
 // Grid of the PCG kernels: enough blocks to fill every SM once, never more
 // than there are 256-REV tiles.
 template <typename T>
 static unsigned pcg_grid(vx_scene* s) {
     unsigned* cached = sizeof(T) == 8 ? &s->grid64 : &s->grid32;
     if (*cached) return *cached;
+    const StreamKernels<T> k = stream_kernels<T>(s->pcg_minb);
     int occ_m = 0, occ_u = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k_matvec<T, 0>, kThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k_update<T, 0>, kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_m, k.matvec[0], kThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, k.update[0], kThreads, 0);
     int occ = occ_m < occ_u ? occ_m : occ_u;
     if (occ < 1) occ = 1;
     unsigned g = (unsigned)(s->sm_count * occ);
@@ -308,10 +324,11 @@ static void enqueue_chunk(vx_scene* s, cudaStream_t st) {
             a0 = args32(s, 0);
             a1 = args32(s, 1);
         }
-        k_matvec<T, 0><<<G, kThreads, 0, st>>>(a0);
-        k_update<T, 0><<<G, kThreads, 0, st>>>(a0);
-        k_matvec<T, 1><<<G, kThreads, 0, st>>>(a1);
-        k_update<T, 1><<<G, kThreads, 0, st>>>(a1);
+        const StreamKernels<T> k = stream_kernels<T>(s->pcg_minb);
+        k.matvec[0]<<<G, kThreads, 0, st>>>(a0);
+        k.update[0]<<<G, kThreads, 0, st>>>(a0);
+        k.matvec[1]<<<G, kThreads, 0, st>>>(a1);
+        k.update[1]<<<G, kThreads, 0, st>>>(a1);
     }
 }
 
@@ -432,7 +449,8 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
     const unsigned G64 = pcg_grid<double>(s);
     const unsigned G32 = pcg_grid<float>(s);
     bool persistent = false;
-    if (kernel != VX_KERNEL_STREAMING) persistent = persistent_plan(s);
+    if (kernel == VX_KERNEL_PERSISTENT || (kernel == VX_KERNEL_AUTO && s->tuned_kernel != VX_KERNEL_STREAMING))
+        persistent = persistent_plan(s);
     if (kernel == VX_KERNEL_PERSISTENT && !persistent) {
         set_error("the persistent inner solve does not fit this scene on this GPU");
         return VX_BAD_INPUT;
@@ -506,11 +524,11 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
             k_init<double><<<G, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[0], s->stream);
-            k_matvec<double, 0><<<G, kThreads, 0, s->stream>>>(a);
+            stream_kernels<double>(s->pcg_minb).matvec[0]<<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[1], s->stream);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[2], s->stream);
-            k_update<double, 0><<<G, kThreads, 0, s->stream>>>(a);
+            stream_kernels<double>(s->pcg_minb).update[0]<<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[3], s->stream);
         } else {
             const unsigned G = pcg_grid<float>(s);
@@ -518,11 +536,11 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
             k_init<float><<<G, kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, 0xFFFFFFFFu);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[0], s->stream);
-            k_matvec<float, 0><<<G, kThreads, 0, s->stream>>>(a);
+            stream_kernels<float>(s->pcg_minb).matvec[0]<<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[1], s->stream);
             if (flush_bytes) cudaMemsetAsync(flush, (int)(r & 0xff), flush_bytes, s->stream);
             cudaEventRecord(ev[2], s->stream);
-            k_update<float, 0><<<G, kThreads, 0, s->stream>>>(a);
+            stream_kernels<float>(s->pcg_minb).update[0]<<<G, kThreads, 0, s->stream>>>(a);
             cudaEventRecord(ev[3], s->stream);
         }
         err = cudaEventSynchronize(ev[3]);
@@ -568,6 +586,73 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
         out_us[3] = its;
     }
     return VX_OK;
+}
+
+
+// ---- autotuning ------------------------------------------------------------------------
+// Selects the register budget of the streaming kernels; the cached graphs
+// and grids of the old budget are dropped.
+static void set_minb(vx_scene* s, int mb) {
+    if (s->pcg_minb == mb) return;
+    cudaStreamSynchronize(s->stream);
+    if (s->chunk64) cudaGraphExecDestroy(s->chunk64);
+    if (s->chunk32) cudaGraphExecDestroy(s->chunk32);
+    s->chunk64 = s->chunk32 = nullptr;
+    s->grid64 = s->grid32 = 0;
+    s->pcg_minb = mb;
+}
+
+// Microseconds per iteration of a 64-iteration inner solve from r = b
+// (tolerance 0, so every iteration runs), CUDA events on the scene stream;
+// the first run of a candidate warms its graph and is not timed.
+int32_t time_candidate(vx_scene* s, int32_t precision, int32_t kernel, int mb, double* us) {
+    const uint32_t iters = 64;
+    set_minb(s, mb);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float ms = 0.f;
+    uint32_t its = 0;
+    int32_t st = VX_OK;
+    cudaError_t err = cudaSuccess;
+    for (int rep = 0; rep < 2 && st == VX_OK && err == cudaSuccess; ++rep) {
+        PcgScalars* sc = precision == VX_PRECISION_FP64 ? s->sc : s->sc32;
+        if (precision == VX_PRECISION_MIXED) {
+            cudaMemsetAsync(s->x64, 0, 3 * (size_t)s->n * sizeof(double), s->stream);
+            IterArgs<double> a64 = args64(s, 0);
+            k_residual64<<<pcg_grid<double>(s), kThreads, 0, s->stream>>>(a64, s->b64, s->r64, s->sc);
+        }
+        cudaEventRecord(e0, s->stream);
+        if (precision == VX_PRECISION_FP64) {
+            IterArgs<double> a = args64(s, 0);
+            k_init<double><<<pcg_grid<double>(s), kThreads, 0, s->stream>>>(a, s->b64, nullptr, 0.0, iters);
+            st = run_chunks<double>(s, sc, iters);
+        } else if (kernel == VX_KERNEL_PERSISTENT) {
+            st = solve_inner_persistent(s, 0.0, iters);
+        } else {
+            IterArgs<float> a = args32(s, 0);
+            k_init<float><<<pcg_grid<float>(s), kThreads, 0, s->stream>>>(a, s->r64, &s->sc->r64_norm, 0.0, iters);
+            st = run_chunks<float>(s, sc, iters);
+        }
+        cudaEventRecord(e1, s->stream);
+        err = cudaEventSynchronize(e1);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        if (err == cudaSuccess) err = cudaMemcpy(&its, &sc->iterations, 4, cudaMemcpyDeviceToHost);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != VX_OK) return st;
+    if (err != cudaSuccess) {
+        set_error("autotune timing failed: %s", cudaGetErrorString(err));
+        return VX_CUDA_ERROR;
+    }
+    *us = its ? 1000.0 * ms / its : 1e30;
+    return VX_OK;
+}
+
+void apply_tuning(vx_scene* s, int32_t kernel, int mb) {
+    set_minb(s, mb);
+    s->tuned_kernel = kernel;
 }
 
 }  // namespace vx

@@ -104,6 +104,19 @@ class VxStepStats(C.Structure):
         return d
 
 
+class VxTuneResult(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("blocks_per_sm", C.c_int32), ("us_per_iteration", C.c_double),
+                ("from_cache", C.c_int32), ("candidates", C.c_uint32), ("candidate_kernel", C.c_int32 * 8),
+                ("candidate_blocks", C.c_int32 * 8), ("candidate_us", C.c_double * 8)]
+
+    def as_dict(self):
+        k = self.candidates
+        return {"kernel": self.kernel, "blocks_per_sm": self.blocks_per_sm,
+                "us_per_iteration": self.us_per_iteration, "from_cache": self.from_cache,
+                "candidates": [(self.candidate_kernel[i], self.candidate_blocks[i], self.candidate_us[i])
+                               for i in range(k)]}
+
+
 class VxServerConfig(C.Structure):
     _fields_ = [("max_revs", C.c_uint64), ("hbm_fraction", C.c_double), ("max_slots", C.c_uint32),
                 ("step", VxStepParams)]
@@ -191,6 +204,7 @@ def load(path: Path | None = None):
                                      C.POINTER(C.c_uint32)]
     L.vx_scene_get_bond_state.argtypes = [C.c_void_p, f32p, f32p, f32p, f32p]
     L.vx_scene_rebuild_clusters.argtypes = [C.c_void_p, u32p, C.POINTER(C.c_uint32)]
+    L.vx_scene_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.POINTER(VxTuneResult)]
     L.vx_server_create.argtypes = [C.c_void_p, C.POINTER(VxServerConfig), C.POINTER(C.c_void_p)]
     L.vx_server_submit.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), u8p, f64p, C.POINTER(VxRequestPlan),
                                    C.POINTER(C.c_uint64)]
@@ -392,6 +406,14 @@ class DeviceScene:
         d, broken = VxDissipation(), C.c_uint32()
         check(load().vx_fracture_commit(self.h, dt, C.byref(cfg or fracture_config()), C.byref(d), C.byref(broken)))
         return d.as_dict(), broken.value
+
+    def autotune(self, precision=PRECISION_MIXED, cache_path=None) -> dict:
+        """vx_scene_autotune: times the candidate launch configurations of the
+        inner solve (after a pass) and keeps the fastest for later passes."""
+        out = VxTuneResult()
+        path = None if cache_path is None else str(cache_path).encode()
+        check(load().vx_scene_autotune(self.h, precision, path, C.byref(out)))
+        return out.as_dict()
 
     def rebuild_clusters(self):
         """(clusters[n], cluster_count) as rebuild_clusters numbers them."""
