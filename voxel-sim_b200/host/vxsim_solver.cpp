@@ -53,7 +53,32 @@ Scene::Scene(vx_ctx* ctx, const std::vector<VoxelSpawn>& voxels, const std::vect
     d.anisotropy = ani.data();
     d.neighbor = nbr.data();
     status_ = vx_scene_create(ctx, &d, &handle_);
-    if (status_ != VX_OK) handle_ = nullptr;
+    if (status_ != VX_OK) {
+        handle_ = nullptr;
+        return;
+    }
+    status_ = rebuild_clusters();  // Scene::from_voxels ends with it (src/scene.rs:571)
+}
+
+std::vector<uint32_t> Scene::neighbors() const {
+    std::vector<uint32_t> out(3 * n_);
+    if (handle_ && n_) vx_scene_get_neighbors(handle_, out.data());
+    return out;
+}
+
+std::vector<float> Scene::bond_damage() const {
+    std::vector<float> out(3 * n_);
+    if (handle_ && n_) vx_scene_get_bond_state(handle_, nullptr, out.data(), nullptr, nullptr);
+    return out;
+}
+
+int32_t Scene::rebuild_clusters(std::vector<uint32_t>* clusters) {
+    if (!handle_) return VX_BAD_INPUT;
+    if (clusters) clusters->assign(n_, 0);
+    uint32_t count = 0;
+    const int32_t r = vx_scene_rebuild_clusters(handle_, clusters && n_ ? clusters->data() : nullptr, &count);
+    if (r == VX_OK) cluster_count = count;
+    return r;
 }
 
 Scene::~Scene() {
@@ -265,7 +290,17 @@ int32_t step_with_axis_targets_and_loads(Scene& s, const std::vector<AxisTargets
     p.pass.precision = s.config.precision;
     p.pass.reuse_preconditioner = s.config.reuse_preconditioner ? 1 : 0;
     p.pass.kernel = s.config.kernel;
-    return vx_scene_step(s.handle(), &p, &s.last_step);
+    p.fracture = s.config.fracture ? 1 : 0;
+    p.fracture_config = s.config.fracture_config;
+    r = vx_scene_step(s.handle(), &p, &s.last_step);
+    if (r != VX_OK && r != VX_NOT_CONVERGED) return r;
+    s.solver_residual = s.last_step.residual;
+    s.broken += s.last_step.broken;
+    if (s.last_step.broken > 0) {
+        const int32_t rc = s.rebuild_clusters();
+        if (rc != VX_OK) return rc;
+    }
+    return r;
 }
 
 }  // namespace solver

@@ -56,6 +56,10 @@ struct SceneConfig {
     int32_t precision = VX_PRECISION_FP64;
     int32_t kernel = VX_KERNEL_AUTO;
     bool reuse_preconditioner = true;  // the CPU path's stale factor from the second pass on
+    // fracture::update after the passes of every substep (src/solver.rs:624-663),
+    // with FractureConfig::default (src/fracture.rs:27-42) in its f32 values
+    bool fracture = true;
+    vx_fracture_config fracture_config{35.0, (double)0.005f, 1000.0, 3.0, 0.5, (double)0.9f};
 };
 
 // One REV of a lattice built from cells (Scene::from_voxels, src/scene.rs:445-573).
@@ -64,7 +68,7 @@ struct VoxelSpawn {
     uint32_t material = 0;
     bool kinematic = false;
     Vec3 fiber{0.f, 0.f, 1.f};  // Microstructure::fibers()
-    float anisotropy = 1.f;
+    float anisotropy = 0.f;  // VoxelSpawn::new (src/scene.rs:97-109)
 };
 
 class Scene {
@@ -88,6 +92,12 @@ public:
     std::vector<std::array<double, 3>> velocities() const;
     std::array<double, 3> position(size_t i) const;
     std::array<double, 3> velocity(size_t i) const;
+    // bond state, axis-major (axis * n + i): Bond::neighbor and Bond::damage
+    std::vector<uint32_t> neighbors() const;
+    std::vector<float> bond_damage() const;
+    // rebuild_clusters (src/solver.rs:828-858): sets cluster_count; the REVs'
+    // cluster ids when asked for
+    int32_t rebuild_clusters(std::vector<uint32_t>* clusters = nullptr);
 
     SceneConfig config;
     std::vector<Vec3> external_forces;
@@ -96,6 +106,9 @@ public:
     std::vector<float> mass;
     std::vector<uint8_t> kinematic;
     vx_step_stats last_step{};
+    uint64_t broken = 0;         // Scene::broken: bonds broken since creation
+    size_t cluster_count = 0;    // Scene::cluster_count
+    double solver_residual = 0;  // Scene::solver_residual of the last pass
 
 private:
     vx_scene* handle_ = nullptr;
@@ -119,7 +132,8 @@ Status release_voxel(Scene& scene, size_t voxel);
 
 // The step functions return the vx status of the device step (VX_OK,
 // VX_NOT_CONVERGED, ...); VX_BAD_INPUT where the reference asserts (target or
-// load slices of the wrong length, non-finite merged targets).
+// load slices of the wrong length, non-finite merged targets). A step that
+// broke bonds rebuilds the clusters (src/solver.rs:741-743).
 int32_t step(Scene& scene);
 int32_t step_with_targets(Scene& scene, const std::vector<std::optional<Vec3>>& targets);
 int32_t step_with_axis_targets(Scene& scene, const std::vector<AxisTargets>& targets);
