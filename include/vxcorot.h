@@ -317,6 +317,48 @@ int32_t vx_scene_get_bond_state(vx_scene* scene, float* plastic_strain, float* d
                                 float* equivalent_plastic_strain, float* fatigue_damage);
 
 /*
+ * ---- contacts (collision::project, src/collision.rs:33-119; contact
+ * velocities, :122-300) ----
+ *
+ * vx_contact_project runs the contact projection over the scene's positions,
+ * with its previous positions (the substep's starts, VX_FIELD_PREVIOUS) as
+ * the swept starts: candidate pairs from the swept bin boxes (:376-444)
+ * without the intact-lattice pairs of each elementary cell (:505-540), then
+ * up to six ordered sweeps that separate overlapping or crossing pairs
+ * (:51-103). Positions and previous positions are corrected in place;
+ * targeted axes (the scene's target mask) have zero inverse mass. The
+ * contacts, sorted by pair with the first one of each pair kept, stay on the
+ * device for vx_contact_resolve_velocities and vx_scene_get_contacts. The
+ * rest positions that decide the intact-lattice pairs are the positions the
+ * scene was created with.
+ */
+typedef struct vx_contact_stats {
+    uint64_t candidates;  /* pairs whose swept boxes share a bin, one REV not kinematic */
+    uint64_t pairs;       /* after the intact-lattice filter */
+    uint32_t contacts;
+    uint32_t sweeps;
+    uint32_t live_max;    /* most pairs replayed in one sweep */
+    uint32_t redone;      /* sweeps replayed with a wider movement bound */
+} vx_contact_stats;
+typedef struct vx_contact_heat {
+    double restitution;  /* J, kinetic loss of the normal impulses */
+    double friction;     /* J, kinetic loss of the friction impulses */
+} vx_contact_heat;
+int32_t vx_contact_project(vx_scene* scene, vx_contact_stats* out);
+/* resolve_velocities_with_precontact over the current contacts; pre_contact 0
+   uses the current velocities as the pre-contact ones (resolve_velocities),
+   1 the last step's drift velocities (as the step does). */
+int32_t vx_contact_resolve_velocities(vx_scene* scene, int32_t pre_contact, double restitution, double friction,
+                                      vx_contact_heat* out);
+/* Contacts as (i, j, normal, new_impact); normal is the signed axis
+   +-(axis + 1). capacity 0 only reports the count. */
+int32_t vx_scene_get_contacts(vx_scene* scene, uint32_t capacity, uint32_t* i, uint32_t* j, int32_t* normal,
+                              uint8_t* new_impact, uint32_t* out_count);
+/* Replaces the current contacts (for velocity resolution of given contacts). */
+int32_t vx_scene_set_contacts(vx_scene* scene, uint32_t count, const uint32_t* i, const uint32_t* j,
+                              const int32_t* normal, const uint8_t* new_impact);
+
+/*
  * ---- the fixed step on the device ----
  *
  * One call of solver::step_with_axis_targets_and_loads (src/solver.rs:438-700)
@@ -345,6 +387,9 @@ typedef struct vx_step_params {
                                         the second pass of a substep on, as the reference's CPU path */
     int32_t fracture;                /* 1: the fracture stage after the passes of every substep */
     vx_fracture_config fracture_config;
+    int32_t contact;                 /* 1: contact projection and contact velocities every substep */
+    double restitution;              /* FractureConfig::restitution, [0, 1] */
+    double friction;                 /* FractureConfig::friction, >= 0 */
 } vx_step_params;
 
 typedef struct vx_step_stats {
@@ -355,6 +400,9 @@ typedef struct vx_step_stats {
     int32_t converged;               /* every pass reached its tolerance */
     uint32_t broken;                 /* bonds broken by the fracture stages */
     vx_dissipation dissipation;      /* summed over the fracture stages */
+    uint32_t contacts;               /* contacts found, summed over substeps */
+    double restitution_heat;         /* J, contact restitution loss, summed over substeps */
+    double friction_heat;            /* J, contact friction loss, summed over substeps */
 } vx_step_stats;
 
 int32_t vx_scene_step(vx_scene* scene, const vx_step_params* params, vx_step_stats* out);
@@ -374,7 +422,7 @@ int32_t vx_scene_update_velocities(vx_scene* scene, uint32_t count, const uint32
  * store the given values on every axis, with no target handling; they serve
  * host calls that change a few REVs (fix_voxel_axes, apply_impulse).
  */
-enum { VX_FIELD_POSITION = 0, VX_FIELD_VELOCITY = 1 };
+enum { VX_FIELD_POSITION = 0, VX_FIELD_VELOCITY = 1, VX_FIELD_PREVIOUS = 2 };
 int32_t vx_scene_read_revs(vx_scene* scene, int32_t field, uint32_t count, const uint32_t* index, double* xyz);
 int32_t vx_scene_write_revs(vx_scene* scene, int32_t field, uint32_t count, const uint32_t* index,
                             const double* xyz);

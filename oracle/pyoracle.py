@@ -83,6 +83,7 @@ class VxoStepConfig(C.Structure):
         ("solver_tolerance", C.c_double), ("corotation_tolerance", C.c_double),
         ("corotation_iterations", C.c_uint32), ("gravity", C.c_double * 3),
         ("fracture", VxoFractureConfig), ("fracture_enabled", C.c_int),
+        ("contact_enabled", C.c_int), ("restitution", C.c_double), ("friction", C.c_double),
     ]
 
 
@@ -93,7 +94,17 @@ class VxoDynamics(C.Structure):
         ("solver_residual", C.c_double), ("broken", C.c_uint64), ("pcg_iterations", C.c_uint64),
         ("external_work", C.c_double), ("plastic_heat", C.c_double), ("stored_plastic", C.c_double),
         ("surface_work", C.c_double), ("damage_heat", C.c_double), ("pending_release", C.c_double),
+        ("rest", f64p), ("contacts", C.c_uint64), ("restitution_heat", C.c_double), ("friction_heat", C.c_double),
     ]
+
+
+class VxoContact(C.Structure):
+    _fields_ = [("i", C.c_uint32), ("j", C.c_uint32), ("normal", C.c_int32), ("new_impact", C.c_int32),
+                ("order", C.c_uint32)]
+
+
+class VxoContactStats(C.Structure):
+    _fields_ = [("candidates", C.c_uint64), ("pairs", C.c_uint64), ("contacts", C.c_uint64), ("sweeps", C.c_uint32)]
 
 
 def default_fracture_config() -> VxoFractureConfig:
@@ -150,6 +161,15 @@ def lib():
         L.vxo_cuda_pcg_emulate.argtypes = [C.c_uint32, f32p, u32p, f32p, f32p, f32p, C.c_uint32, C.c_float,
                                            f32p, u32p, f32p]
         L.vxo_step.argtypes = [C.POINTER(VxoScene), C.POINTER(VxoStepConfig), C.POINTER(VxoDynamics)]
+        L.vxo_contact_project.restype = C.c_uint32
+        L.vxo_contact_project.argtypes = [C.c_uint32, f64p, f64p, f64p, u8p, f64p, u8p, u32p,
+                                          C.POINTER(C.POINTER(VxoContact)), C.POINTER(VxoContactStats)]
+        L.vxo_resolve_velocities.argtypes = [C.c_uint32, f64p, f64p, u8p, f64p, u8p, C.POINTER(VxoContact),
+                                             C.c_uint32, C.c_double, C.c_double, f64p, f64p]
+        L.vxo_contact_box.argtypes = [f64p, f64p, C.c_uint32, i32p, i32p]
+        L.vxo_local_continuum_pair.restype = C.c_int
+        L.vxo_local_continuum_pair.argtypes = [f64p, u32p, C.c_uint32, C.c_uint32]
+        L.free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -373,7 +393,8 @@ class OracleStepper:
 
     def __init__(self, scene, *, fixed_dt, substeps, iterations, solver_tolerance=1e-5,
                  corotation_tolerance=1e-5, corotation_iterations=2, gravity=(0, 0, 0),
-                 fracture=True, fracture_config=None):
+                 fracture=True, fracture_config=None, contact=False, restitution=0.1, friction=0.35,
+                 rest=None):
         self.o = OracleScene(scene)
         n = scene.n
         self.velocity = np.ascontiguousarray(scene.velocity, np.float64).reshape(-1).copy()
@@ -386,11 +407,15 @@ class OracleStepper:
         self.last_force = np.zeros(9 * max(n, 1), np.float64)
         self.cfg = VxoStepConfig(fixed_dt, substeps, iterations, solver_tolerance, corotation_tolerance,
                                  corotation_iterations, (C.c_double * 3)(*gravity),
-                                 fracture_config or default_fracture_config(), int(fracture))
+                                 fracture_config or default_fracture_config(), int(fracture), int(contact),
+                                 restitution, friction)
+        # Scene::rest_positions: the creation positions, f32 (src/scene.rs:520-522)
+        r = scene.position if rest is None else rest
+        self.rest = np.ascontiguousarray(np.asarray(r, np.float32), np.float64).reshape(-1).copy()
         self.d = VxoDynamics(ptr(self.velocity, C.c_double), ptr(self.previous, C.c_double),
                              ptr(self.o.target_mask, C.c_uint8), ptr(self.target, C.c_double),
                              ptr(self.o.loads, C.c_double), self.bonds, ptr(self.last_force, C.c_double),
-                             0.0, 0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+                             0.0, 0, 0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, ptr(self.rest, C.c_double), 0, 0.0, 0.0)
 
     def set_targets(self, mask, values):
         self.o.target_mask[:] = mask
@@ -420,3 +445,51 @@ def rebuild_clusters(neighbor, kinematic):
     lib().vxo_rebuild_clusters.restype = C.c_uint32
     cnt = lib().vxo_rebuild_clusters(n, ptr(nb, C.c_uint32), ptr(kin, C.c_uint8), ptr(out, C.c_uint32))
     return out[:n].copy(), int(cnt)
+
+
+def contact_project(position, previous, rest, kinematic, mass, neighbor, target_mask=None):
+    """vxo_contact_project (collision::project): corrected (position, previous)
+    as (n, 3) arrays, the contacts as a structured array (i, j, normal,
+    new_impact) sorted by (i, j), and the pair statistics."""
+    pos = np.ascontiguousarray(position, np.float64).reshape(-1).copy()
+    prev = np.ascontiguousarray(previous, np.float64).reshape(-1).copy()
+    rst = np.ascontiguousarray(np.asarray(rest, np.float32), np.float64).reshape(-1).copy()
+    kin = np.ascontiguousarray(kinematic, np.uint8)
+    m = np.ascontiguousarray(mass, np.float64)
+    nb = np.ascontiguousarray(neighbor, np.uint32).reshape(-1)
+    n = len(kin)
+    tm = None if target_mask is None else np.ascontiguousarray(target_mask, np.uint8)
+    out = C.POINTER(VxoContact)()
+    st = VxoContactStats()
+    cnt = lib().vxo_contact_project(n, ptr(pos, C.c_double), ptr(prev, C.c_double), ptr(rst, C.c_double),
+                                    ptr(kin, C.c_uint8), ptr(m, C.c_double),
+                                    None if tm is None else ptr(tm, C.c_uint8), ptr(nb, C.c_uint32),
+                                    C.byref(out), C.byref(st))
+    contacts = np.zeros(cnt, dtype=CONTACT_DTYPE)
+    for k in range(cnt):
+        c = out[k]
+        contacts[k] = (c.i, c.j, c.normal, c.new_impact)
+    lib().free(C.cast(out, C.c_void_p))
+    stats = dict(candidates=st.candidates, pairs=st.pairs, contacts=st.contacts, sweeps=st.sweeps)
+    return pos.reshape(-1, 3), prev.reshape(-1, 3), contacts, stats
+
+
+CONTACT_DTYPE = np.dtype([("i", "<u4"), ("j", "<u4"), ("normal", "<i4"), ("new_impact", "<i4")])
+
+
+def resolve_velocities(velocity, pre_contact, kinematic, mass, contacts, restitution, friction, target_mask=None):
+    """vxo_resolve_velocities (resolve_velocities_with_precontact): the new
+    (n, 3) velocities and the (restitution, friction) heat."""
+    vel = np.ascontiguousarray(velocity, np.float64).reshape(-1).copy()
+    pre = np.ascontiguousarray(pre_contact, np.float64).reshape(-1).copy()
+    kin = np.ascontiguousarray(kinematic, np.uint8)
+    m = np.ascontiguousarray(mass, np.float64)
+    tm = None if target_mask is None else np.ascontiguousarray(target_mask, np.uint8)
+    arr = (VxoContact * max(len(contacts), 1))()
+    for k, c in enumerate(contacts):
+        arr[k] = VxoContact(int(c["i"]), int(c["j"]), int(c["normal"]), int(c["new_impact"]), k)
+    rh, fh = np.zeros(1), np.zeros(1)
+    lib().vxo_resolve_velocities(len(kin), ptr(vel, C.c_double), ptr(pre, C.c_double), ptr(kin, C.c_uint8),
+                                 ptr(m, C.c_double), None if tm is None else ptr(tm, C.c_uint8), arr, len(contacts),
+                                 restitution, friction, ptr(rh, C.c_double), ptr(fh, C.c_double))
+    return vel.reshape(-1, 3), float(rh[0]), float(fh[0])

@@ -1261,6 +1261,8 @@ int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d) {
     double* start_vel = (double*)malloc(m3 * sizeof(double));
     double* solved = (double*)malloc(m3 * sizeof(double));
     double* factor = (double*)calloc(9 * (size_t)(n ? n : 1), sizeof(double));
+    double* load_vel = (double*)malloc(m3 * sizeof(double));
+    uint8_t* work_mode = (uint8_t*)malloc((size_t)(n ? n : 1));
     vxo_system sys;
     vxo_system_alloc(&sys, n);
     for (uint32_t sub = 0; sub < cfg->substeps; ++sub) {
@@ -1295,6 +1297,21 @@ int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d) {
             if (change <= cfg->corotation_tolerance && d->solver_residual <= cfg->solver_tolerance) break;
         }
         memcpy(solved, s->pos, 3 * (size_t)n * sizeof(double));
+        /* contacts after the solve, before fracture reads the positions
+           (src/solver.rs:575-590) */
+        memset(work_mode, 0, (size_t)(n ? n : 1));
+        vxo_contact* contacts = NULL;
+        uint32_t ncontacts = 0;
+        if (cfg->contact_enabled) {
+            ncontacts = vxo_contact_project(n, s->pos, d->previous, d->rest, s->kinematic, s->mass, d->target_mask,
+                                            s->nbr, &contacts, NULL);
+            d->contacts += ncontacts;
+            for (uint32_t k = 0; k < ncontacts; ++k) {
+                uint8_t mode = contacts[k].new_impact ? 2 : 1;
+                if (work_mode[contacts[k].i] < mode) work_mode[contacts[k].i] = mode;
+                if (work_mode[contacts[k].j] < mode) work_mode[contacts[k].j] = mode;
+            }
+        }
         if (cfg->fracture_enabled) {
             for (uint32_t c = 0; c < sys.c_count; ++c) {
                 uint32_t i = sys.c_i[c], j = sys.c_j[c], axis = sys.c_axis[c];
@@ -1344,17 +1361,29 @@ int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d) {
                     d->velocity[t] = drift[t] + (solved[t] - predicted[t]) / h;
             }
         }
+        memcpy(load_vel, d->velocity, 3 * (size_t)n * sizeof(double));
+        if (cfg->contact_enabled)
+            vxo_resolve_velocities(n, d->velocity, drift, s->kinematic, s->mass, d->target_mask, contacts, ncontacts,
+                                   cfg->restitution, cfg->friction, &d->restitution_heat, &d->friction_heat);
+        free(contacts);
+        /* external work (src/solver.rs:744-760): the velocity quadrature, or the
+           projected displacement under a persistent contact */
         for (uint32_t i = 0; i < n; ++i) {
             if (s->kinematic[i]) continue;
             double w = 0.0;
             for (int a = 0; a < 3; ++a) {
                 size_t t = 3 * (size_t)i + a;
                 double force = d->applied_loads[t] + cfg->gravity[a] * s->mass[i];
-                w += force * (start_vel[t] + d->velocity[t]) * (0.5 * h);
+                if (work_mode[i] == 1)
+                    w += force * (s->pos[t] - start_pos[t]);
+                else
+                    w += force * (start_vel[t] + load_vel[t]) * (0.5 * h);
             }
             d->external_work += w;
         }
     }
+    free(work_mode);
+    free(load_vel);
     vxo_system_free(&sys);
     free(predicted);
     free(drift);
@@ -1402,4 +1431,425 @@ uint32_t vxo_rebuild_clusters(uint32_t n, const uint32_t* neighbor, const uint8_
     free(parent);
     free(ids);
     return count;
+}
+
+/* ---- contact projection (collision::project, src/collision.rs:33-119, :376-505)
+ * and velocity resolution (src/collision.rs:133-300), in double precision.
+ * The reference's f32 literals are used at their f32 values.                 */
+static const double C_BIN_HALF = 0.5001999735832214;     /* 0.5 + 2e-4 in f32 (bin_bounds, :437-444) */
+static const double C_START_TOUCH = 0.009998999536037445; /* CELL - 1e-6 (swept_normal, :553) */
+static const double C_NEW_IMPACT = 0.010001999326050282;  /* CELL + 2e-6 (project, :75) */
+static const double C_1EM6 = 9.999999974752427e-07;
+static const double C_SLOP = 1.9999999949504854e-06;     /* CONTACT_SLOP (:447) */
+static const double C_1EM8 = 9.99999993922529e-09;
+static const double C_1EM12 = 9.999999960041972e-13;
+static const double C_1EM3 = 0.0010000000474974513;
+
+typedef struct {
+    uint64_t key;
+    uint32_t id;
+} bin_entry;
+
+static int cmp_bin_entry(const void* a, const void* b) {
+    const bin_entry* x = (const bin_entry*)a;
+    const bin_entry* y = (const bin_entry*)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->id < y->id ? -1 : (x->id > y->id);
+}
+static int cmp_u64(const void* a, const void* b) {
+    uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return x < y ? -1 : (x > y);
+}
+
+static uint64_t bin_key(int32_t x, int32_t y, int32_t z) {
+    return ((uint64_t)(uint32_t)(x + (1 << 20)) << 42) | ((uint64_t)(uint32_t)(y + (1 << 20)) << 21) |
+           (uint64_t)(uint32_t)(z + (1 << 20));
+}
+
+/* bin_bounds (:437-444) over the swept box of REV i, in cell units */
+void vxo_contact_box(const double* start, const double* pos, uint32_t i, int32_t lo[3], int32_t hi[3]) {
+    for (int t = 0; t < 3; ++t) {
+        double s = start[3 * (size_t)i + t], p = pos[3 * (size_t)i + t];
+        double a = fmin(s, p) / VXO_CELL, b = fmax(s, p) / VXO_CELL;
+        lo[t] = (int32_t)floor(a - C_BIN_HALF);
+        hi[t] = (int32_t)floor(b + C_BIN_HALF);
+    }
+}
+
+/* open-addressing set of pair keys (i << 32 | j) */
+typedef struct {
+    uint64_t* slot; /* key + 1, 0 = empty */
+    size_t cap, count;
+} pair_set;
+
+static int pair_set_insert(pair_set* s, uint64_t key);
+static void pair_set_grow(pair_set* s) {
+    pair_set t = {(uint64_t*)calloc(s->cap * 2, sizeof(uint64_t)), s->cap * 2, 0};
+    for (size_t k = 0; k < s->cap; ++k)
+        if (s->slot[k]) pair_set_insert(&t, s->slot[k] - 1);
+    free(s->slot);
+    *s = t;
+}
+static int pair_set_insert(pair_set* s, uint64_t key) {
+    if (2 * (s->count + 1) > s->cap) pair_set_grow(s);
+    uint64_t h = (key * 0x9E3779B97F4A7C15ull) >> 17;
+    for (size_t k = (size_t)h & (s->cap - 1);; k = (k + 1) & (s->cap - 1)) {
+        if (s->slot[k] == key + 1) return 0;
+        if (!s->slot[k]) {
+            s->slot[k] = key + 1;
+            s->count++;
+            return 1;
+        }
+    }
+}
+
+/* candidate_pairs (:376-435): every pair whose swept bin boxes share a bin,
+   at least one REV non-kinematic; sorted (i < j). */
+static uint64_t* candidate_pairs(uint32_t n, const double* start, const double* pos, const uint8_t* kin,
+                                 size_t* out_count) {
+    size_t cap = 64, cnt = 0, scap = 64, scnt = 0;
+    bin_entry* dyn = (bin_entry*)malloc(cap * sizeof(bin_entry));
+    bin_entry* sta = (bin_entry*)malloc(scap * sizeof(bin_entry));
+    for (uint32_t i = 0; i < n; ++i) {
+        int32_t lo[3], hi[3];
+        vxo_contact_box(start, pos, i, lo, hi);
+        for (int32_t z = lo[2]; z <= hi[2]; ++z)
+            for (int32_t y = lo[1]; y <= hi[1]; ++y)
+                for (int32_t x = lo[0]; x <= hi[0]; ++x) {
+                    bin_entry e = {bin_key(x, y, z), i};
+                    if (kin[i]) {
+                        if (scnt == scap) sta = (bin_entry*)realloc(sta, (scap *= 2) * sizeof(bin_entry));
+                        sta[scnt++] = e;
+                    } else {
+                        if (cnt == cap) dyn = (bin_entry*)realloc(dyn, (cap *= 2) * sizeof(bin_entry));
+                        dyn[cnt++] = e;
+                    }
+                }
+    }
+    qsort(dyn, cnt, sizeof(bin_entry), cmp_bin_entry);
+    qsort(sta, scnt, sizeof(bin_entry), cmp_bin_entry);
+    pair_set set = {(uint64_t*)calloc(1024, sizeof(uint64_t)), 1024, 0};
+    size_t s0 = 0;
+    for (size_t a = 0; a < cnt;) {
+        size_t b = a;
+        while (b < cnt && dyn[b].key == dyn[a].key) ++b;
+        for (size_t p = a; p < b; ++p)
+            for (size_t q = p + 1; q < b; ++q) {
+                uint32_t i = dyn[p].id < dyn[q].id ? dyn[p].id : dyn[q].id;
+                uint32_t j = dyn[p].id < dyn[q].id ? dyn[q].id : dyn[p].id;
+                pair_set_insert(&set, ((uint64_t)i << 32) | j);
+            }
+        while (s0 < scnt && sta[s0].key < dyn[a].key) ++s0;
+        for (size_t q = s0; q < scnt && sta[q].key == dyn[a].key; ++q)
+            for (size_t p = a; p < b; ++p) {
+                uint32_t i = dyn[p].id < sta[q].id ? dyn[p].id : sta[q].id;
+                uint32_t j = dyn[p].id < sta[q].id ? sta[q].id : dyn[p].id;
+                pair_set_insert(&set, ((uint64_t)i << 32) | j);
+            }
+        a = b;
+    }
+    uint64_t* pairs = (uint64_t*)malloc((set.count ? set.count : 1) * sizeof(uint64_t));
+    size_t m = 0;
+    for (size_t k = 0; k < set.cap; ++k)
+        if (set.slot[k]) pairs[m++] = set.slot[k] - 1;
+    qsort(pairs, m, sizeof(uint64_t), cmp_u64);
+    free(set.slot);
+    free(dyn);
+    free(sta);
+    *out_count = m;
+    return pairs;
+}
+
+/* adjacency (:491-503): [6] per REV, slot 2a+1 the +a neighbour, 2a the -a one */
+static void contact_adjacency(uint32_t n, const uint32_t* nbr, uint32_t* adj) {
+    for (size_t k = 0; k < 6 * (size_t)n; ++k) adj[k] = VX_EMPTY;
+    for (int a = 0; a < 3; ++a)
+        for (uint32_t i = 0; i < n; ++i) {
+            uint32_t j = nbr[(size_t)a * n + i];
+            if (j == VX_EMPTY) continue;
+            adj[6 * (size_t)i + 2 * a + 1] = j;
+            adj[6 * (size_t)j + 2 * a] = i;
+        }
+}
+
+static int monotone_connected(const uint32_t* adj, uint32_t i, uint32_t j, const double steps[3]) {
+    if (steps[0] == 0.0 && steps[1] == 0.0 && steps[2] == 0.0) return i == j;
+    for (int a = 0; a < 3; ++a) {
+        if (steps[a] == 0.0) continue;
+        uint32_t next = adj[6 * (size_t)i + 2 * a + (steps[a] > 0.0 ? 1 : 0)];
+        if (next == VX_EMPTY) continue;
+        double rem[3] = {steps[0], steps[1], steps[2]};
+        rem[a] = 0.0;
+        if (monotone_connected(adj, next, j, rem)) return 1;
+    }
+    return 0;
+}
+
+/* local_continuum_pair (:505-540) */
+int vxo_local_continuum_pair(const double* rest, const uint32_t* adj, uint32_t i, uint32_t j) {
+    double steps[3], dev = 0.0, big = 0.0;
+    for (int t = 0; t < 3; ++t) {
+        double d = (rest[3 * (size_t)j + t] - rest[3 * (size_t)i + t]) / VXO_CELL;
+        steps[t] = round(d);
+        dev = fmax(dev, fabs(d - steps[t]));
+        big = fmax(big, fabs(steps[t]));
+    }
+    if (dev > C_1EM3 || big > 1.0) return 0;
+    return monotone_connected(adj, i, j, steps);
+}
+
+/* swept_normal (:546-590); returns the signed axis code +-(axis + 1), or 0 */
+static int swept_normal(const double si[3], const double sj[3], const double ei[3], const double ej[3]) {
+    double d0[3], rel[3];
+    int inside = 1;
+    for (int t = 0; t < 3; ++t) {
+        d0[t] = sj[t] - si[t];
+        double di = ei[t] - si[t], dj = ej[t] - sj[t];
+        rel[t] = dj - di;
+        if (!(fabs(d0[t]) <= C_START_TOUCH)) inside = 0;
+    }
+    if (inside) return 0;
+    double enter = 0.0, exit_ = 1.0, sign = 1.0;
+    int hit = -1;
+    for (int a = 0; a < 3; ++a) {
+        if (fabs(rel[a]) < C_1EM12) {
+            if (fabs(d0[a]) > VXO_CELL) return 0;
+            continue;
+        }
+        double t0 = (-VXO_CELL - d0[a]) / rel[a];
+        double t1 = (VXO_CELL - d0[a]) / rel[a];
+        double nearv = fmin(t0, t1), farv = fmax(t0, t1);
+        if (nearv > enter || (hit < 0 && nearv >= enter)) {
+            enter = nearv;
+            hit = a;
+            sign = d0[a] + rel[a] * enter >= 0.0 ? 1.0 : -1.0;
+        }
+        exit_ = fmin(exit_, farv);
+        if (enter > exit_) return 0;
+    }
+    if (exit_ < 0.0 || enter > 1.0 || hit < 0) return 0;
+    return sign > 0.0 ? hit + 1 : -(hit + 1);
+}
+
+/* overlap_normal (:592-616): axis code, penetration */
+static int overlap_normal(const double a[3], const double b[3], const double fallback[3], double* penetration) {
+    double d[3], o[3];
+    for (int t = 0; t < 3; ++t) {
+        d[t] = b[t] - a[t];
+        o[t] = VXO_CELL - fabs(d[t]);
+    }
+    if (fmin(fmin(o[0], o[1]), o[2]) <= 0.0) return 0;
+    int axis = (o[0] <= o[1] && o[0] <= o[2]) ? 0 : (o[1] <= o[2] ? 1 : 2);
+    double src = fabs(d[axis]) > C_1EM8 ? d[axis] : (fabs(fallback[axis]) > C_1EM8 ? fallback[axis] : 1.0);
+    *penetration = o[axis];
+    return signbit(src) ? -(axis + 1) : axis + 1;
+}
+
+/* touching_normal (:446-468) */
+static int touching_normal(const double a[3], const double b[3]) {
+    double d[3], g[3];
+    for (int t = 0; t < 3; ++t) {
+        d[t] = b[t] - a[t];
+        g[t] = fabs(d[t]) - VXO_CELL;
+    }
+    int axis = (g[0] >= g[1] && g[0] >= g[2]) ? 0 : (g[1] >= g[2] ? 1 : 2);
+    if (g[axis] > C_SLOP) return 0;
+    for (int o = 0; o < 3; ++o)
+        if (o != axis && g[o] >= -C_SLOP) return 0;
+    return d[axis] >= 0.0 ? axis + 1 : -(axis + 1);
+}
+
+static double contact_inverse_mass(const uint8_t* kin, const double* mass, const uint8_t* tmask, uint32_t i, int axis) {
+    if (kin[i] || (tmask && ((tmask[i] >> axis) & 1))) return 0.0;
+    return 1.0 / mass[i];
+}
+
+/* separate (:631-654) */
+static int separate(double* pos, double* prev, const uint8_t* kin, const double* mass, const uint8_t* tmask,
+                    uint32_t i, uint32_t j, int code, double amount) {
+    int axis = (code > 0 ? code : -code) - 1;
+    double wi = contact_inverse_mass(kin, mass, tmask, i, axis);
+    double wj = contact_inverse_mass(kin, mass, tmask, j, axis);
+    double denom = wi + wj;
+    if (denom <= 0.0) return 0;
+    double nrm[3] = {0.0, 0.0, 0.0};
+    nrm[axis] = code > 0 ? 1.0 : -1.0;
+    double si = amount * wi / denom, sj = amount * wj / denom;
+    for (int t = 0; t < 3; ++t) {
+        double di = -nrm[t] * si, dj = nrm[t] * sj;
+        pos[3 * (size_t)i + t] += di;
+        pos[3 * (size_t)j + t] += dj;
+        prev[3 * (size_t)i + t] += di;
+        prev[3 * (size_t)j + t] += dj;
+    }
+    return 1;
+}
+
+static double code_dot(int code, const double v[3]) {
+    double nrm[3] = {0.0, 0.0, 0.0};
+    int axis = (code > 0 ? code : -code) - 1;
+    nrm[axis] = code > 0 ? 1.0 : -1.0;
+    return v[0] * nrm[0] + v[1] * nrm[1] + v[2] * nrm[2];
+}
+
+static int cmp_contact(const void* a, const void* b) {
+    const vxo_contact* x = (const vxo_contact*)a;
+    const vxo_contact* y = (const vxo_contact*)b;
+    if (x->i != y->i) return x->i < y->i ? -1 : 1;
+    if (x->j != y->j) return x->j < y->j ? -1 : 1;
+    return x->order < y->order ? -1 : (x->order > y->order);
+}
+
+uint32_t vxo_contact_project(uint32_t n, double* pos, double* prev, const double* rest, const uint8_t* kin,
+                             const double* mass, const uint8_t* tmask, const uint32_t* nbr, vxo_contact** out,
+                             vxo_contact_stats* st) {
+    double* start = (double*)malloc(3 * (size_t)(n ? n : 1) * sizeof(double));
+    memcpy(start, prev, 3 * (size_t)n * sizeof(double));
+    uint32_t* adj = (uint32_t*)malloc(6 * (size_t)(n ? n : 1) * sizeof(uint32_t));
+    contact_adjacency(n, nbr, adj);
+    size_t cand = 0;
+    uint64_t* pairs = candidate_pairs(n, start, pos, kin, &cand);
+    size_t m = 0;
+    for (size_t k = 0; k < cand; ++k) {
+        uint32_t i = (uint32_t)(pairs[k] >> 32), j = (uint32_t)pairs[k];
+        if (!vxo_local_continuum_pair(rest, adj, i, j)) pairs[m++] = pairs[k];
+    }
+    size_t ccap = 64, ccnt = 0;
+    vxo_contact* c = (vxo_contact*)malloc(ccap * sizeof(vxo_contact));
+    uint32_t sweeps = 0;
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        int changed = 0;
+        sweeps++;
+        for (size_t k = 0; k < m; ++k) {
+            uint32_t i = (uint32_t)(pairs[k] >> 32), j = (uint32_t)pairs[k];
+            const double *si = start + 3 * (size_t)i, *sj = start + 3 * (size_t)j;
+            double* pi = pos + 3 * (size_t)i;
+            double* pj = pos + 3 * (size_t)j;
+            double d0[3] = {sj[0] - si[0], sj[1] - si[1], sj[2] - si[2]};
+            int code = swept_normal(si, sj, pi, pj);
+            int impact = 0;
+            if (code) {
+                double dd[3] = {pj[0] - pi[0], pj[1] - pi[1], pj[2] - pi[2]};
+                double separation = code_dot(code, dd);
+                if (separation < VXO_CELL)
+                    changed |= separate(pos, prev, kin, mass, tmask, i, j, code, VXO_CELL - separation + C_1EM6);
+                impact = code_dot(code, d0) > C_NEW_IMPACT;
+            } else {
+                double pen = 0.0;
+                code = overlap_normal(pi, pj, d0, &pen);
+                if (code) {
+                    changed |= separate(pos, prev, kin, mass, tmask, i, j, code, pen + C_1EM6);
+                    impact = code_dot(code, d0) > C_NEW_IMPACT;
+                } else {
+                    code = touching_normal(pi, pj);
+                }
+            }
+            if (code) {
+                if (ccnt == ccap) c = (vxo_contact*)realloc(c, (ccap *= 2) * sizeof(vxo_contact));
+                c[ccnt].i = i;
+                c[ccnt].j = j;
+                c[ccnt].normal = code;
+                c[ccnt].new_impact = impact;
+                c[ccnt].order = (uint32_t)ccnt;
+                ccnt++;
+            }
+        }
+        if (!changed) break;
+    }
+    /* sort by (i, j) and keep the first contact of each pair (:105-106) */
+    qsort(c, ccnt, sizeof(vxo_contact), cmp_contact);
+    size_t u = 0;
+    for (size_t k = 0; k < ccnt; ++k)
+        if (u == 0 || c[k].i != c[u - 1].i || c[k].j != c[u - 1].j) c[u++] = c[k];
+    if (st) {
+        st->candidates = cand;
+        st->pairs = m;
+        st->contacts = u;
+        st->sweeps = sweeps;
+    }
+    free(start);
+    free(adj);
+    free(pairs);
+    *out = c;
+    return (uint32_t)u;
+}
+
+/* resolve_velocities_with_precontact (:133-300), velocity AoS 3n */
+void vxo_resolve_velocities(uint32_t n, double* vel, const double* pre_contact, const uint8_t* kin, const double* mass,
+                            const uint8_t* tmask, const vxo_contact* c, uint32_t count, double restitution_cfg,
+                            double friction, double* restitution_heat, double* friction_heat) {
+    double* phys = (double*)malloc(3 * (size_t)(n ? n : 1) * sizeof(double));
+    memcpy(phys, pre_contact, 3 * (size_t)n * sizeof(double));
+    for (int iteration = 0; iteration < 4; ++iteration) {
+        int changed = 0;
+        for (uint32_t k = 0; k < count; ++k) {
+            uint32_t i = c[k].i, j = c[k].j;
+            int axis = (c[k].normal > 0 ? c[k].normal : -c[k].normal) - 1;
+            double nrm[3] = {0.0, 0.0, 0.0};
+            nrm[axis] = c[k].normal > 0 ? 1.0 : -1.0;
+            double wi = contact_inverse_mass(kin, mass, tmask, i, axis);
+            double wj = contact_inverse_mass(kin, mass, tmask, j, axis);
+            double denom = wi + wj;
+            if (denom <= 0.0) continue;
+            double* vi = vel + 3 * (size_t)i;
+            double* vj = vel + 3 * (size_t)j;
+            double rv[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+            double closing = rv[0] * nrm[0] + rv[1] * nrm[1] + rv[2] * nrm[2];
+            double normal_impulse = 0.0;
+            if (closing < -C_1EM6) {
+                double rest = (c[k].new_impact && iteration == 0) ? restitution_cfg : 0.0;
+                normal_impulse = -(1.0 + rest) * closing / denom;
+                double* qi = phys + 3 * (size_t)i;
+                double* qj = phys + 3 * (size_t)j;
+                double pr[3] = {qj[0] - qi[0], qj[1] - qi[1], qj[2] - qi[2]};
+                double physical_closing = pr[0] * nrm[0] + pr[1] * nrm[1] + pr[2] * nrm[2];
+                double physical_impulse = c[k].new_impact ? normal_impulse
+                                          : (physical_closing < -C_1EM6 ? fmin(-physical_closing / denom, normal_impulse)
+                                                                         : 0.0);
+                for (int t = 0; t < 3; ++t) {
+                    vi[t] -= nrm[t] * (normal_impulse * wi);
+                    vj[t] += nrm[t] * (normal_impulse * wj);
+                }
+                double heat_closing = c[k].new_impact ? closing : physical_closing;
+                double rh = 0.0;
+                if (heat_closing < -C_1EM6 && physical_impulse > 0.0)
+                    rh = fmax(physical_impulse * -heat_closing - 0.5 * (physical_impulse * physical_impulse) * denom, 0.0);
+                if (rh > 0.0) *restitution_heat += rh;
+                for (int t = 0; t < 3; ++t) {
+                    qi[t] -= nrm[t] * (physical_impulse * wi);
+                    qj[t] += nrm[t] * (physical_impulse * wj);
+                }
+                changed = 1;
+            }
+            if (normal_impulse > 0.0 && friction > 0.0) {
+                double rel[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+                double rn = rel[0] * nrm[0] + rel[1] * nrm[1] + rel[2] * nrm[2];
+                double tr[3], rt[3];
+                for (int t = 0; t < 3; ++t) {
+                    double tangent = rel[t] - nrm[t] * rn;
+                    tr[t] = contact_inverse_mass(kin, mass, tmask, i, t) + contact_inverse_mass(kin, mass, tmask, j, t);
+                    rt[t] = tr[t] > 0.0 ? tangent : 0.0;
+                }
+                double speed = sqrt(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2]);
+                if (speed > C_1EM6) {
+                    double dir[3] = {rt[0] / speed, rt[1] / speed, rt[2] / speed};
+                    double tw = 0.0;
+                    for (int t = 0; t < 3; ++t) tw += dir[t] * dir[t] * tr[t];
+                    if (tw > 0.0) {
+                        double mag = fmin(speed / tw, friction * normal_impulse);
+                        for (int t = 0; t < 3; ++t) {
+                            double imp = -dir[t] * mag;
+                            vi[t] -= imp * contact_inverse_mass(kin, mass, tmask, i, t);
+                            vj[t] += imp * contact_inverse_mass(kin, mass, tmask, j, t);
+                        }
+                        double fh = fmax(mag * speed - 0.5 * (mag * mag) * tw, 0.0);
+                        if (fh > 0.0 && (!kin[i] || !kin[j])) *friction_heat += fh;
+                        changed = 1;
+                    }
+                }
+            }
+        }
+        if (!changed) break;
+    }
+    free(phys);
 }

@@ -152,7 +152,7 @@ int vxo_cuda_pcg_emulate(uint32_t n, const float* rhs, const uint32_t* nbr6,
                          uint32_t max_iterations, float tolerance, float* dx,
                          uint32_t* iterations, float* residual);
 
-/* ---- one fixed step (src/solver.rs:440-763 without tool/contact/thermal) -- */
+/* ---- one fixed step (src/solver.rs:440-763 without tool/thermal) --------- */
 typedef struct vxo_step_config {
     double fixed_dt;
     uint32_t substeps;
@@ -163,6 +163,9 @@ typedef struct vxo_step_config {
     double gravity[3];
     vxo_fracture_config fracture;
     int fracture_enabled;
+    int contact_enabled;   /* collision::project and resolve_velocities_with_precontact */
+    double restitution;    /* FractureConfig::restitution */
+    double friction;       /* FractureConfig::friction */
 } vxo_step_config;
 
 typedef struct vxo_dynamics {
@@ -178,9 +181,45 @@ typedef struct vxo_dynamics {
     uint64_t pcg_iterations;
     double external_work;
     double plastic_heat, stored_plastic, surface_work, damage_heat, pending_release;
+    const double* rest;      /* 3n Scene::rest_positions (contacts only) */
+    uint64_t contacts;       /* contacts found, summed over substeps */
+    double restitution_heat, friction_heat;
 } vxo_dynamics;
 
 int vxo_step(vxo_scene* s, const vxo_step_config* cfg, vxo_dynamics* d);
+
+/* ---- contacts (src/collision.rs) ------------------------------------------ */
+/* normal: signed axis code +-(axis + 1); order: position in the push order */
+typedef struct vxo_contact {
+    uint32_t i, j;
+    int32_t normal;
+    int32_t new_impact;
+    uint32_t order;
+} vxo_contact;
+
+typedef struct vxo_contact_stats {
+    uint64_t candidates; /* pairs from the bins */
+    uint64_t pairs;      /* after the local-continuum filter */
+    uint64_t contacts;
+    uint32_t sweeps;
+} vxo_contact_stats;
+
+/* bin_bounds of REV i's swept box (src/collision.rs:437-444), cell units */
+void vxo_contact_box(const double* start, const double* pos, uint32_t i, int32_t lo[3], int32_t hi[3]);
+/* local_continuum_pair (src/collision.rs:505-540); adj[6n] as adjacency() builds it */
+int vxo_local_continuum_pair(const double* rest, const uint32_t* adj, uint32_t i, uint32_t j);
+/* collision::project (src/collision.rs:33-119): positions and previous (3n) are
+   corrected in place; starts are previous on entry. *out (malloc'd, caller
+   frees) receives the contacts sorted by (i, j), the first of each pair kept.
+   tmask (or NULL): targeted axes have zero inverse mass. */
+uint32_t vxo_contact_project(uint32_t n, double* pos, double* prev, const double* rest, const uint8_t* kinematic,
+                             const double* mass, const uint8_t* tmask, const uint32_t* nbr, vxo_contact** out,
+                             vxo_contact_stats* st);
+/* resolve_velocities_with_precontact (src/collision.rs:133-300); heat totals
+   are added to *restitution_heat and *friction_heat. */
+void vxo_resolve_velocities(uint32_t n, double* velocity, const double* pre_contact, const uint8_t* kinematic,
+                            const double* mass, const uint8_t* tmask, const vxo_contact* contacts, uint32_t count,
+                            double restitution, double friction, double* restitution_heat, double* friction_heat);
 
 /* rebuild_clusters (src/solver.rs:828-858): union-find over every bond with a
    neighbour; non-kinematic REVs get ids in the order their components first

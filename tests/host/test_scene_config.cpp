@@ -251,6 +251,7 @@ static void solver_settings_follow_the_file() {
     CHECK(s.fracture);
     CHECK(s.fracture_config.damage_rate == 30.0 && s.fracture_config.energy_release == (double)0.01f);
     CHECK(s.fracture_config.plastic_heat_fraction == (double)0.85f);
+    CHECK(s.contact && s.restitution == 0.2f && s.friction == 0.3f);
     // the mirror's defaults equal FractureConfig::default's f32 values
     const SceneConfig d;
     const SceneConfig from_default = SceneFileConfig{}.solver_config();

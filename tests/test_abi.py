@@ -43,7 +43,8 @@ int main(void) {{
          offsetof(vx_step_params, pass), sizeof(vx_step_stats));
   printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(vx_server_config), sizeof(vx_request_plan), sizeof(vx_request_result),
          sizeof(vx_server_stats), sizeof(vx_fracture_config), sizeof(vx_dissipation));
-  printf("%zu\\n", sizeof(vx_tune_result));
+  printf("%zu %zu %zu %zu %zu\\n", sizeof(vx_tune_result), sizeof(vx_contact_stats), sizeof(vx_contact_heat),
+         offsetof(vx_step_params, contact), offsetof(vx_step_stats, contacts));
   return 0;
 }}''')
     exe = tmp_path / "layout"
@@ -53,7 +54,8 @@ int main(void) {{
             N.VxSceneDesc.neighbor.offset, C.sizeof(N.VxStepParams), N.VxStepParams.pass_.offset,
             C.sizeof(N.VxStepStats), C.sizeof(N.VxServerConfig), C.sizeof(N.VxRequestPlan),
             C.sizeof(N.VxRequestResult), C.sizeof(N.VxServerStats), C.sizeof(N.VxFractureConfig),
-            C.sizeof(N.VxDissipation), C.sizeof(N.VxTuneResult)]
+            C.sizeof(N.VxDissipation), C.sizeof(N.VxTuneResult), C.sizeof(N.VxContactStats),
+            C.sizeof(N.VxContactHeat), N.VxStepParams.contact.offset, N.VxStepStats.contacts.offset]
     assert got == want
 
 

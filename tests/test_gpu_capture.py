@@ -3,9 +3,9 @@ src/bin/solver_scale_capture.rs) against the oracle's step.
 
 A 36 x 32 x 32 iron block with its bottom layer kinematic is stepped under
 gravity with SceneConfig::default settings (4 substeps, 2 passes, PCG cap
-160, tolerance 1e-5, fracture on). The kinematic layer is not bonded to the
-block (their kinematic flags differ) and contact is not part of the step, so
-the block falls; the oracle's step does the same. The CSV's positions are
+160, tolerance 1e-5, fracture and contact on). The kinematic layer is not
+bonded to the block (their kinematic flags differ): the block stands on it
+through the contact stage, as in the oracle's step. The CSV's positions are
 f32 values in Rust's shortest form: they must read back to the oracle's
 positions rounded to f32.
 """
@@ -90,7 +90,8 @@ def test_capture_records_the_oracle_step(tmp_path):
         assert f[2:11] == ["0", "0", "0", "0", "0", "0", "1", "0", "0"] and f[11:] == ["0", "1", "0"], f
     o = O.OracleStepper(scene, fixed_dt=float(np.float32(1e-3)), substeps=4, iterations=160,
                         solver_tolerance=float(np.float32(1e-5)), corotation_tolerance=float(np.float32(1e-5)),
-                        corotation_iterations=2, gravity=(0.0, 0.0, float(np.float32(-9.81))), fracture=True)
+                        corotation_iterations=2, gravity=(0.0, 0.0, float(np.float32(-9.81))), fracture=True,
+                        contact=True, restitution=float(np.float32(0.1)), friction=float(np.float32(0.35)))
     lost = np.array([_lost(scene.neighbor, x, y, z) for _, _, x, y, z in surface])
     for frame in range(4):
         if frame:
@@ -112,10 +113,14 @@ def test_capture_records_the_oracle_step(tmp_path):
         assert np.max(np.abs(got - want)) <= ulp, (frame, np.max(np.abs(got - want)))
         assert np.all(np.array([float(r[6]) for r in rows]) == 0.0)
         assert np.array_equal(np.array([int(r[7]) for r in rows]), lost)
-    # the free block fell by the implicit-Euler drop of 12 substeps of 0.25 ms
-    # (78 g h^2 = 4.78e-5 m); the kinematic layer stayed
+    # contact holds the layer on the kinematic floor at its rest height (the
+    # projection leaves it 1e-6 m above); the layers above settle through the
+    # lattice, less than the free fall of 12 substeps of 0.25 ms (78 g h^2 =
+    # 4.78e-5 m); the kinematic layer stayed
     idx = np.array([s[1] for s in surface])
-    free = cells[idx, 2] > 0
-    assert np.all(got[free, 2] - scene.position[idx[free], 2] < -4e-5)
-    assert np.array_equal(got[~free], scene.position[idx[~free]].astype(np.float32).astype(np.float64))
+    dz = got[:, 2] - scene.position[idx, 2]
+    z = cells[idx, 2]
+    assert np.all(dz[z == 1] >= -1e-7) and np.all(dz[z == 1] <= 2e-6)
+    assert np.all(dz[z > 1] > -4.78e-5)
+    assert np.array_equal(got[z == 0], scene.position[idx[z == 0]].astype(np.float32).astype(np.float64))
     assert "complete" in log

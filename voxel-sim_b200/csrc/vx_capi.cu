@@ -87,6 +87,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->vel = A.take<double>(3 * m);
     s->prev = A.take<double>(3 * m);
     s->drift = A.take<double>(3 * m);
+    s->rest = A.take<float>(3 * m);
     s->save_pos = A.take<double>(3 * m);
     s->save_rot = A.take<double4>(m);
     s->out_ratio = A.take<float>(3 * m);
@@ -184,6 +185,7 @@ int32_t scene_alloc(vx_scene* s, vx_ctx* ctx, uint32_t n, uint32_t material_coun
 void scene_release(vx_scene* s) {
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    contact_release(s);
     if (s->chunk64) cudaGraphExecDestroy(s->chunk64);
     if (s->chunk32) cudaGraphExecDestroy(s->chunk32);
     for (int k = 0; k < 2; ++k)
@@ -431,6 +433,8 @@ int32_t vx_scene_create(vx_ctx* ctx, const vx_scene_desc* d, vx_scene** out) {
             return r;
         }
         e = cudaMemcpyAsync(s->pred, s->pos, 3 * m * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(s->prev, s->pos, 3 * m * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = launch_rest_positions(s);
         if (e == cudaSuccess) e = launch_reverse_neighbors(s);
         if (e == cudaSuccess) e = launch_flags(s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -560,7 +564,7 @@ int32_t vx_scene_update_velocities(vx_scene* s, uint32_t count, const uint32_t* 
 static int32_t indexed_field(vx_scene* s, int32_t field, uint32_t count, const uint32_t* index, double* xyz,
                              bool write, const char* who) {
     clear_error();
-    if (!s || (count && (!index || !xyz)) || (field != VX_FIELD_POSITION && field != VX_FIELD_VELOCITY)) {
+    if (!s || (count && (!index || !xyz)) || (field != VX_FIELD_POSITION && field != VX_FIELD_VELOCITY && field != VX_FIELD_PREVIOUS)) {
         set_error("%s: bad argument", who);
         return VX_BAD_INPUT;
     }
@@ -578,7 +582,7 @@ static int32_t indexed_field(vx_scene* s, int32_t field, uint32_t count, const u
     }
     if (count == 0) return VX_OK;
     cudaSetDevice(s->device);
-    double* dev_field = field == VX_FIELD_POSITION ? s->pos : s->vel;
+    double* dev_field = field == VX_FIELD_POSITION ? s->pos : (field == VX_FIELD_VELOCITY ? s->vel : s->prev);
     for (uint32_t base = 0; base < count;) {
         const uint32_t chunk = (uint32_t)std::min<size_t>(count - base, s->stage_revs);
         VX_TRY(cudaStreamSynchronize(s->stream), who);

@@ -1,0 +1,1430 @@
+// vx_contact.cu — contact projection (collision::project, src/collision.rs:33-119,
+// :376-590) and contact velocity resolution (resolve_velocities_with_precontact,
+// :133-300) on the device, in FP64 over the scene's FP64 positions and
+// velocities. This file is compiled without fused multiply-adds so that every
+// value rounds as the FP64 restatement of the same expressions does.
+//
+// Broadphase. Every REV's swept box (previous and current position, each
+// widened by half a cell and 2e-4 cells, floored to bins; bin_bounds :437-444)
+// is computed in parallel. Two REVs are a candidate pair when their boxes share
+// a bin and at least one of them is not kinematic, which is exactly the set the
+// reference's bin maps produce (candidate_pairs :376-435). Small boxes (at most
+// 4 bins per axis) are found through a hash of box corners; the rare larger
+// boxes of fast REVs through a hash of every bin they cover. Pairs joined
+// through the intact lattice inside their elementary cell are dropped
+// (local_continuum_pair :505-540) and each pair is written to the segment of
+// its smaller REV, so after a per-segment sort the list is the reference's
+// sorted pair list.
+//
+// Projection. The reference sweeps the pairs in order, and each correction is
+// seen by the pairs after it (Gauss-Seidel). The device keeps that order
+// exactly: with a bound M on how far any REV moves during a sweep, a pair whose
+// boxes stay farther apart than the contact tests reach even after both REVs
+// move by M cannot act or report a contact in that sweep ("inert"). The other
+// ("live") pairs are grouped into connected components over shared REVs; one
+// thread replays each component's pairs in pair order, so every pair sees the
+// same positions it sees in the reference's sweep. After the sweep the largest
+// movement of any REV is checked against M; when it is larger the sweep is
+// restored and replayed with a wider bound (finally with every pair live).
+// Contact velocity resolution runs the same way over components of the
+// contact list; its sweeps stop per component when nothing changes, which is
+// what the reference's global stop does to that component.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "vx_device.cuh"
+#include "vx_kernels.h"
+
+namespace vx {
+
+namespace {
+
+// The reference's f32 literals, at their f32 values.
+constexpr double kBinHalf = 0.5001999735832214;      // 0.5 + 2e-4 (bin_bounds)
+constexpr double kStartTouch = 0.009998999536037445;  // CELL - 1e-6 (swept_normal)
+constexpr double kNewImpact = 0.010001999326050282;   // CELL + 2e-6 (project)
+constexpr double k1em6 = 9.999999974752427e-07;
+constexpr double kSlop = 1.9999999949504854e-06;  // CONTACT_SLOP (touching_normal)
+constexpr double k1em8 = 9.99999993922529e-09;
+constexpr double k1em12 = 9.999999960041972e-13;
+constexpr double k1em3 = 0.0010000000474974513;
+
+constexpr int kSmallExtent = 4;          // bins per axis of a box found through its corner
+constexpr int32_t kCoordLimit = 1 << 20;  // |bin coordinate| bound of the 21-bit key fields
+constexpr unsigned kProbeLimit = 1u << 20;
+constexpr unsigned kUnionRetries = 1u << 16;
+constexpr uint64_t kMaxLargeVolume = 1ull << 24;  // bins one fast REV may sweep in a substep
+constexpr unsigned long long kEmptyKey = ~0ull;
+constexpr unsigned kScanBlock = 1024;
+
+enum : uint32_t {
+    E_OK = 0,
+    E_RANGE = 1,     // a non-finite position or a bin outside the key range
+    E_TABLE = 2,     // a hash probe exceeded its bound
+    E_UNION = 4,     // a union exceeded its retry bound
+    E_VOLUME = 8,    // a swept box larger than kMaxLargeVolume bins
+};
+
+// scalars in ContactState::scal
+enum { S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_COUNT = 8 };
+
+__device__ __forceinline__ unsigned long long bin_key(int32_t x, int32_t y, int32_t z) {
+    return ((unsigned long long)(uint32_t)(x + kCoordLimit) << 42) |
+           ((unsigned long long)(uint32_t)(y + kCoordLimit) << 21) | (unsigned long long)(uint32_t)(z + kCoordLimit);
+}
+__device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
+    k ^= k >> 31;
+    k *= 0x9E3779B97F4A7C15ull;
+    k ^= k >> 29;
+    return (uint32_t)k;
+}
+
+// Hash slot holding key, or VX_EMPTY_U32.
+__device__ uint32_t table_find(const unsigned long long* keys, uint32_t mask, unsigned long long key) {
+    uint32_t slot = key_hash(key) & mask;
+    for (unsigned probe = 0; probe <= mask && probe < kProbeLimit; ++probe) {
+        const unsigned long long k = keys[slot];
+        if (k == key) return slot;
+        if (k == kEmptyKey) return VX_EMPTY_U32;
+        slot = (slot + 1) & mask;
+    }
+    return VX_EMPTY_U32;
+}
+// Slot for key, claiming an empty one; VX_EMPTY_U32 when the probe bound is hit.
+__device__ uint32_t table_claim(unsigned long long* keys, uint32_t mask, unsigned long long key) {
+    uint32_t slot = key_hash(key) & mask;
+    for (unsigned probe = 0; probe <= mask && probe < kProbeLimit; ++probe) {
+        const unsigned long long old = atomicCAS(keys + slot, kEmptyKey, key);
+        if (old == kEmptyKey || old == key) return slot;
+        slot = (slot + 1) & mask;
+    }
+    return VX_EMPTY_U32;
+}
+
+__device__ __forceinline__ v3 load3(const double* f, uint32_t n, uint32_t i) {
+    return mk(f[i], f[(size_t)n + i], f[2 * (size_t)n + i]);
+}
+__device__ __forceinline__ void add3(double* f, uint32_t n, uint32_t i, int axis, double d) {
+    f[(size_t)axis * n + i] += d;
+}
+
+// ---- narrow-phase tests, as the FP64 restatement --------------------------
+
+// swept_normal (:546-590): signed axis code +-(axis + 1), or 0
+__device__ int swept_normal(v3 si, v3 sj, v3 ei, v3 ej) {
+    const double d0[3] = {sj.x - si.x, sj.y - si.y, sj.z - si.z};
+    const double di[3] = {ei.x - si.x, ei.y - si.y, ei.z - si.z};
+    const double dj[3] = {ej.x - sj.x, ej.y - sj.y, ej.z - sj.z};
+    double rel[3];
+    bool inside = true;
+    for (int t = 0; t < 3; ++t) {
+        rel[t] = dj[t] - di[t];
+        if (!(fabs(d0[t]) <= kStartTouch)) inside = false;
+    }
+    if (inside) return 0;
+    double enter = 0.0, exit_ = 1.0, sign = 1.0;
+    int hit = -1;
+    for (int a = 0; a < 3; ++a) {
+        if (fabs(rel[a]) < k1em12) {
+            if (fabs(d0[a]) > kCell) return 0;
+            continue;
+        }
+        const double t0 = (-kCell - d0[a]) / rel[a];
+        const double t1 = (kCell - d0[a]) / rel[a];
+        const double nearv = fmin(t0, t1), farv = fmax(t0, t1);
+        if (nearv > enter || (hit < 0 && nearv >= enter)) {
+            enter = nearv;
+            hit = a;
+            sign = d0[a] + rel[a] * enter >= 0.0 ? 1.0 : -1.0;
+        }
+        exit_ = fmin(exit_, farv);
+        if (enter > exit_) return 0;
+    }
+    if (exit_ < 0.0 || enter > 1.0 || hit < 0) return 0;
+    return sign > 0.0 ? hit + 1 : -(hit + 1);
+}
+
+// overlap_normal (:592-616)
+__device__ int overlap_normal(v3 a, v3 b, v3 fallback, double* penetration) {
+    const double d[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
+    const double f[3] = {fallback.x, fallback.y, fallback.z};
+    double o[3];
+    for (int t = 0; t < 3; ++t) o[t] = kCell - fabs(d[t]);
+    if (fmin(fmin(o[0], o[1]), o[2]) <= 0.0) return 0;
+    const int axis = (o[0] <= o[1] && o[0] <= o[2]) ? 0 : (o[1] <= o[2] ? 1 : 2);
+    const double src = fabs(d[axis]) > k1em8 ? d[axis] : (fabs(f[axis]) > k1em8 ? f[axis] : 1.0);
+    *penetration = o[axis];
+    return signbit(src) ? -(axis + 1) : axis + 1;
+}
+
+// touching_normal (:446-468)
+__device__ int touching_normal(v3 a, v3 b) {
+    const double d[3] = {b.x - a.x, b.y - a.y, b.z - a.z};
+    double g[3];
+    for (int t = 0; t < 3; ++t) g[t] = fabs(d[t]) - kCell;
+    const int axis = (g[0] >= g[1] && g[0] >= g[2]) ? 0 : (g[1] >= g[2] ? 1 : 2);
+    if (g[axis] > kSlop) return 0;
+    for (int o = 0; o < 3; ++o)
+        if (o != axis && g[o] >= -kSlop) return 0;
+    return d[axis] >= 0.0 ? axis + 1 : -(axis + 1);
+}
+
+__device__ __forceinline__ double code_dot(int code, v3 v) {
+    const int axis = (code > 0 ? code : -code) - 1;
+    const double nx = axis == 0 ? (code > 0 ? 1.0 : -1.0) : 0.0;
+    const double ny = axis == 1 ? (code > 0 ? 1.0 : -1.0) : 0.0;
+    const double nz = axis == 2 ? (code > 0 ? 1.0 : -1.0) : 0.0;
+    return v.x * nx + v.y * ny + v.z * nz;
+}
+
+// inverse_mass (:620-627): kinematic REVs and targeted axes are immovable
+__device__ __forceinline__ double inverse_mass(const uint8_t* kin, const float4* param1, const uint8_t* tmask, uint32_t i,
+                                               int axis) {
+    if (kin[i] || ((tmask[i] >> axis) & 1)) return 0.0;
+    return 1.0 / (double)param1[i].w;
+}
+
+// ---- local continuum test -------------------------------------------------
+
+// adjacency (:491-503): +a neighbour from the bond table, -a from its reverse
+__device__ __forceinline__ uint32_t adjacent(const uint32_t* nbr, const uint32_t* rev, uint32_t n, uint32_t i, int a,
+                                             bool plus) {
+    return plus ? nbr[(size_t)a * n + i] : rev[(size_t)a * n + i];
+}
+
+// local_continuum_pair (:505-540). The recursion tries the remaining axes in
+// ascending order and backtracks, so it succeeds iff some order of the
+// nonzero steps walks from i to j over existing bonds: every order is tried.
+__device__ bool local_continuum(const float* rest, const uint32_t* nbr, const uint32_t* rev, uint32_t n, uint32_t i,
+                                uint32_t j) {
+    double steps[3], dev = 0.0, big = 0.0;
+    for (int t = 0; t < 3; ++t) {
+        const double d = ((double)rest[(size_t)t * n + j] - (double)rest[(size_t)t * n + i]) / kCell;
+        steps[t] = round(d);
+        dev = fmax(dev, fabs(d - steps[t]));
+        big = fmax(big, fabs(steps[t]));
+    }
+    if (dev > k1em3 || big > 1.0) return false;
+    int axes[3], m = 0;
+    for (int t = 0; t < 3; ++t)
+        if (steps[t] != 0.0) axes[m++] = t;
+    if (m == 0) return i == j;
+    // the permutations of m <= 3 axes
+    const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    const int count = m == 1 ? 1 : (m == 2 ? 2 : 6);
+    for (int p = 0; p < count; ++p) {
+        uint32_t at = i;
+        bool ok = true;
+        for (int s = 0; s < m && ok; ++s) {
+            const int slot = m == 2 ? (p == 0 ? s : 1 - s) : perms[p][s];
+            const int a = axes[slot];
+            at = adjacent(nbr, rev, n, at, a, steps[a] > 0.0);
+            ok = at != VX_EMPTY_U32;
+        }
+        if (ok && at == j) return true;
+    }
+    return false;
+}
+
+// ---- broadphase -------------------------------------------------------------
+
+struct Boxes {
+    int32_t* lo;   // [3][n]
+    int32_t* hi;   // [3][n]
+    uint8_t* large;
+};
+
+__global__ void k_boxes(uint32_t n, const double* __restrict__ pos, const double* __restrict__ start, Boxes b,
+                        uint32_t* __restrict__ scal) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool large = false, bad = false;
+    int32_t ext[3];
+    for (int t = 0; t < 3; ++t) {
+        const double s = start[(size_t)t * n + i], p = pos[(size_t)t * n + i];
+        const double a = fmin(s, p) / kCell - kBinHalf, c = fmax(s, p) / kCell + kBinHalf;
+        if (!(fabs(a) < (double)(kCoordLimit - 1)) || !(fabs(c) < (double)(kCoordLimit - 1))) {
+            bad = true;
+            b.lo[(size_t)t * n + i] = 0;
+            b.hi[(size_t)t * n + i] = 0;
+            ext[t] = 1;
+            continue;
+        }
+        const int32_t lo = (int32_t)floor(a), hi = (int32_t)floor(c);
+        b.lo[(size_t)t * n + i] = lo;
+        b.hi[(size_t)t * n + i] = hi;
+        ext[t] = hi - lo + 1;
+        if (ext[t] > kSmallExtent) large = true;
+    }
+    if (bad) atomicOr(scal + S_ERR, E_RANGE);
+    b.large[i] = large ? 1 : 0;
+    if (large) {
+        atomicAdd(scal + S_LARGE, 1u);
+    } else {
+        for (int t = 0; t < 3; ++t) atomicMax(scal + S_EXT + t, (uint32_t)ext[t]);
+    }
+}
+
+// Small boxes: chain REVs by box corner.
+__global__ void k_insert_corners(uint32_t n, Boxes b, unsigned long long* keys, uint32_t* heads, uint32_t* next,
+                                 uint32_t mask, uint32_t* scal) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || b.large[i]) return;
+    const unsigned long long key = bin_key(b.lo[i], b.lo[(size_t)n + i], b.lo[2 * (size_t)n + i]);
+    const uint32_t slot = table_claim(keys, mask, key);
+    if (slot == VX_EMPTY_U32) {
+        atomicOr(scal + S_ERR, E_TABLE);
+        next[i] = VX_EMPTY_U32;
+        return;
+    }
+    next[i] = atomicExch(heads + slot, i);
+}
+
+__global__ void k_large_volume(uint32_t n, Boxes b, uint32_t* vol, uint32_t* scal) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t v = 0;
+    if (b.large[i]) {
+        v = 1;
+        for (int t = 0; t < 3; ++t)
+            v *= (uint64_t)(b.hi[(size_t)t * n + i] - b.lo[(size_t)t * n + i] + 1);
+        if (v > kMaxLargeVolume) {
+            atomicOr(scal + S_ERR, E_VOLUME);
+            v = 0;
+        }
+    }
+    vol[i] = (uint32_t)v;
+}
+
+// Large boxes: one entry per covered bin, chained by bin.
+__global__ void k_insert_large(uint32_t n, Boxes b, const uint32_t* __restrict__ off, unsigned long long* keys,
+                               uint32_t* heads, uint32_t* ent_id, uint32_t* ent_next, uint32_t mask, uint32_t* scal) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !b.large[i]) return;
+    uint32_t e = off[i];
+    const uint32_t end = off[i + 1];
+    const int32_t x0 = b.lo[i], y0 = b.lo[(size_t)n + i], z0 = b.lo[2 * (size_t)n + i];
+    const int32_t x1 = b.hi[i], y1 = b.hi[(size_t)n + i], z1 = b.hi[2 * (size_t)n + i];
+    for (int32_t z = z0; z <= z1; ++z)
+        for (int32_t y = y0; y <= y1; ++y)
+            for (int32_t x = x0; x <= x1 && e < end; ++x, ++e) {
+                const uint32_t slot = table_claim(keys, mask, bin_key(x, y, z));
+                ent_id[e] = i;
+                if (slot == VX_EMPTY_U32) {
+                    atomicOr(scal + S_ERR, E_TABLE);
+                    ent_next[e] = VX_EMPTY_U32;
+                    continue;
+                }
+                ent_next[e] = atomicExch(heads + slot, e);
+            }
+}
+
+struct PairArgs {
+    uint32_t n;
+    Boxes b;
+    const uint8_t* kin;
+    const float* rest;
+    const uint32_t* nbr;
+    const uint32_t* rev;
+    const unsigned long long* keys1;  // corner table
+    const uint32_t* heads1;
+    const uint32_t* next1;
+    uint32_t mask1;
+    const unsigned long long* keys2;  // large-box table (mask2 = 0: none)
+    const uint32_t* heads2;
+    const uint32_t* ent_id;
+    const uint32_t* ent_next;
+    uint32_t mask2;
+    int32_t wx, wy, wz;  // largest small extent per axis
+    uint32_t* count;     // per owner: pairs (count pass) / cursor (write pass)
+    const uint32_t* off;
+    uint32_t* pi;
+    uint32_t* pj;
+    uint32_t* scal;
+};
+
+template <bool kWrite>
+__device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand) {
+    const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
+    if (a.kin[lo] && a.kin[hi]) return;
+    ++cand;
+    if (local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
+    if (kWrite) {
+        const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
+        a.pi[slot] = lo;
+        a.pj[slot] = hi;
+    } else {
+        atomicAdd(a.count + lo, 1u);
+    }
+}
+
+__device__ __forceinline__ void box_of(const Boxes& b, uint32_t n, uint32_t i, int32_t lo[3], int32_t hi[3]) {
+    for (int t = 0; t < 3; ++t) {
+        lo[t] = b.lo[(size_t)t * n + i];
+        hi[t] = b.hi[(size_t)t * n + i];
+    }
+}
+
+template <bool kWrite>
+__global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const uint32_t n = a.n;
+    int32_t lo[3], hi[3];
+    box_of(a.b, n, i, lo, hi);
+    uint32_t cand = 0;
+    const bool large_i = a.b.large[i] != 0;
+    if (!large_i) {
+        // small-small: corners within reach of this box; the smaller REV finds the pair
+        const int32_t w[3] = {a.wx, a.wy, a.wz};
+        for (int32_t z = lo[2] - (w[2] - 1); z <= hi[2]; ++z)
+            for (int32_t y = lo[1] - (w[1] - 1); y <= hi[1]; ++y)
+                for (int32_t x = lo[0] - (w[0] - 1); x <= hi[0]; ++x) {
+                    const uint32_t slot = table_find(a.keys1, a.mask1, bin_key(x, y, z));
+                    if (slot == VX_EMPTY_U32) continue;
+                    for (uint32_t j = a.heads1[slot]; j != VX_EMPTY_U32; j = a.next1[j]) {
+                        if (j <= i) continue;
+                        int32_t lj[3], hj[3];
+                        box_of(a.b, n, j, lj, hj);
+                        if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] && lj[2] <= hi[2] &&
+                            lo[2] <= hj[2])
+                            emit<kWrite>(a, i, j, cand);
+                    }
+                }
+    }
+    if (a.mask2) {
+        // pairs with large boxes: the bins of this box, each pair counted at the
+        // lowest corner of the two boxes' intersection
+        for (int32_t z = lo[2]; z <= hi[2]; ++z)
+            for (int32_t y = lo[1]; y <= hi[1]; ++y)
+                for (int32_t x = lo[0]; x <= hi[0]; ++x) {
+                    const uint32_t slot = table_find(a.keys2, a.mask2, bin_key(x, y, z));
+                    if (slot == VX_EMPTY_U32) continue;
+                    for (uint32_t e = a.heads2[slot]; e != VX_EMPTY_U32; e = a.ent_next[e]) {
+                        const uint32_t j = a.ent_id[e];
+                        if (j == i || (large_i && j < i)) continue;
+                        int32_t lj[3], hj[3];
+                        box_of(a.b, n, j, lj, hj);
+                        if (x == max(lo[0], lj[0]) && y == max(lo[1], lj[1]) && z == max(lo[2], lj[2]))
+                            emit<kWrite>(a, i, j, cand);
+                    }
+                }
+    }
+    if (!kWrite && cand) {
+        const unsigned long long prev =
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
+        (void)prev;
+    }
+}
+
+// Sorts each REV's pair segment by partner (insertion sort; segments are short).
+__global__ void k_sort_segments(uint32_t n, const uint32_t* __restrict__ off, uint32_t* pj) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = off[i], e = off[i + 1];
+    for (uint32_t k = b + 1; k < e; ++k) {
+        const uint32_t v = pj[k];
+        uint32_t m = k;
+        while (m > b && pj[m - 1] > v) {
+            pj[m] = pj[m - 1];
+            --m;
+        }
+        pj[m] = v;
+    }
+}
+
+// ---- projection sweeps -----------------------------------------------------
+
+// A pair is live when, with both REVs moved by at most M, one of the three
+// tests can still answer: its end separation within H = CELL + slop + 2M (+ a
+// rounding margin) on every axis, or (unless the starts already overlap) its
+// relative path from the start separation to the end one meeting the box of
+// half-width H.
+__global__ void k_classify(uint32_t count, const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj, uint32_t n,
+                           const double* __restrict__ pos, const double* __restrict__ start, double half,
+                           uint8_t* __restrict__ live) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t i = pi[k], j = pj[k];
+    const v3 si = load3(start, n, i), sj = load3(start, n, j), ei = load3(pos, n, i), ej = load3(pos, n, j);
+    const double d0[3] = {sj.x - si.x, sj.y - si.y, sj.z - si.z};
+    const double e[3] = {ej.x - ei.x, ej.y - ei.y, ej.z - ei.z};
+    bool near_end = true, starts_inside = true;
+    for (int t = 0; t < 3; ++t) {
+        if (!(fabs(e[t]) <= half)) near_end = false;
+        if (!(fabs(d0[t]) <= kStartTouch)) starts_inside = false;
+    }
+    bool hit = near_end;
+    if (!hit && !starts_inside) {
+        double t0 = 0.0, t1 = 1.0;
+        hit = true;
+        for (int t = 0; t < 3 && hit; ++t) {
+            const double r = e[t] - d0[t];
+            if (r == 0.0) {
+                hit = fabs(d0[t]) <= half;
+                continue;
+            }
+            const double a = (-half - d0[t]) / r, b = (half - d0[t]) / r;
+            t0 = fmax(t0, fmin(a, b));
+            t1 = fmin(t1, fmax(a, b));
+            hit = t0 <= t1;
+        }
+    }
+    live[k] = hit ? 1 : 0;
+}
+
+__global__ void k_compact(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                          uint32_t* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count && flag[k]) out[off[k]] = k;
+}
+
+__global__ void k_iota(uint32_t n, uint32_t* __restrict__ v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
+    uint32_t p = __ldcg(parent + x);
+    while (p != x) {
+        const uint32_t g = __ldcg(parent + p);
+        if (g != p) __stcg(parent + x, g);
+        x = p;
+        p = g;
+    }
+    return x;
+}
+
+// Joins the two REVs of each listed item (pairs or contacts).
+__global__ void k_union(uint32_t count, const uint32_t* __restrict__ items, const uint32_t* __restrict__ ia,
+                        const uint32_t* __restrict__ ja, uint32_t* parent, uint32_t* scal) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t k = items ? items[t] : t;
+    const uint32_t i = ia[k], j = ja[k];
+    for (unsigned tries = 0; tries < kUnionRetries; ++tries) {
+        const uint32_t ri = uf_find(parent, i), rj = uf_find(parent, j);
+        if (ri == rj) return;
+        const uint32_t lo = ri < rj ? ri : rj, hi = ri < rj ? rj : ri;
+        if (atomicCAS(parent + hi, hi, lo) == hi) return;
+    }
+    atomicOr(scal + S_ERR, E_UNION);
+}
+
+// After the unions: each item's component root (read-only walk) and the
+// component sizes.
+__global__ void k_roots(uint32_t count, const uint32_t* __restrict__ items, const uint32_t* __restrict__ ia,
+                        const uint32_t* __restrict__ parent, uint32_t* __restrict__ root, uint32_t* comp_count) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t k = items ? items[t] : t;
+    uint32_t x = ia[k], p = parent[x];
+    while (p != x) {
+        x = p;
+        p = parent[p];
+    }
+    root[t] = x;
+    atomicAdd(comp_count + x, 1u);
+}
+
+__global__ void k_fill(uint32_t count, const uint32_t* __restrict__ items, const uint32_t* __restrict__ root,
+                       const uint32_t* __restrict__ comp_off, uint32_t* comp_cursor, uint32_t* __restrict__ out) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t r = root[t];
+    out[comp_off[r] + atomicAdd(comp_cursor + r, 1u)] = items ? items[t] : t;
+}
+
+__device__ void sort_range(uint32_t* v, uint32_t b, uint32_t e) {
+    for (uint32_t k = b + 1; k < e; ++k) {
+        const uint32_t x = v[k];
+        uint32_t m = k;
+        while (m > b && v[m - 1] > x) {
+            v[m] = v[m - 1];
+            --m;
+        }
+        v[m] = x;
+    }
+}
+
+struct SweepArgs {
+    uint32_t n;
+    const uint32_t* comp_off;
+    uint32_t* items;
+    const uint32_t* pi;
+    const uint32_t* pj;
+    double* pos;
+    double* prev;
+    const double* start;
+    const uint8_t* kin;
+    const float4* param1;
+    const uint8_t* tmask;
+    double* move;
+    int8_t* code;
+    uint8_t* impact;
+    uint32_t* scal;
+};
+
+// separate (:631-654); returns whether the pair could move (denominator > 0)
+__device__ bool separate(const SweepArgs& a, uint32_t i, uint32_t j, int code, double amount) {
+    const int axis = (code > 0 ? code : -code) - 1;
+    const double wi = inverse_mass(a.kin, a.param1, a.tmask, i, axis);
+    const double wj = inverse_mass(a.kin, a.param1, a.tmask, j, axis);
+    const double denom = wi + wj;
+    if (denom <= 0.0) return false;
+    const double s = code > 0 ? 1.0 : -1.0;
+    const double di = -s * (amount * wi / denom), dj = s * (amount * wj / denom);
+    // the other two components of -normal * x and normal * x are signed
+    // zeros: adding them leaves every coordinate unchanged
+    add3(a.pos, a.n, i, axis, di);
+    add3(a.pos, a.n, j, axis, dj);
+    add3(a.prev, a.n, i, axis, di);
+    add3(a.prev, a.n, j, axis, dj);
+    a.move[i] += fabs(di);
+    a.move[j] += fabs(dj);
+    return true;
+}
+
+// One thread replays one component's live pairs in pair order.
+__global__ void k_sweep(SweepArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n) return;
+    const uint32_t b = a.comp_off[r], e = a.comp_off[r + 1];
+    if (b == e) return;
+    sort_range(a.items, b, e);
+    bool changed = false;
+    for (uint32_t t = b; t < e; ++t) {
+        const uint32_t k = a.items[t];
+        const uint32_t i = a.pi[k], j = a.pj[k];
+        const v3 si = load3(a.start, a.n, i), sj = load3(a.start, a.n, j);
+        const v3 pi = load3(a.pos, a.n, i), pj = load3(a.pos, a.n, j);
+        const v3 d0 = sj - si;
+        int code = swept_normal(si, sj, pi, pj);
+        bool impact = false;
+        if (code) {
+            const double separation = code_dot(code, pj - pi);
+            if (separation < kCell) changed |= separate(a, i, j, code, kCell - separation + k1em6);
+            impact = code_dot(code, d0) > kNewImpact;
+        } else {
+            double pen = 0.0;
+            code = overlap_normal(pi, pj, d0, &pen);
+            if (code) {
+                changed |= separate(a, i, j, code, pen + k1em6);
+                impact = code_dot(code, d0) > kNewImpact;
+            } else {
+                code = touching_normal(pi, pj);
+            }
+        }
+        a.code[k] = (int8_t)code;
+        a.impact[k] = impact ? 1 : 0;
+    }
+    if (changed) atomicOr(a.scal + S_CHANGED, 1u);
+}
+
+__global__ void k_max_move(uint32_t n, const double* __restrict__ move, unsigned long long* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double m = move[i];
+    if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// The first contact of each pair over the sweeps is kept (the reference sorts
+// the pushed contacts by pair and keeps one per pair).
+__global__ void k_merge(uint32_t count, const uint32_t* __restrict__ live_list, const int8_t* __restrict__ code,
+                        const uint8_t* __restrict__ impact, int8_t* __restrict__ first_code,
+                        uint8_t* __restrict__ first_impact) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t k = live_list[t];
+    if (code[k] && !first_code[k]) {
+        first_code[k] = code[k];
+        first_impact[k] = impact[k];
+    }
+}
+
+__global__ void k_contact_flags(uint32_t count, const int8_t* __restrict__ code, uint8_t* __restrict__ flag) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) flag[k] = code[k] != 0;
+}
+
+__global__ void k_contact_write(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                                const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj,
+                                const int8_t* __restrict__ code, const uint8_t* __restrict__ impact, uint32_t* ci,
+                                uint32_t* cj, int8_t* cn, uint8_t* cm) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || !flag[k]) return;
+    const uint32_t o = off[k];
+    ci[o] = pi[k];
+    cj[o] = pj[k];
+    cn[o] = code[k];
+    cm[o] = impact[k];
+}
+
+// ---- contact velocities -------------------------------------------------
+
+struct ResolveArgs {
+    uint32_t n;
+    const uint32_t* comp_off;
+    uint32_t* items;
+    const uint32_t* ci;
+    const uint32_t* cj;
+    const int8_t* cn;
+    const uint8_t* cm;
+    double* vel;
+    double* phys;  // pre-contact velocities, updated with the physical impulses
+    const uint8_t* kin;
+    const float4* param1;
+    const uint8_t* tmask;
+    double restitution;
+    double friction;
+    double* heat;  // [2][n]: restitution, friction heat per component root
+};
+
+// resolve_velocities_with_precontact (:133-300) over one component's contacts
+__global__ void k_resolve(ResolveArgs a) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= a.n) return;
+    const uint32_t b = a.comp_off[r], e = a.comp_off[r + 1];
+    if (b == e) return;
+    sort_range(a.items, b, e);
+    const uint32_t n = a.n;
+    double rheat = 0.0, fheat = 0.0;
+    for (int iteration = 0; iteration < 4; ++iteration) {
+        bool changed = false;
+        for (uint32_t t = b; t < e; ++t) {
+            const uint32_t c = a.items[t];
+            const uint32_t i = a.ci[c], j = a.cj[c];
+            const int code = a.cn[c];
+            const bool new_impact = a.cm[c] != 0;
+            const int axis = (code > 0 ? code : -code) - 1;
+            double nrm[3] = {0.0, 0.0, 0.0};
+            nrm[axis] = code > 0 ? 1.0 : -1.0;
+            const double wi = inverse_mass(a.kin, a.param1, a.tmask, i, axis);
+            const double wj = inverse_mass(a.kin, a.param1, a.tmask, j, axis);
+            const double denom = wi + wj;
+            if (denom <= 0.0) continue;
+            double vi[3], vj[3];
+            for (int q = 0; q < 3; ++q) {
+                vi[q] = a.vel[(size_t)q * n + i];
+                vj[q] = a.vel[(size_t)q * n + j];
+            }
+            const double rv[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+            const double closing = rv[0] * nrm[0] + rv[1] * nrm[1] + rv[2] * nrm[2];
+            double normal_impulse = 0.0;
+            if (closing < -k1em6) {
+                const double rest = (new_impact && iteration == 0) ? a.restitution : 0.0;
+                normal_impulse = -(1.0 + rest) * closing / denom;
+                double qi[3], qj[3];
+                for (int q = 0; q < 3; ++q) {
+                    qi[q] = a.phys[(size_t)q * n + i];
+                    qj[q] = a.phys[(size_t)q * n + j];
+                }
+                const double pr[3] = {qj[0] - qi[0], qj[1] - qi[1], qj[2] - qi[2]};
+                const double physical_closing = pr[0] * nrm[0] + pr[1] * nrm[1] + pr[2] * nrm[2];
+                const double physical_impulse =
+                    new_impact ? normal_impulse
+                               : (physical_closing < -k1em6 ? fmin(-physical_closing / denom, normal_impulse) : 0.0);
+                for (int q = 0; q < 3; ++q) {
+                    vi[q] -= nrm[q] * (normal_impulse * wi);
+                    vj[q] += nrm[q] * (normal_impulse * wj);
+                }
+                const double heat_closing = new_impact ? closing : physical_closing;
+                double rh = 0.0;
+                if (heat_closing < -k1em6 && physical_impulse > 0.0)
+                    rh = fmax(physical_impulse * -heat_closing - 0.5 * (physical_impulse * physical_impulse) * denom,
+                              0.0);
+                if (rh > 0.0) rheat += rh;
+                for (int q = 0; q < 3; ++q) {
+                    a.phys[(size_t)q * n + i] = qi[q] - nrm[q] * (physical_impulse * wi);
+                    a.phys[(size_t)q * n + j] = qj[q] + nrm[q] * (physical_impulse * wj);
+                }
+                changed = true;
+            }
+            if (normal_impulse > 0.0 && a.friction > 0.0) {
+                const double rel[3] = {vj[0] - vi[0], vj[1] - vi[1], vj[2] - vi[2]};
+                const double rn = rel[0] * nrm[0] + rel[1] * nrm[1] + rel[2] * nrm[2];
+                double tr[3], rt[3];
+                for (int q = 0; q < 3; ++q) {
+                    const double tangent = rel[q] - nrm[q] * rn;
+                    tr[q] = inverse_mass(a.kin, a.param1, a.tmask, i, q) + inverse_mass(a.kin, a.param1, a.tmask, j, q);
+                    rt[q] = tr[q] > 0.0 ? tangent : 0.0;
+                }
+                const double speed = sqrt(rt[0] * rt[0] + rt[1] * rt[1] + rt[2] * rt[2]);
+                if (speed > k1em6) {
+                    const double dir[3] = {rt[0] / speed, rt[1] / speed, rt[2] / speed};
+                    double tw = 0.0;
+                    for (int q = 0; q < 3; ++q) tw += dir[q] * dir[q] * tr[q];
+                    if (tw > 0.0) {
+                        const double mag = fmin(speed / tw, a.friction * normal_impulse);
+                        for (int q = 0; q < 3; ++q) {
+                            const double imp = -dir[q] * mag;
+                            vi[q] -= imp * inverse_mass(a.kin, a.param1, a.tmask, i, q);
+                            vj[q] += imp * inverse_mass(a.kin, a.param1, a.tmask, j, q);
+                        }
+                        const double fh = fmax(mag * speed - 0.5 * (mag * mag) * tw, 0.0);
+                        if (fh > 0.0 && (!a.kin[i] || !a.kin[j])) fheat += fh;
+                        changed = true;
+                    }
+                }
+            }
+            for (int q = 0; q < 3; ++q) {
+                a.vel[(size_t)q * n + i] = vi[q];
+                a.vel[(size_t)q * n + j] = vj[q];
+            }
+        }
+        if (!changed) break;
+    }
+    a.heat[r] = rheat;
+    a.heat[(size_t)n + r] = fheat;
+}
+
+// Fixed-order sum of [count] doubles into out (one block).
+__global__ void __launch_bounds__(256) k_sum(uint32_t count, const double* __restrict__ v, double* out) {
+    __shared__ double part[256];
+    double s = 0.0;
+    for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) s += v[k];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (unsigned w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}
+
+// ---- exclusive scan (u8 or u32 input, u32 output; out[count] = total) -----
+
+template <class T>
+__global__ void __launch_bounds__(256) k_scan_blocks(uint32_t count, const T* __restrict__ in, uint32_t* __restrict__ out,
+                                                     uint32_t* __restrict__ bsum) {
+    __shared__ uint32_t warp_tot[8];
+    const uint32_t base = blockIdx.x * kScanBlock + threadIdx.x * 4;
+    uint32_t v[4], local = 0;
+    for (int k = 0; k < 4; ++k) {
+        v[k] = base + k < count ? (uint32_t)in[base + k] : 0u;
+        local += v[k];
+    }
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (unsigned w = 0; w < warp; ++w) before += warp_tot[w];
+    uint32_t run = before + incl - local;
+    for (int k = 0; k < 4; ++k) {
+        if (base + k < count) out[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == blockDim.x - 1) bsum[blockIdx.x] = before + incl;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t nb, uint32_t* bsum) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t lo = 0; lo < nb; lo += blockDim.x) {
+        const uint32_t k = lo + threadIdx.x;
+        const uint32_t v = k < nb ? bsum[k] : 0u;
+        uint32_t incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += t;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        uint32_t before = 0;
+        for (unsigned w = 0; w < warp; ++w) before += warp_tot[w];
+        const uint32_t c0 = carry;
+        if (k < nb) bsum[k] = c0 + before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = c0 + before + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void k_scan_add(uint32_t count, uint32_t* __restrict__ out, const uint32_t* __restrict__ bsum, uint32_t nb) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) out[k] += bsum[k / kScanBlock];
+    if (k == 0) out[count] = bsum[nb];
+}
+
+inline unsigned grid(size_t count) { return (unsigned)((count + 255) / 256); }
+
+}  // namespace
+
+// Grow-only device buffers of the contact stage, owned by the scene.
+struct ContactState {
+    uint32_t n = 0;
+    size_t pair_cap = 0;
+    size_t large_cap = 0;  // entries of the large-box table
+    uint32_t table1 = 0, table2 = 0;
+    // per REV
+    Boxes box{};
+    double* start = nullptr;    // [3][n] previous positions when the call began
+    double* snap = nullptr;     // [6][n] positions and previous at the start of a sweep
+    double* move = nullptr;     // [n]
+    double* heat = nullptr;     // [2][n]
+    double* phys = nullptr;     // [3][n]
+    uint32_t* next1 = nullptr;  // [n]
+    uint32_t* cnt = nullptr;    // [n + 1]
+    uint32_t* off = nullptr;    // [n + 1]
+    uint32_t* parent = nullptr; // [n]
+    uint32_t* comp_cnt = nullptr;  // [n + 1]
+    uint32_t* comp_off = nullptr;  // [n + 1]
+    uint32_t* bsum = nullptr;      // scan block sums
+    size_t bsum_cap = 0;
+    unsigned long long* keys1 = nullptr;
+    uint32_t* heads1 = nullptr;
+    // large boxes
+    unsigned long long* keys2 = nullptr;
+    uint32_t* heads2 = nullptr;
+    uint32_t* ent_id = nullptr;
+    uint32_t* ent_next = nullptr;
+    // per pair
+    uint32_t* pi = nullptr;
+    uint32_t* pj = nullptr;
+    uint8_t* live = nullptr;
+    uint32_t* live_off = nullptr;  // [cap + 1]
+    uint32_t* live_list = nullptr;
+    uint32_t* root = nullptr;
+    uint32_t* items = nullptr;
+    int8_t* code = nullptr;
+    uint8_t* impact = nullptr;
+    int8_t* first_code = nullptr;
+    uint8_t* first_impact = nullptr;
+    // contacts
+    uint32_t* ci = nullptr;
+    uint32_t* cj = nullptr;
+    int8_t* cn = nullptr;
+    uint8_t* cm = nullptr;
+    uint32_t contacts = 0;
+    // scalars: [0] error bits, [1..3] small extents, [4] large count, [5] changed,
+    // [6..7] candidate count (u64); max movement (u64 bits of a double); the
+    // host copies
+    uint32_t* scal = nullptr;
+    unsigned long long* max_move = nullptr;
+    double* heat_sum = nullptr;  // [2]
+    uint32_t* h_scal = nullptr;  // pinned [32]: [0, 16) the scalars, [16, 18) max movement, [18] a count
+};
+
+namespace {
+
+int32_t cuda_fail(cudaError_t e, const char* what) {
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? VX_OOM : VX_CUDA_ERROR;
+}
+
+template <class T>
+cudaError_t grow(T*& p, size_t& cap, size_t want) {
+    if (want <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+    if (e == cudaSuccess) cap = want;
+    return e;
+}
+
+template <class T>
+cudaError_t alloc(T*& p, size_t count) {
+    return cudaMalloc(&p, (count ? count : 1) * sizeof(T));
+}
+
+uint32_t pow2_at_least(size_t v) {
+    uint32_t p = 1024;
+    while (p < v && p < (1u << 31)) p <<= 1;
+    return p;
+}
+
+// out[0..count) = exclusive scan of in, out[count] = total.
+template <class T>
+cudaError_t scan(ContactState* c, cudaStream_t st, const T* in, uint32_t* out, uint32_t count) {
+    const uint32_t nb = (count + kScanBlock - 1) / kScanBlock;
+    cudaError_t e = grow(c->bsum, c->bsum_cap, (size_t)nb + 2);
+    if (e != cudaSuccess) return e;
+    if (count == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
+    k_scan_blocks<T><<<nb, 256, 0, st>>>(count, in, out, c->bsum);
+    k_scan_sums<<<1, 1024, 0, st>>>(nb, c->bsum);
+    k_scan_add<<<grid(count), 256, 0, st>>>(count, out, c->bsum, nb);
+    return cudaGetLastError();
+}
+
+cudaError_t ensure_state(vx_scene* s) {
+    ContactState* c = s->contact;
+    if (c && c->n == s->n) return cudaSuccess;
+    if (c) {
+        contact_release(s);
+    }
+    c = new (std::nothrow) ContactState();
+    if (!c) return cudaErrorMemoryAllocation;
+    s->contact = c;
+    const size_t n = s->n ? s->n : 1;
+    c->n = s->n;
+    c->table1 = pow2_at_least(2 * n);
+    cudaError_t e = alloc(c->box.lo, 3 * n);
+    if (e == cudaSuccess) e = alloc(c->box.hi, 3 * n);
+    if (e == cudaSuccess) e = alloc(c->box.large, n);
+    if (e == cudaSuccess) e = alloc(c->start, 3 * n);
+    if (e == cudaSuccess) e = alloc(c->snap, 6 * n);
+    if (e == cudaSuccess) e = alloc(c->move, n);
+    if (e == cudaSuccess) e = alloc(c->heat, 2 * n);
+    if (e == cudaSuccess) e = alloc(c->phys, 3 * n);
+    if (e == cudaSuccess) e = alloc(c->next1, n);
+    if (e == cudaSuccess) e = alloc(c->cnt, n + 1);
+    if (e == cudaSuccess) e = alloc(c->off, n + 1);
+    if (e == cudaSuccess) e = alloc(c->parent, n);
+    if (e == cudaSuccess) e = alloc(c->comp_cnt, n + 1);
+    if (e == cudaSuccess) e = alloc(c->comp_off, n + 1);
+    if (e == cudaSuccess) e = alloc(c->keys1, c->table1);
+    if (e == cudaSuccess) e = alloc(c->heads1, c->table1);
+    if (e == cudaSuccess) e = alloc(c->scal, 16);
+    if (e == cudaSuccess) e = alloc(c->max_move, 1);
+    if (e == cudaSuccess) e = alloc(c->heat_sum, 2);
+    if (e == cudaSuccess) e = cudaMallocHost(&c->h_scal, 32 * sizeof(uint32_t));
+    return e;
+}
+
+cudaError_t ensure_pairs(ContactState* c, size_t want) {
+    if (want <= c->pair_cap && c->pi) return cudaSuccess;
+    size_t cap = std::max<size_t>(want + want / 4, 4096);
+    void* ptrs[] = {c->pi, c->pj, c->live, c->live_off, c->live_list, c->root, c->items,
+                    c->code, c->impact, c->first_code, c->first_impact, c->ci, c->cj, c->cn, c->cm};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    c->pair_cap = 0;
+    cudaError_t e = alloc(c->pi, cap);
+    if (e == cudaSuccess) e = alloc(c->pj, cap);
+    if (e == cudaSuccess) e = alloc(c->live, cap);
+    if (e == cudaSuccess) e = alloc(c->live_off, cap + 1);
+    if (e == cudaSuccess) e = alloc(c->live_list, cap);
+    if (e == cudaSuccess) e = alloc(c->root, cap);
+    if (e == cudaSuccess) e = alloc(c->items, cap);
+    if (e == cudaSuccess) e = alloc(c->code, cap);
+    if (e == cudaSuccess) e = alloc(c->impact, cap);
+    if (e == cudaSuccess) e = alloc(c->first_code, cap);
+    if (e == cudaSuccess) e = alloc(c->first_impact, cap);
+    if (e == cudaSuccess) e = alloc(c->ci, cap);
+    if (e == cudaSuccess) e = alloc(c->cj, cap);
+    if (e == cudaSuccess) e = alloc(c->cn, cap);
+    if (e == cudaSuccess) e = alloc(c->cm, cap);
+    if (e == cudaSuccess) c->pair_cap = cap;
+    return e;
+}
+
+cudaError_t ensure_large(ContactState* c, size_t entries) {
+    if (entries <= c->large_cap && c->ent_id) return cudaSuccess;
+    if (c->ent_id) cudaFree(c->ent_id);
+    if (c->ent_next) cudaFree(c->ent_next);
+    if (c->keys2) cudaFree(c->keys2);
+    if (c->heads2) cudaFree(c->heads2);
+    c->ent_id = c->ent_next = c->heads2 = nullptr;
+    c->keys2 = nullptr;
+    c->large_cap = 0;
+    const size_t cap = std::max<size_t>(entries + entries / 4, 4096);
+    c->table2 = pow2_at_least(2 * cap);
+    cudaError_t e = alloc(c->ent_id, cap);
+    if (e == cudaSuccess) e = alloc(c->ent_next, cap);
+    if (e == cudaSuccess) e = alloc(c->keys2, c->table2);
+    if (e == cudaSuccess) e = alloc(c->heads2, c->table2);
+    if (e == cudaSuccess) c->large_cap = cap;
+    return e;
+}
+
+int32_t read_scalars(vx_scene* s, ContactState* c, const char* what) {
+    cudaError_t e = cudaMemcpyAsync(c->h_scal, c->scal, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->h_scal + 16, c->max_move, sizeof(unsigned long long),
+                                              cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    const uint32_t err = c->h_scal[S_ERR];
+    if (err & E_RANGE) {
+        set_error("%s: a position is non-finite or farther than %d cells from the origin", what, kCoordLimit - 2);
+        return VX_NONFINITE;
+    }
+    if (err & E_VOLUME) {
+        set_error("%s: a REV swept more than %llu bins in one substep", what, (unsigned long long)kMaxLargeVolume);
+        return VX_BAD_INPUT;
+    }
+    if (err & (E_TABLE | E_UNION)) {
+        set_error("%s: a hash probe or a union exceeded its bound", what);
+        return VX_TIMEOUT;
+    }
+    return VX_OK;
+}
+
+// Components of the listed items over shared REVs: comp_off (by root REV) and
+// items grouped per component (unsorted inside a component).
+cudaError_t components(vx_scene* s, ContactState* c, uint32_t count, const uint32_t* list, const uint32_t* ia,
+                       const uint32_t* ja, uint32_t* grouped) {
+    const uint32_t n = s->n;
+    cudaStream_t st = s->stream;
+    k_iota<<<grid(n), 256, 0, st>>>(n, c->parent);
+    cudaError_t e = cudaMemsetAsync(c->comp_cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+    if (e != cudaSuccess || count == 0) {
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->comp_off, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+        return e;
+    }
+    k_union<<<grid(count), 256, 0, st>>>(count, list, ia, ja, c->parent, c->scal);
+    k_roots<<<grid(count), 256, 0, st>>>(count, list, ia, c->parent, c->root, c->comp_cnt);
+    e = scan(c, st, c->comp_cnt, c->comp_off, n);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->comp_cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    k_fill<<<grid(count), 256, 0, st>>>(count, list, c->root, c->comp_off, c->comp_cnt, grouped);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+void contact_release(vx_scene* s) {
+    ContactState* c = s->contact;
+    if (!c) return;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->start, c->snap, c->move, c->heat, c->phys, c->next1,
+                    c->cnt, c->off, c->parent, c->comp_cnt, c->comp_off, c->bsum, c->keys1, c->heads1, c->keys2,
+                    c->heads2, c->ent_id, c->ent_next, c->pi, c->pj, c->live, c->live_off, c->live_list, c->root,
+                    c->items, c->code, c->impact, c->first_code, c->first_impact, c->ci, c->cj, c->cn, c->cm,
+                    c->scal, c->max_move, c->heat_sum};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (c->h_scal) cudaFreeHost(c->h_scal);
+    delete c;
+    s->contact = nullptr;
+}
+
+// collision::project over the scene's positions, with its previous positions
+// as the swept starts; targeted axes have zero inverse mass.
+int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
+    const char* what = "vx_contact_project";
+    vx_contact_stats st_out{};
+    cudaError_t e = ensure_state(s);
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return VX_OOM;
+    }
+    ContactState* c = s->contact;
+    const uint32_t n = s->n;
+    cudaStream_t st = s->stream;
+    c->contacts = 0;
+    if (n < 2) {
+        if (out) *out = st_out;
+        return VX_OK;
+    }
+    const size_t v3b = 3 * (size_t)n * sizeof(double);
+    e = cudaMemcpyAsync(c->start, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->keys1, 0xFF, (size_t)c->table1 * sizeof(unsigned long long), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->heads1, 0xFF, (size_t)c->table1 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    k_boxes<<<grid(n), 256, 0, st>>>(n, s->pos, c->start, c->box, c->scal);
+    k_insert_corners<<<grid(n), 256, 0, st>>>(n, c->box, c->keys1, c->heads1, c->next1, c->table1 - 1, c->scal);
+    int32_t r = read_scalars(s, c, what);
+    if (r != VX_OK) return r;
+    const uint32_t large = c->h_scal[S_LARGE];
+    uint32_t mask2 = 0;
+    if (large) {
+        k_large_volume<<<grid(n), 256, 0, st>>>(n, c->box, c->cnt, c->scal);
+        e = scan(c, st, c->cnt, c->off, n);
+        uint32_t entries = 0;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        r = read_scalars(s, c, what);
+        if (r != VX_OK) return r;
+        entries = c->h_scal[18];
+        e = ensure_large(c, entries);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->keys2, 0xFF, (size_t)c->table2 * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->heads2, 0xFF, (size_t)c->table2 * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        k_insert_large<<<grid(n), 256, 0, st>>>(n, c->box, c->off, c->keys2, c->heads2, c->ent_id, c->ent_next,
+                                                 c->table2 - 1, c->scal);
+        mask2 = c->table2 - 1;
+    }
+    PairArgs pa{};
+    pa.n = n;
+    pa.b = c->box;
+    pa.kin = s->kin;
+    pa.rest = s->rest;
+    pa.nbr = s->nbr;
+    pa.rev = s->rev;
+    pa.keys1 = c->keys1;
+    pa.heads1 = c->heads1;
+    pa.next1 = c->next1;
+    pa.mask1 = c->table1 - 1;
+    pa.keys2 = c->keys2;
+    pa.heads2 = c->heads2;
+    pa.ent_id = c->ent_id;
+    pa.ent_next = c->ent_next;
+    pa.mask2 = mask2;
+    pa.wx = std::max<int32_t>(1, (int32_t)c->h_scal[S_EXT]);
+    pa.wy = std::max<int32_t>(1, (int32_t)c->h_scal[S_EXT + 1]);
+    pa.wz = std::max<int32_t>(1, (int32_t)c->h_scal[S_EXT + 2]);
+    pa.count = c->cnt;
+    pa.off = c->off;
+    pa.scal = c->scal;
+    e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
+    e = scan(c, st, c->cnt, c->off, n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    r = read_scalars(s, c, what);
+    if (r != VX_OK) return r;
+    const uint32_t pairs = c->h_scal[18];
+    st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
+    st_out.pairs = pairs;
+    e = ensure_pairs(c, pairs);
+    if (e != cudaSuccess) {
+        set_error("%s: %u pairs: %s", what, pairs, cudaGetErrorString(e));
+        return VX_OOM;
+    }
+    pa.pi = c->pi;
+    pa.pj = c->pj;
+    e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+    if (e == cudaSuccess && pairs) e = cudaMemsetAsync(c->first_code, 0, pairs, st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    if (pairs) {
+        k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
+        k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
+    }
+    // the sweeps (project :51-103)
+    SweepArgs sa{};
+    sa.n = n;
+    sa.comp_off = c->comp_off;
+    sa.items = c->items;
+    sa.pi = c->pi;
+    sa.pj = c->pj;
+    sa.pos = s->pos;
+    sa.prev = s->prev;
+    sa.start = c->start;
+    sa.kin = s->kin;
+    sa.param1 = s->param1;
+    sa.tmask = s->tmask;
+    sa.move = c->move;
+    sa.code = c->code;
+    sa.impact = c->impact;
+    sa.scal = c->scal;
+    const double base_bound = 1e-3;  // M: metres a REV may move in one sweep
+    if (!pairs) st_out.sweeps = 1;   // the reference's first sweep runs over an empty list
+    for (int sweep = 0; sweep < 6 && pairs; ++sweep) {
+        st_out.sweeps += 1;
+        e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        double bound = base_bound;
+        bool changed = false;
+        for (int attempt = 0;; ++attempt) {
+            const bool all_live = attempt >= 4;
+            const double half = all_live ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9;
+            e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            k_classify<<<grid(pairs), 256, 0, st>>>(pairs, c->pi, c->pj, n, s->pos, c->start, half, c->live);
+            e = scan(c, st, c->live, c->live_off, pairs);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            k_compact<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->live_list);
+            e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            const uint32_t live = c->h_scal[18];
+            st_out.live_max = std::max(st_out.live_max, live);
+            e = components(s, c, live, c->live_list, c->pi, c->pj, c->items);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            if (live) k_sweep<<<grid(n), 256, 0, st>>>(sa);
+            k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
+            r = read_scalars(s, c, what);
+            if (r != VX_OK) return r;
+            unsigned long long bits = (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
+            double moved = 0.0;
+            std::memcpy(&moved, &bits, sizeof moved);
+            changed = c->h_scal[S_CHANGED] != 0;
+            if (all_live || moved <= bound) {
+                if (live) k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
+                                                              c->first_impact);
+                break;
+            }
+            // a REV moved farther than the bound: replay from the sweep's start
+            st_out.redone += 1;
+            e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            bound = std::max(2.0 * moved, 4.0 * bound);
+        }
+        if (!changed) break;
+    }
+    // contacts in pair order
+    if (pairs) {
+        k_contact_flags<<<grid(pairs), 256, 0, st>>>(pairs, c->first_code, c->live);
+        e = scan(c, st, c->live, c->live_off, pairs);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        k_contact_write<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->pi, c->pj, c->first_code,
+                                                     c->first_impact, c->ci, c->cj, c->cn, c->cm);
+        e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        c->contacts = c->h_scal[18];
+    }
+    st_out.contacts = c->contacts;
+    if (out) *out = st_out;
+    return VX_OK;
+}
+
+// resolve_velocities_with_precontact over the contacts of the last projection
+// (or those set by vx_scene_set_contacts); pre_contact = NULL uses the current
+// velocities (resolve_velocities, :122-131).
+int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restitution, double friction,
+                        vx_contact_heat* out) {
+    const char* what = "vx_contact_resolve_velocities";
+    cudaError_t e = ensure_state(s);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    ContactState* c = s->contact;
+    const uint32_t n = s->n, count = c->contacts;
+    cudaStream_t st = s->stream;
+    vx_contact_heat heat{};
+    if (count && n) {
+        const size_t v3b = 3 * (size_t)n * sizeof(double);
+        e = cudaMemcpyAsync(c->phys, pre_contact ? pre_contact : s->vel, v3b, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->heat, 0, 2 * (size_t)n * sizeof(double), st);
+        if (e == cudaSuccess) e = components(s, c, count, nullptr, c->ci, c->cj, c->items);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        ResolveArgs ra{};
+        ra.n = n;
+        ra.comp_off = c->comp_off;
+        ra.items = c->items;
+        ra.ci = c->ci;
+        ra.cj = c->cj;
+        ra.cn = c->cn;
+        ra.cm = c->cm;
+        ra.vel = s->vel;
+        ra.phys = c->phys;
+        ra.kin = s->kin;
+        ra.param1 = s->param1;
+        ra.tmask = s->tmask;
+        ra.restitution = restitution;
+        ra.friction = friction;
+        ra.heat = c->heat;
+        k_resolve<<<grid(n), 256, 0, st>>>(ra);
+        k_sum<<<1, 256, 0, st>>>(n, c->heat, c->heat_sum);
+        k_sum<<<1, 256, 0, st>>>(n, c->heat + n, c->heat_sum + 1);
+        double h[2] = {0.0, 0.0};
+        e = cudaMemcpyAsync(h, c->heat_sum, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        int32_t r = read_scalars(s, c, what);
+        if (r != VX_OK) return r;
+        heat.restitution = h[0];
+        heat.friction = h[1];
+    }
+    if (out) *out = heat;
+    return VX_OK;
+}
+
+uint32_t contact_count(const vx_scene* s) { return s->contact ? s->contact->contacts : 0; }
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" int32_t vx_contact_project(vx_scene* s, vx_contact_stats* out) {
+    clear_error();
+    if (!s) {
+        set_error("vx_contact_project: null scene");
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(s->device);
+    return contact_project(s, out);
+}
+
+extern "C" int32_t vx_contact_resolve_velocities(vx_scene* s, int32_t pre_contact, double restitution,
+                                                 double friction, vx_contact_heat* out) {
+    clear_error();
+    if (!s || pre_contact < 0 || pre_contact > 1) {
+        set_error("vx_contact_resolve_velocities: null scene or unknown pre_contact %d", pre_contact);
+        return VX_BAD_INPUT;
+    }
+    if (!std::isfinite(restitution) || !std::isfinite(friction)) {
+        set_error("vx_contact_resolve_velocities: non-finite restitution or friction");
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(s->device);
+    return contact_resolve(s, pre_contact ? s->drift : nullptr, restitution, friction, out);
+}
+
+extern "C" int32_t vx_scene_get_contacts(vx_scene* s, uint32_t capacity, uint32_t* i, uint32_t* j, int32_t* normal,
+                                         uint8_t* new_impact, uint32_t* out_count) {
+    clear_error();
+    if (!s) {
+        set_error("vx_scene_get_contacts: null scene");
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(s->device);
+    const uint32_t count = contact_count(s);
+    if (out_count) *out_count = count;
+    if (count == 0 || capacity == 0) return VX_OK;
+    if (capacity < count) {
+        set_error("vx_scene_get_contacts: %u contacts, capacity %u", count, capacity);
+        return VX_BAD_INPUT;
+    }
+    ContactState* c = s->contact;
+    std::vector<int8_t> cn(count);
+    cudaError_t e = cudaSuccess;
+    if (i) e = cudaMemcpyAsync(i, c->ci, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && j) e = cudaMemcpyAsync(j, c->cj, count * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && normal) e = cudaMemcpyAsync(cn.data(), c->cn, count, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess && new_impact) e = cudaMemcpyAsync(new_impact, c->cm, count, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "vx_scene_get_contacts");
+    if (normal)
+        for (uint32_t k = 0; k < count; ++k) normal[k] = cn[k];
+    return VX_OK;
+}
+
+extern "C" int32_t vx_scene_set_contacts(vx_scene* s, uint32_t count, const uint32_t* i, const uint32_t* j,
+                                         const int32_t* normal, const uint8_t* new_impact) {
+    clear_error();
+    if (!s || (count && (!i || !j || !normal || !new_impact))) {
+        set_error("vx_scene_set_contacts: null argument");
+        return VX_BAD_INPUT;
+    }
+    for (uint32_t k = 0; k < count; ++k) {
+        const int32_t a = normal[k] > 0 ? normal[k] : -normal[k];
+        if (i[k] >= s->n || j[k] >= s->n || i[k] == j[k] || a < 1 || a > 3) {
+            set_error("vx_scene_set_contacts: contact %u (%u, %u, normal %d) is invalid", k, i[k], j[k], normal[k]);
+            return VX_BAD_INPUT;
+        }
+    }
+    cudaSetDevice(s->device);
+    cudaError_t e = ensure_state(s);
+    if (e == cudaSuccess) e = ensure_pairs(s->contact, count);
+    if (e != cudaSuccess) return cuda_fail(e, "vx_scene_set_contacts");
+    ContactState* c = s->contact;
+    std::vector<int8_t> cn(count);
+    for (uint32_t k = 0; k < count; ++k) cn[k] = (int8_t)normal[k];
+    if (count) {
+        e = cudaMemcpyAsync(c->ci, i, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->cj, j, count * sizeof(uint32_t), cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->cn, cn.data(), count, cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->cm, new_impact, count, cudaMemcpyHostToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "vx_scene_set_contacts");
+    }
+    c->contacts = count;
+    return VX_OK;
+}

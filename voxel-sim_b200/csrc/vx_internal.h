@@ -12,6 +12,8 @@
 
 namespace vx {
 
+struct ContactState;  // grow-only buffers of the contact stage (vx_contact.cu)
+
 // Thread-local error message returned by vx_last_error().
 void set_error(const char* fmt, ...);
 void clear_error();
@@ -128,6 +130,8 @@ struct vx_scene {
     double* vel;                  // [3][n] velocity, m/s (Voxel::velocity)
     double* prev;                 // [3][n] positions at the start of the substep (Scene::previous)
     double* drift;                // [3][n] predicted velocity of the substep (drift_velocity)
+    float* rest;                  // [3][n] creation positions (Scene::rest_positions)
+    vx::ContactState* contact = nullptr;  // allocated by the first contact call
     double* save_pos;             // [3][n] checkpoint
     double4* save_rot;            // [n]
     float* out_ratio;             // [3n] bond stress outputs

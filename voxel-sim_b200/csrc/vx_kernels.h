@@ -56,6 +56,14 @@ cudaError_t launch_gather3(vx_scene* s, uint32_t count, const uint32_t* d_index,
 cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index, const double* d_value,
                             double* field);
 // connected components of the bond graph with the reference's cluster numbering (vx_clusters.cu)
+// collision::project and resolve_velocities_with_precontact (vx_contact.cu)
+int32_t contact_project(vx_scene* s, vx_contact_stats* out);
+int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restitution, double friction,
+                        vx_contact_heat* out);
+uint32_t contact_count(const vx_scene* s);
+void contact_release(vx_scene* s);
+cudaError_t launch_rest_positions(vx_scene* s);
+
 cudaError_t launch_rebuild_clusters(vx_scene* s);
 uint32_t cluster_scan_blocks(uint32_t n);
 // fracture stage: fracture::update on every bond of the last assembly (dt = substep)

@@ -1060,6 +1060,10 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
                   prm->fixed_dt, prm->substeps, prm->corotation_iterations);
         return VX_BAD_INPUT;
     }
+    if (prm->contact) {
+        set_error("vx_pool_step: the contact stage runs on single scenes (vx_scene_step) only");
+        return VX_BAD_INPUT;
+    }
     cudaSetDevice(p->s.device);
     const uint32_t S = p->slots;
     const double h = prm->fixed_dt / (double)prm->substeps;

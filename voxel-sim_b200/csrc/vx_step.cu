@@ -138,6 +138,19 @@ cudaError_t launch_predict(vx_scene* s, const double* gravity, double h) {
     return cudaGetLastError();
 }
 
+__global__ void k_rest_positions(size_t count, const double* __restrict__ pos, float* __restrict__ rest) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t < count) rest[t] = (float)pos[t];
+}
+
+// Scene::rest_positions: the creation positions in f32 (src/scene.rs:520-522)
+cudaError_t launch_rest_positions(vx_scene* s) {
+    const size_t count = 3 * (size_t)s->n;
+    if (count == 0) return cudaSuccess;
+    k_rest_positions<<<(unsigned)((count + 255) / 256), 256, 0, s->stream>>>(count, s->pos, s->rest);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_velocity(vx_scene* s, double h) {
     if (s->n == 0) return cudaSuccess;
     k_velocity<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->n, s->pos, s->vel, s->prev, s->drift, s->pred, s->kin,
@@ -167,6 +180,11 @@ extern "C" int32_t vx_scene_step(vx_scene* s, const vx_step_params* p, vx_step_s
         !std::isfinite(p->gravity[0]) || !std::isfinite(p->gravity[1]) || !std::isfinite(p->gravity[2])) {
         set_error("vx_scene_step: invalid fixed_dt=%g, substeps=%u, corotation_iterations=%u or gravity",
                   p->fixed_dt, p->substeps, p->corotation_iterations);
+        return VX_BAD_INPUT;
+    }
+    if (p->contact && (!(p->restitution >= 0.0 && p->restitution <= 1.0) || !(p->friction >= 0.0) ||
+                       !std::isfinite(p->friction))) {
+        set_error("vx_scene_step: invalid restitution=%g or friction=%g", p->restitution, p->friction);
         return VX_BAD_INPUT;
     }
     cudaSetDevice(s->device);
@@ -205,6 +223,20 @@ extern "C" int32_t vx_scene_step(vx_scene* s, const vx_step_params* p, vx_step_s
             st.max_angle = angle;
             if (angle <= p->corotation_tolerance && st.residual <= p->pass.tolerance) break;
         }
+        // Velocities come from the solved positions (src/solver.rs:667-681), so
+        // they are formed before the contact projection moves positions; the
+        // fracture stage then reads the projected ones (src/solver.rs:575-665).
+        e = launch_velocity(s, h);
+        if (e != cudaSuccess) {
+            set_error("vx_scene_step: velocity update failed: %s", cudaGetErrorString(e));
+            return VX_CUDA_ERROR;
+        }
+        if (p->contact) {
+            vx_contact_stats cs{};
+            r = contact_project(s, &cs);
+            if (r != VX_OK) return r;
+            st.contacts += cs.contacts;
+        }
         if (p->fracture) {
             vx_dissipation d{};
             uint32_t broken = 0;
@@ -217,8 +249,14 @@ extern "C" int32_t vx_scene_step(vx_scene* s, const vx_step_params* p, vx_step_s
             st.dissipation.damage_heat += d.damage_heat;
             st.dissipation.released += d.released;
         }
-        e = launch_velocity(s, h);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (p->contact) {
+            vx_contact_heat heat{};
+            r = contact_resolve(s, s->drift, p->restitution, p->friction, &heat);
+            if (r != VX_OK) return r;
+            st.restitution_heat += heat.restitution;
+            st.friction_heat += heat.friction;
+        }
+        e = cudaStreamSynchronize(s->stream);
         if (e != cudaSuccess) {
             set_error("vx_scene_step: velocity update failed: %s", cudaGetErrorString(e));
             return VX_CUDA_ERROR;

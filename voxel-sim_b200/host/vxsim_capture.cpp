@@ -13,9 +13,10 @@
 // shortest decimal form that reads back to the same f32 (Rust's `{}`). The
 // scene settings are SceneConfig::default with dimensions 36 x 32 x 32 and
 // fixed_dt 1 ms, or those of a RON scene file given as the fourth argument.
-// Contact between the block and the fixed layer (collision::project) is not
-// part of the device step: the two are not bonded (their kinematic flags
-// differ), so the block is carried only by its own lattice.
+// The block and the fixed layer are not bonded (their kinematic flags
+// differ): the block stands on the layer through the contact stage of the
+// step (collision::project and the contact velocities). VXSIM_PRECISION=1
+// selects the mixed-precision solve.
 #include <charconv>
 #include <chrono>
 #include <cstdio>

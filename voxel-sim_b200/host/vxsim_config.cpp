@@ -525,6 +525,9 @@ SceneConfig SceneFileConfig::solver_config() const {
     c.fracture_config.fatigue_exponent = fracture.fatigue_exponent;
     c.fracture_config.fatigue_threshold = fracture.fatigue_threshold;
     c.fracture_config.plastic_heat_fraction = fracture.plastic_heat_fraction;
+    c.contact = true;
+    c.restitution = fracture.restitution;
+    c.friction = fracture.friction;
     return c;
 }
 

@@ -292,6 +292,9 @@ int32_t step_with_axis_targets_and_loads(Scene& s, const std::vector<AxisTargets
     p.pass.kernel = s.config.kernel;
     p.fracture = s.config.fracture ? 1 : 0;
     p.fracture_config = s.config.fracture_config;
+    p.contact = s.config.contact ? 1 : 0;
+    p.restitution = s.config.restitution;
+    p.friction = s.config.friction;
     r = vx_scene_step(s.handle(), &p, &s.last_step);
     if (r != VX_OK && r != VX_NOT_CONVERGED) return r;
     s.solver_residual = s.last_step.residual;

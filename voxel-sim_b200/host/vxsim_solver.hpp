@@ -60,6 +60,10 @@ struct SceneConfig {
     // with FractureConfig::default (src/fracture.rs:27-42) in its f32 values
     bool fracture = true;
     vx_fracture_config fracture_config{35.0, (double)0.005f, 1000.0, 3.0, 0.5, (double)0.9f};
+    // collision::project and the contact velocities (src/solver.rs:575-690)
+    bool contact = true;
+    float restitution = 0.1f;  // FractureConfig::restitution
+    float friction = 0.35f;    // FractureConfig::friction
 };
 
 // One REV of a lattice built from cells (Scene::from_voxels, src/scene.rs:445-573).

@@ -90,18 +90,35 @@ class VxDissipation(C.Structure):
 class VxStepParams(C.Structure):
     _fields_ = [("fixed_dt", C.c_double), ("substeps", C.c_uint32), ("corotation_iterations", C.c_uint32),
                 ("corotation_tolerance", C.c_double), ("gravity", C.c_double * 3), ("pass_", VxPassParams),
-                ("fracture", C.c_int32), ("fracture_config", VxFractureConfig)]
+                ("fracture", C.c_int32), ("fracture_config", VxFractureConfig), ("contact", C.c_int32),
+                ("restitution", C.c_double), ("friction", C.c_double)]
 
 
 class VxStepStats(C.Structure):
     _fields_ = [("passes", C.c_uint32), ("pcg_iterations", C.c_uint32), ("residual", C.c_double),
                 ("max_angle", C.c_double), ("converged", C.c_int32), ("broken", C.c_uint32),
-                ("dissipation", VxDissipation)]
+                ("dissipation", VxDissipation), ("contacts", C.c_uint32), ("restitution_heat", C.c_double),
+                ("friction_heat", C.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}
         d["dissipation"] = self.dissipation.as_dict()
         return d
+
+
+class VxContactStats(C.Structure):
+    _fields_ = [("candidates", C.c_uint64), ("pairs", C.c_uint64), ("contacts", C.c_uint32), ("sweeps", C.c_uint32),
+                ("live_max", C.c_uint32), ("redone", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class VxContactHeat(C.Structure):
+    _fields_ = [("restitution", C.c_double), ("friction", C.c_double)]
+
+
+FIELD_POSITION, FIELD_VELOCITY, FIELD_PREVIOUS = 0, 1, 2
 
 
 class VxTuneResult(C.Structure):
@@ -149,11 +166,12 @@ class VxServerStats(C.Structure):
 
 def step_params(fixed_dt, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5, gravity=(0.0, 0.0, 0.0),
                 tolerance=1e-5, max_iterations=10000, precision=PRECISION_FP64, reuse=False, inner_tolerance=0.0,
-                max_outer=0, kernel=KERNEL_AUTO, fracture=False, fracture_cfg=None) -> VxStepParams:
+                max_outer=0, kernel=KERNEL_AUTO, fracture=False, fracture_cfg=None, contact=False,
+                restitution=0.1, friction=0.35) -> VxStepParams:
     return VxStepParams(fixed_dt, substeps, corotation_iterations, corotation_tolerance, (C.c_double * 3)(*gravity),
                         VxPassParams(fixed_dt / substeps, tolerance, max_iterations, precision, int(reuse),
                                      inner_tolerance, max_outer, kernel),
-                        int(fracture), fracture_cfg or fracture_config())
+                        int(fracture), fracture_cfg or fracture_config(), int(contact), restitution, friction)
 
 
 _lib = None
@@ -214,6 +232,13 @@ def load(path: Path | None = None):
     L.vx_scene_set_velocities.argtypes = [C.c_void_p, f64p]
     L.vx_scene_get_velocities.argtypes = [C.c_void_p, f64p]
     L.vx_scene_update_velocities.argtypes = [C.c_void_p, C.c_uint32, u32p, f64p, C.c_int32]
+    L.vx_scene_read_revs.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, u32p, f64p]
+    L.vx_scene_write_revs.argtypes = [C.c_void_p, C.c_int32, C.c_uint32, u32p, f64p]
+    L.vx_contact_project.argtypes = [C.c_void_p, C.POINTER(VxContactStats)]
+    L.vx_contact_resolve_velocities.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double,
+                                                C.POINTER(VxContactHeat)]
+    L.vx_scene_get_contacts.argtypes = [C.c_void_p, C.c_uint32, u32p, u32p, i32p, u8p, C.POINTER(C.c_uint32)]
+    L.vx_scene_set_contacts.argtypes = [C.c_void_p, C.c_uint32, u32p, u32p, i32p, u8p]
     for name in header_symbols():
         getattr(L, name)  # every declared entry point is exported
     _lib = L
@@ -439,6 +464,53 @@ class DeviceScene:
         out = np.zeros(3 * self.n, np.float64)
         check(load().vx_scene_get_velocities(self.h, _p(out, C.c_double)))
         return out.reshape(-1, 3)
+
+    def write_field(self, field, values, index=None):
+        """vx_scene_write_revs: every REV (index None) or the listed ones."""
+        idx = np.arange(self.n, dtype=np.uint32) if index is None else np.ascontiguousarray(index, np.uint32)
+        val = np.ascontiguousarray(values, np.float64).reshape(-1)
+        check(load().vx_scene_write_revs(self.h, field, len(idx), _p(idx, C.c_uint32), _p(val, C.c_double)))
+
+    def read_field(self, field, index=None) -> np.ndarray:
+        idx = np.arange(self.n, dtype=np.uint32) if index is None else np.ascontiguousarray(index, np.uint32)
+        out = np.zeros(3 * len(idx), np.float64)
+        check(load().vx_scene_read_revs(self.h, field, len(idx), _p(idx, C.c_uint32), _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def contact_project(self) -> dict:
+        """vx_contact_project (collision::project) over the current positions,
+        with the previous positions as the swept starts."""
+        st = VxContactStats()
+        check(load().vx_contact_project(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def contacts(self) -> np.ndarray:
+        """The current contacts as a structured array (i, j, normal, new_impact)."""
+        cnt = C.c_uint32()
+        check(load().vx_scene_get_contacts(self.h, 0, None, None, None, None, C.byref(cnt)))
+        k = cnt.value
+        i, j, nrm, imp = (np.zeros(max(k, 1), np.uint32), np.zeros(max(k, 1), np.uint32),
+                          np.zeros(max(k, 1), np.int32), np.zeros(max(k, 1), np.uint8))
+        if k:
+            check(load().vx_scene_get_contacts(self.h, k, _p(i, C.c_uint32), _p(j, C.c_uint32), _p(nrm, C.c_int32),
+                                               _p(imp, C.c_uint8), C.byref(cnt)))
+        out = np.zeros(k, dtype=[("i", "<u4"), ("j", "<u4"), ("normal", "<i4"), ("new_impact", "<i4")])
+        out["i"], out["j"], out["normal"], out["new_impact"] = i[:k], j[:k], nrm[:k], imp[:k]
+        return out
+
+    def set_contacts(self, contacts):
+        c = np.asarray(contacts)
+        i = np.ascontiguousarray(c["i"], np.uint32)
+        j = np.ascontiguousarray(c["j"], np.uint32)
+        nrm = np.ascontiguousarray(c["normal"], np.int32)
+        imp = np.ascontiguousarray(c["new_impact"], np.uint8)
+        check(load().vx_scene_set_contacts(self.h, len(i), _p(i, C.c_uint32), _p(j, C.c_uint32),
+                                           _p(nrm, C.c_int32), _p(imp, C.c_uint8)))
+
+    def resolve_contact_velocities(self, restitution, friction, pre_contact=0):
+        heat = VxContactHeat()
+        check(load().vx_contact_resolve_velocities(self.h, pre_contact, restitution, friction, C.byref(heat)))
+        return heat.restitution, heat.friction
 
     def update_velocities(self, index, values, add=False):
         idx = np.ascontiguousarray(index, np.uint32).reshape(-1)
