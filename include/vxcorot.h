@@ -339,6 +339,7 @@ typedef struct vx_contact_stats {
     uint32_t sweeps;
     uint32_t live_max;    /* most pairs replayed in one sweep */
     uint32_t redone;      /* sweeps replayed with a wider movement bound */
+    uint32_t launches;    /* kernels launched by the call */
 } vx_contact_stats;
 typedef struct vx_contact_heat {
     double restitution;  /* J, kinetic loss of the normal impulses */

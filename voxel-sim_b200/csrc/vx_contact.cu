@@ -498,13 +498,22 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
     return x;
 }
 
-// Joins the two REVs of each listed item (pairs or contacts).
+// A REV whose every axis has zero inverse mass (kinematic, or all three axes
+// targeted) is never moved by a correction or an impulse: items that share
+// only such REVs do not depend on one another.
+__device__ __forceinline__ bool movable(const uint8_t* kin, const uint8_t* tmask, uint32_t i) {
+    return !kin[i] && (tmask[i] & 7u) != 7u;
+}
+
+// Joins the two REVs of each listed item (pairs or contacts) when both can move.
 __global__ void k_union(uint32_t count, const uint32_t* __restrict__ items, const uint32_t* __restrict__ ia,
-                        const uint32_t* __restrict__ ja, uint32_t* parent, uint32_t* scal) {
+                        const uint32_t* __restrict__ ja, const uint8_t* __restrict__ kin,
+                        const uint8_t* __restrict__ tmask, uint32_t* parent, uint32_t* scal) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const uint32_t k = items ? items[t] : t;
     const uint32_t i = ia[k], j = ja[k];
+    if (!movable(kin, tmask, i) || !movable(kin, tmask, j)) return;
     for (unsigned tries = 0; tries < kUnionRetries; ++tries) {
         const uint32_t ri = uf_find(parent, i), rj = uf_find(parent, j);
         if (ri == rj) return;
@@ -514,14 +523,18 @@ __global__ void k_union(uint32_t count, const uint32_t* __restrict__ items, cons
     atomicOr(scal + S_ERR, E_UNION);
 }
 
-// After the unions: each item's component root (read-only walk) and the
-// component sizes.
+// After the unions: each item's component root (read-only walk from a REV
+// that can move, else from its first REV) and the component sizes.
 __global__ void k_roots(uint32_t count, const uint32_t* __restrict__ items, const uint32_t* __restrict__ ia,
-                        const uint32_t* __restrict__ parent, uint32_t* __restrict__ root, uint32_t* comp_count) {
+                        const uint32_t* __restrict__ ja, const uint8_t* __restrict__ kin,
+                        const uint8_t* __restrict__ tmask, const uint32_t* __restrict__ parent,
+                        uint32_t* __restrict__ root, uint32_t* comp_count) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const uint32_t k = items ? items[t] : t;
-    uint32_t x = ia[k], p = parent[x];
+    const uint32_t i = ia[k], j = ja[k];
+    uint32_t x = (movable(kin, tmask, i) || !movable(kin, tmask, j)) ? i : j;
+    uint32_t p = parent[x];
     while (p != x) {
         x = p;
         p = parent[p];
@@ -538,15 +551,41 @@ __global__ void k_fill(uint32_t count, const uint32_t* __restrict__ items, const
     out[comp_off[r] + atomicAdd(comp_cursor + r, 1u)] = items ? items[t] : t;
 }
 
+// Ascending sort of v[b, e): insertion sort for short ranges, heapsort for
+// long ones (a large component is replayed by one thread).
 __device__ void sort_range(uint32_t* v, uint32_t b, uint32_t e) {
-    for (uint32_t k = b + 1; k < e; ++k) {
-        const uint32_t x = v[k];
-        uint32_t m = k;
-        while (m > b && v[m - 1] > x) {
-            v[m] = v[m - 1];
-            --m;
+    const uint32_t len = e - b;
+    if (len <= 32) {
+        for (uint32_t k = b + 1; k < e; ++k) {
+            const uint32_t x = v[k];
+            uint32_t m = k;
+            while (m > b && v[m - 1] > x) {
+                v[m] = v[m - 1];
+                --m;
+            }
+            v[m] = x;
         }
-        v[m] = x;
+        return;
+    }
+    uint32_t* a = v + b;
+    auto sift = [a](uint32_t root, uint32_t end) {
+        for (;;) {
+            uint32_t child = 2 * root + 1;
+            if (child >= end) return;
+            if (child + 1 < end && a[child] < a[child + 1]) ++child;
+            if (!(a[root] < a[child])) return;
+            const uint32_t t = a[root];
+            a[root] = a[child];
+            a[child] = t;
+            root = child;
+        }
+    };
+    for (uint32_t k = len / 2; k-- > 0;) sift(k, len);
+    for (uint32_t end = len - 1; end > 0; --end) {
+        const uint32_t t = a[0];
+        a[0] = a[end];
+        a[end] = t;
+        sift(0, end);
     }
 }
 
@@ -577,14 +616,20 @@ __device__ bool separate(const SweepArgs& a, uint32_t i, uint32_t j, int code, d
     if (denom <= 0.0) return false;
     const double s = code > 0 ? 1.0 : -1.0;
     const double di = -s * (amount * wi / denom), dj = s * (amount * wj / denom);
-    // the other two components of -normal * x and normal * x are signed
-    // zeros: adding them leaves every coordinate unchanged
-    add3(a.pos, a.n, i, axis, di);
-    add3(a.pos, a.n, j, axis, dj);
-    add3(a.prev, a.n, i, axis, di);
-    add3(a.prev, a.n, j, axis, dj);
-    a.move[i] += fabs(di);
-    a.move[j] += fabs(dj);
+    // The other two components of -normal * x and normal * x, and the whole
+    // correction of an endpoint with zero inverse mass on this axis, are
+    // signed zeros: adding them leaves every coordinate unchanged, so only the
+    // moving endpoints are written.
+    if (wi > 0.0) {
+        add3(a.pos, a.n, i, axis, di);
+        add3(a.prev, a.n, i, axis, di);
+        a.move[i] += fabs(di);
+    }
+    if (wj > 0.0) {
+        add3(a.pos, a.n, j, axis, dj);
+        add3(a.prev, a.n, j, axis, dj);
+        a.move[j] += fabs(dj);
+    }
     return true;
 }
 
@@ -737,9 +782,11 @@ __global__ void k_resolve(ResolveArgs a) {
                     rh = fmax(physical_impulse * -heat_closing - 0.5 * (physical_impulse * physical_impulse) * denom,
                               0.0);
                 if (rh > 0.0) rheat += rh;
+                // an endpoint with zero inverse mass on the normal axis keeps
+                // its physical velocity (the update is a signed zero)
                 for (int q = 0; q < 3; ++q) {
-                    a.phys[(size_t)q * n + i] = qi[q] - nrm[q] * (physical_impulse * wi);
-                    a.phys[(size_t)q * n + j] = qj[q] + nrm[q] * (physical_impulse * wj);
+                    if (wi > 0.0) a.phys[(size_t)q * n + i] = qi[q] - nrm[q] * (physical_impulse * wi);
+                    if (wj > 0.0) a.phys[(size_t)q * n + j] = qj[q] + nrm[q] * (physical_impulse * wj);
                 }
                 changed = true;
             }
@@ -770,9 +817,12 @@ __global__ void k_resolve(ResolveArgs a) {
                     }
                 }
             }
+            // REVs that cannot move keep their velocities (every update to them
+            // is a signed zero); they may be shared with other components
+            const bool mi = movable(a.kin, a.tmask, i), mj = movable(a.kin, a.tmask, j);
             for (int q = 0; q < 3; ++q) {
-                a.vel[(size_t)q * n + i] = vi[q];
-                a.vel[(size_t)q * n + j] = vj[q];
+                if (mi) a.vel[(size_t)q * n + i] = vi[q];
+                if (mj) a.vel[(size_t)q * n + j] = vj[q];
             }
         }
         if (!changed) break;
@@ -908,6 +958,7 @@ struct ContactState {
     int8_t* cn = nullptr;
     uint8_t* cm = nullptr;
     uint32_t contacts = 0;
+    uint32_t launches = 0;  // kernels launched by the current call
     // scalars: [0] error bits, [1..3] small extents, [4] large count, [5] changed,
     // [6..7] candidate count (u64); max movement (u64 bits of a double); the
     // host copies
@@ -956,6 +1007,7 @@ cudaError_t scan(ContactState* c, cudaStream_t st, const T* in, uint32_t* out, u
     k_scan_blocks<T><<<nb, 256, 0, st>>>(count, in, out, c->bsum);
     k_scan_sums<<<1, 1024, 0, st>>>(nb, c->bsum);
     k_scan_add<<<grid(count), 256, 0, st>>>(count, out, c->bsum, nb);
+    c->launches += 3;
     return cudaGetLastError();
 }
 
@@ -1072,13 +1124,15 @@ cudaError_t components(vx_scene* s, ContactState* c, uint32_t count, const uint3
     const uint32_t n = s->n;
     cudaStream_t st = s->stream;
     k_iota<<<grid(n), 256, 0, st>>>(n, c->parent);
+    c->launches += 1;
     cudaError_t e = cudaMemsetAsync(c->comp_cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
     if (e != cudaSuccess || count == 0) {
         if (e == cudaSuccess) e = cudaMemsetAsync(c->comp_off, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
         return e;
     }
-    k_union<<<grid(count), 256, 0, st>>>(count, list, ia, ja, c->parent, c->scal);
-    k_roots<<<grid(count), 256, 0, st>>>(count, list, ia, c->parent, c->root, c->comp_cnt);
+    k_union<<<grid(count), 256, 0, st>>>(count, list, ia, ja, s->kin, s->tmask, c->parent, c->scal);
+    k_roots<<<grid(count), 256, 0, st>>>(count, list, ia, ja, s->kin, s->tmask, c->parent, c->root, c->comp_cnt);
+    c->launches += 3;
     e = scan(c, st, c->comp_cnt, c->comp_off, n);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->comp_cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
@@ -1119,6 +1173,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     const uint32_t n = s->n;
     cudaStream_t st = s->stream;
     c->contacts = 0;
+    c->launches = 0;
     if (n < 2) {
         if (out) *out = st_out;
         return VX_OK;
@@ -1130,13 +1185,16 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     if (e == cudaSuccess) e = cudaMemsetAsync(c->heads1, 0xFF, (size_t)c->table1 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return cuda_fail(e, what);
     k_boxes<<<grid(n), 256, 0, st>>>(n, s->pos, c->start, c->box, c->scal);
+    c->launches += 1;
     k_insert_corners<<<grid(n), 256, 0, st>>>(n, c->box, c->keys1, c->heads1, c->next1, c->table1 - 1, c->scal);
+    c->launches += 1;
     int32_t r = read_scalars(s, c, what);
     if (r != VX_OK) return r;
     const uint32_t large = c->h_scal[S_LARGE];
     uint32_t mask2 = 0;
     if (large) {
         k_large_volume<<<grid(n), 256, 0, st>>>(n, c->box, c->cnt, c->scal);
+        c->launches += 1;
         e = scan(c, st, c->cnt, c->off, n);
         uint32_t entries = 0;
         if (e == cudaSuccess)
@@ -1152,6 +1210,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
         if (e != cudaSuccess) return cuda_fail(e, what);
         k_insert_large<<<grid(n), 256, 0, st>>>(n, c->box, c->off, c->keys2, c->heads2, c->ent_id, c->ent_next,
                                                  c->table2 - 1, c->scal);
+        c->launches += 1;
         mask2 = c->table2 - 1;
     }
     PairArgs pa{};
@@ -1179,6 +1238,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
     if (e != cudaSuccess) return cuda_fail(e, what);
     k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
+    c->launches += 1;
     e = scan(c, st, c->cnt, c->off, n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return cuda_fail(e, what);
@@ -1200,6 +1260,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     if (pairs) {
         k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
         k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
+        c->launches += 2;
     }
     // the sweeps (project :51-103)
     SweepArgs sa{};
@@ -1235,9 +1296,11 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
             if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
             if (e != cudaSuccess) return cuda_fail(e, what);
             k_classify<<<grid(pairs), 256, 0, st>>>(pairs, c->pi, c->pj, n, s->pos, c->start, half, c->live);
+            c->launches += 1;
             e = scan(c, st, c->live, c->live_off, pairs);
             if (e != cudaSuccess) return cuda_fail(e, what);
             k_compact<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->live_list);
+            c->launches += 1;
             e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return cuda_fail(e, what);
@@ -1245,8 +1308,12 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
             st_out.live_max = std::max(st_out.live_max, live);
             e = components(s, c, live, c->live_list, c->pi, c->pj, c->items);
             if (e != cudaSuccess) return cuda_fail(e, what);
-            if (live) k_sweep<<<grid(n), 256, 0, st>>>(sa);
+            if (live) {
+                k_sweep<<<grid(n), 256, 0, st>>>(sa);
+                c->launches += 1;
+            }
             k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
+            c->launches += 1;
             r = read_scalars(s, c, what);
             if (r != VX_OK) return r;
             unsigned long long bits = (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
@@ -1254,8 +1321,11 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
             std::memcpy(&moved, &bits, sizeof moved);
             changed = c->h_scal[S_CHANGED] != 0;
             if (all_live || moved <= bound) {
-                if (live) k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
-                                                              c->first_impact);
+                if (live) {
+                    k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
+                                                        c->first_impact);
+                    c->launches += 1;
+                }
                 break;
             }
             // a REV moved farther than the bound: replay from the sweep's start
@@ -1271,16 +1341,19 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     // contacts in pair order
     if (pairs) {
         k_contact_flags<<<grid(pairs), 256, 0, st>>>(pairs, c->first_code, c->live);
+        c->launches += 1;
         e = scan(c, st, c->live, c->live_off, pairs);
         if (e != cudaSuccess) return cuda_fail(e, what);
         k_contact_write<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->pi, c->pj, c->first_code,
                                                      c->first_impact, c->ci, c->cj, c->cn, c->cm);
+        c->launches += 1;
         e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_fail(e, what);
         c->contacts = c->h_scal[18];
     }
     st_out.contacts = c->contacts;
+    st_out.launches = c->launches;
     if (out) *out = st_out;
     return VX_OK;
 }
@@ -1321,8 +1394,10 @@ int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restituti
         ra.friction = friction;
         ra.heat = c->heat;
         k_resolve<<<grid(n), 256, 0, st>>>(ra);
+        c->launches += 1;
         k_sum<<<1, 256, 0, st>>>(n, c->heat, c->heat_sum);
         k_sum<<<1, 256, 0, st>>>(n, c->heat + n, c->heat_sum + 1);
+        c->launches += 2;
         double h[2] = {0.0, 0.0};
         e = cudaMemcpyAsync(h, c->heat_sum, 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

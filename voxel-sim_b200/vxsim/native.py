@@ -108,7 +108,7 @@ class VxStepStats(C.Structure):
 
 class VxContactStats(C.Structure):
     _fields_ = [("candidates", C.c_uint64), ("pairs", C.c_uint64), ("contacts", C.c_uint32), ("sweeps", C.c_uint32),
-                ("live_max", C.c_uint32), ("redone", C.c_uint32)]
+                ("live_max", C.c_uint32), ("redone", C.c_uint32), ("launches", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
