@@ -627,7 +627,8 @@ def contact_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"contact: iron block {edge}^3 on its kinematic layer after one substep",
                        "revs": scene.n, "candidates": stats["candidates"], "pairs": stats["pairs"],
-                       "contacts": stats["contacts"], "sweeps": stats["sweeps"], "live_max": stats["live_max"],
+                       "stored_pairs": stats["stored"], "contacts": stats["contacts"], "sweeps": stats["sweeps"],
+                       "live_max": stats["live_max"],
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
             "e2e": {"value": stats["candidates"] / (e2e_ms / 1000.0) * world, "unit": "candidate pairs/s",
                     "h2d_bytes_per_step": 2 * 24 * scene.n, "d2h_bytes_per_step": 24 * scene.n + 13 * len(c),

@@ -338,8 +338,9 @@ typedef struct vx_contact_stats {
     uint32_t contacts;
     uint32_t sweeps;
     uint32_t live_max;    /* most pairs replayed in one sweep */
-    uint32_t redone;      /* sweeps replayed with a wider movement bound */
+    uint32_t redone;      /* sweeps replayed because a REV moved farther than the bound */
     uint32_t launches;    /* kernels launched by the call */
+    uint64_t stored;      /* pairs kept for the sweeps: those that can act within them */
 } vx_contact_stats;
 typedef struct vx_contact_heat {
     double restitution;  /* J, kinetic loss of the normal impulses */
@@ -479,6 +480,16 @@ int32_t vx_pool_bond_stress(vx_pool* pool, uint32_t slot, float* ratio, float* f
  * result is the same whichever other slots share the call. out[max_slots].
  */
 int32_t vx_pool_step(vx_pool* pool, const uint8_t* enabled, const vx_step_params* params, vx_step_stats* out);
+/* Previous positions of a slot (the swept starts of the contact stage). */
+int32_t vx_pool_set_previous(vx_pool* pool, uint32_t slot, const double* xyz);
+int32_t vx_pool_get_previous(vx_pool* pool, uint32_t slot, double* xyz);
+/* The contact projection of every selected slot, each on its own (pairs never
+   join two slots); slot_contacts[max_slots] (or NULL) receives the contacts
+   per slot. With contact = 1, vx_pool_step runs the contact stage for every
+   slot as vx_scene_step does; its per-slot contact heat is the pool-wide total,
+   like its broken-bond count. Pool keys hold at most 1024 slots. */
+int32_t vx_pool_contact_project(vx_pool* pool, const uint8_t* enabled, vx_contact_stats* out,
+                                uint32_t* slot_contacts);
 int32_t vx_pool_checkpoint(vx_pool* pool, int32_t op);
 
 /*

@@ -235,11 +235,67 @@ def test_step_keeps_unbonded_revs_apart(ctx):
     d.close()
 
 
-def test_pools_reject_the_contact_stage(ctx):
-    s, _ = _block(3, 3, 3)
-    pool = N.DevicePool(ctx, 4096, 2)
-    pool.add(s)
-    p = N.step_params(1e-3, contact=True)
-    with pytest.raises(N.VxError):
-        pool.step(p)
+def test_pool_projects_every_slot_on_its_own(ctx):
+    """Three rubble scenes at overlapping coordinates in one pool: each selected
+    slot's projection is the oracle's projection of that scene alone (pairs
+    never join two slots, the tile padding takes no part), and the slot left
+    out of the call is untouched."""
+    cases = [_rubble(11), _rubble(12, n_side=5), _rubble(13, jitter=0.2, speed=0.1)]
+    pool = N.DevicePool(ctx, 8192, 4)
+    slots = []
+    for s, pos, prev in cases:
+        k = pool.add(s)
+        pool.set_positions(k, pos)
+        pool.set_previous(k, prev)
+        slots.append(k)
+    st, per = pool.contact_project(enabled=slots[:2])
+    pairs = 0
+    for (s, pos, prev), k in zip(cases[:2], slots[:2]):
+        op, oq, oc, ost = O.contact_project(pos, prev, s.position, s.kinematic, s.mass.astype(np.float64),
+                                            s.neighbor)
+        assert np.array_equal(pool.positions(k), op)
+        assert np.array_equal(pool.previous(k), oq)
+        assert per[k] == len(oc) > 0
+        pairs += ost["pairs"]
+    assert st["pairs"] == pairs and st["contacts"] == per[slots[0]] + per[slots[1]]
+    s, pos, prev = cases[2]
+    assert np.array_equal(pool.positions(slots[2]), pos) and np.array_equal(pool.previous(slots[2]), prev)
+    assert per[slots[2]] == 0
+    pool.close()
+
+
+def test_pool_step_with_contact_matches_single_scene_steps(ctx):
+    """vx_pool_step with the contact stage against vx_scene_step on each scene:
+    two blocks resting on their floors and a free pair flying apart, three
+    steps; both solve every pass to 1e-10, so positions agree to the solve
+    error and the contact counts are equal."""
+    sc = [_block()[0], _block(5, 4, 6)[0], S.scene_new((2, 1, 1))]
+    sc[2].neighbor[0, 0] = S.EMPTY
+    g = (0.0, 0.0, float(np.float32(-9.81)))
+    p = N.step_params(1e-3, substeps=2, corotation_iterations=2, corotation_tolerance=0.0, gravity=g,
+                      tolerance=1e-10, max_iterations=20000, precision=N.PRECISION_MIXED, fracture=True,
+                      contact=True)
+    pool = N.DevicePool(ctx, 16384, 4)
+    slots = [pool.add(s) for s in sc]
+    pool.set_velocities(slots[2], np.array([[20.0, 0, 0], [-20.0, 0, 0]]))
+    counts = np.zeros(len(sc), np.int64)
+    for _ in range(3):
+        status, stats = pool.step(p)
+        assert status == N.VX_OK
+        counts += [stats[k]["contacts"] for k in slots]
+    for idx, (s, k) in enumerate(zip(sc, slots)):
+        d = N.DeviceScene(ctx, s)
+        if idx == 2:
+            d.set_velocities(np.array([[20.0, 0, 0], [-20.0, 0, 0]]))
+        c = 0
+        for _ in range(3):
+            st = d.step(p)
+            assert st["status"] == N.VX_OK
+            c += st["contacts"]
+        assert c == counts[idx] > 0
+        x0 = s.position
+        assert np.linalg.norm(pool.positions(k) - d.positions()) <= 1e-6 * max(np.linalg.norm(d.positions() - x0), 1e-9)
+        d.close()
+    x = pool.positions(slots[2])
+    assert x[1, 0] - x[0, 0] >= CELL - 1e-5
     pool.close()

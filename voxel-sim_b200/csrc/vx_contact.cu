@@ -53,12 +53,15 @@ constexpr double k1em12 = 9.999999960041972e-13;
 constexpr double k1em3 = 0.0010000000474974513;
 
 constexpr int kSmallExtent = 4;          // bins per axis of a box found through its corner
-constexpr int32_t kCoordLimit = 1 << 20;  // |bin coordinate| bound of the 21-bit key fields
+constexpr int kSceneBits = 21;  // bin coordinate bits of a single scene's keys
+constexpr int kPoolBits = 18;   // ... and of a pool's, whose keys carry the slot
+constexpr uint32_t kPoolKeySlots = 1u << (64 - 3 * kPoolBits);
 constexpr unsigned kProbeLimit = 1u << 20;
 constexpr unsigned kUnionRetries = 1u << 16;
 constexpr uint64_t kMaxLargeVolume = 1ull << 24;  // bins one fast REV may sweep in a substep
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kScanBlock = 1024;
+constexpr double kSweepBound = 5e-4;  // metres a REV may move in one sweep before the call is replayed
 
 enum : uint32_t {
     E_OK = 0,
@@ -69,11 +72,33 @@ enum : uint32_t {
 };
 
 // scalars in ContactState::scal
-enum { S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_COUNT = 8 };
+enum { S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_PAIRS_LO = 8, S_PAIRS_HI = 9 };
 
-__device__ __forceinline__ unsigned long long bin_key(int32_t x, int32_t y, int32_t z) {
-    return ((unsigned long long)(uint32_t)(x + kCoordLimit) << 42) |
-           ((unsigned long long)(uint32_t)(y + kCoordLimit) << 21) | (unsigned long long)(uint32_t)(z + kCoordLimit);
+// Which scene a REV belongs to. A single scene is slot 0 for every REV. In a
+// pool, REVs of free tiles, of slots not taking part in the call, and the
+// padding after a slot's last REV have no slot (VX_EMPTY_U32).
+struct RevFilter {
+    const uint8_t* tile_on;      // per 256-REV tile, null = all on
+    const uint32_t* tile_scene;  // per tile: slot, null for a single scene
+    const uint32_t* slot_first;  // per slot: first tile
+    const uint32_t* slot_revs;   // per slot: REV count
+};
+__device__ __forceinline__ uint32_t rev_slot(const RevFilter& f, uint32_t i) {
+    if (!f.tile_scene) return 0;
+    const uint32_t tile = i >> 8;
+    if (f.tile_on && !f.tile_on[tile]) return VX_EMPTY_U32;
+    const uint32_t slot = f.tile_scene[tile];
+    if (slot == VX_EMPTY_U32) return VX_EMPTY_U32;
+    return i - f.slot_first[slot] * 256u < f.slot_revs[slot] ? slot : VX_EMPTY_U32;
+}
+
+// Hash key of a bin of one scene: the slot above three biased bin
+// coordinates of `bits` bits each (21 for a single scene, 18 in a pool, which
+// leaves 10 bits for up to 1024 slots).
+__device__ __forceinline__ unsigned long long bin_key(uint32_t slot, int32_t x, int32_t y, int32_t z, int bits) {
+    const int32_t bias = 1 << (bits - 1);
+    return ((unsigned long long)slot << (3 * bits)) | ((unsigned long long)(uint32_t)(x + bias) << (2 * bits)) |
+           ((unsigned long long)(uint32_t)(y + bias) << bits) | (unsigned long long)(uint32_t)(z + bias);
 }
 __device__ __forceinline__ uint32_t key_hash(unsigned long long k) {
     k ^= k >> 31;
@@ -187,6 +212,36 @@ __device__ __forceinline__ double inverse_mass(const uint8_t* kin, const float4*
     return 1.0 / (double)param1[i].w;
 }
 
+// True when the pair can act or report a contact while each REV moves at
+// most M: its end separation within half = CELL + slop + 2M (+ a rounding
+// margin) on every axis, or, unless the starts already overlap (swept_normal
+// then answers nothing), its relative path from the start separation to the
+// end one meeting the box of that half-width.
+__device__ bool may_act(v3 si, v3 sj, v3 ei, v3 ej, double half) {
+    const double d0[3] = {sj.x - si.x, sj.y - si.y, sj.z - si.z};
+    const double e[3] = {ej.x - ei.x, ej.y - ei.y, ej.z - ei.z};
+    bool near_end = true, starts_inside = true;
+    for (int t = 0; t < 3; ++t) {
+        if (!(fabs(e[t]) <= half)) near_end = false;
+        if (!(fabs(d0[t]) <= kStartTouch)) starts_inside = false;
+    }
+    if (near_end) return true;
+    if (starts_inside) return false;
+    double t0 = 0.0, t1 = 1.0;
+    for (int t = 0; t < 3; ++t) {
+        const double r = e[t] - d0[t];
+        if (r == 0.0) {
+            if (!(fabs(d0[t]) <= half)) return false;
+            continue;
+        }
+        const double a = (-half - d0[t]) / r, b = (half - d0[t]) / r;
+        t0 = fmax(t0, fmin(a, b));
+        t1 = fmin(t1, fmax(a, b));
+        if (!(t0 <= t1)) return false;
+    }
+    return true;
+}
+
 // ---- local continuum test -------------------------------------------------
 
 // adjacency (:491-503): +a neighbour from the bond table, -a from its reverse
@@ -232,21 +287,32 @@ __device__ bool local_continuum(const float* rest, const uint32_t* nbr, const ui
 // ---- broadphase -------------------------------------------------------------
 
 struct Boxes {
-    int32_t* lo;   // [3][n]
-    int32_t* hi;   // [3][n]
-    uint8_t* large;
+    int32_t* lo;     // [3][n]
+    int32_t* hi;     // [3][n]
+    uint8_t* large;  // 0 small box, 1 large box, 2 not taking part
+    uint32_t* slot;  // [n] the REV's scene (rev_slot)
+    int bits;        // key coordinate bits
 };
 
 __global__ void k_boxes(uint32_t n, const double* __restrict__ pos, const double* __restrict__ start, Boxes b,
-                        uint32_t* __restrict__ scal) {
+                        RevFilter f, uint32_t* __restrict__ scal) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const uint32_t slot = rev_slot(f, i);
+    b.slot[i] = slot;
+    if (slot == VX_EMPTY_U32) {
+        b.large[i] = 2;
+        for (int t = 0; t < 3; ++t) b.lo[(size_t)t * n + i] = b.hi[(size_t)t * n + i] = 0;
+        return;
+    }
+    // |bin| stays 8 below the key range, so corner probes (reach 3) stay inside it
+    const double limit = (double)((1 << (b.bits - 1)) - 8);
     bool large = false, bad = false;
     int32_t ext[3];
     for (int t = 0; t < 3; ++t) {
         const double s = start[(size_t)t * n + i], p = pos[(size_t)t * n + i];
         const double a = fmin(s, p) / kCell - kBinHalf, c = fmax(s, p) / kCell + kBinHalf;
-        if (!(fabs(a) < (double)(kCoordLimit - 1)) || !(fabs(c) < (double)(kCoordLimit - 1))) {
+        if (!(fabs(a) < limit) || !(fabs(c) < limit)) {
             bad = true;
             b.lo[(size_t)t * n + i] = 0;
             b.hi[(size_t)t * n + i] = 0;
@@ -273,7 +339,7 @@ __global__ void k_insert_corners(uint32_t n, Boxes b, unsigned long long* keys, 
                                  uint32_t mask, uint32_t* scal) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || b.large[i]) return;
-    const unsigned long long key = bin_key(b.lo[i], b.lo[(size_t)n + i], b.lo[2 * (size_t)n + i]);
+    const unsigned long long key = bin_key(b.slot[i], b.lo[i], b.lo[(size_t)n + i], b.lo[2 * (size_t)n + i], b.bits);
     const uint32_t slot = table_claim(keys, mask, key);
     if (slot == VX_EMPTY_U32) {
         atomicOr(scal + S_ERR, E_TABLE);
@@ -287,7 +353,7 @@ __global__ void k_large_volume(uint32_t n, Boxes b, uint32_t* vol, uint32_t* sca
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint64_t v = 0;
-    if (b.large[i]) {
+    if (b.large[i] == 1) {
         v = 1;
         for (int t = 0; t < 3; ++t)
             v *= (uint64_t)(b.hi[(size_t)t * n + i] - b.lo[(size_t)t * n + i] + 1);
@@ -303,7 +369,7 @@ __global__ void k_large_volume(uint32_t n, Boxes b, uint32_t* vol, uint32_t* sca
 __global__ void k_insert_large(uint32_t n, Boxes b, const uint32_t* __restrict__ off, unsigned long long* keys,
                                uint32_t* heads, uint32_t* ent_id, uint32_t* ent_next, uint32_t mask, uint32_t* scal) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !b.large[i]) return;
+    if (i >= n || b.large[i] != 1) return;
     uint32_t e = off[i];
     const uint32_t end = off[i + 1];
     const int32_t x0 = b.lo[i], y0 = b.lo[(size_t)n + i], z0 = b.lo[2 * (size_t)n + i];
@@ -311,7 +377,7 @@ __global__ void k_insert_large(uint32_t n, Boxes b, const uint32_t* __restrict__
     for (int32_t z = z0; z <= z1; ++z)
         for (int32_t y = y0; y <= y1; ++y)
             for (int32_t x = x0; x <= x1 && e < end; ++x, ++e) {
-                const uint32_t slot = table_claim(keys, mask, bin_key(x, y, z));
+                const uint32_t slot = table_claim(keys, mask, bin_key(b.slot[i], x, y, z, b.bits));
                 ent_id[e] = i;
                 if (slot == VX_EMPTY_U32) {
                     atomicOr(scal + S_ERR, E_TABLE);
@@ -339,6 +405,9 @@ struct PairArgs {
     const uint32_t* ent_next;
     uint32_t mask2;
     int32_t wx, wy, wz;  // largest small extent per axis
+    const double* pos;   // current positions
+    const double* start; // swept starts
+    double half;         // pairs that cannot act within this reach are not stored
     uint32_t* count;     // per owner: pairs (count pass) / cursor (write pass)
     const uint32_t* off;
     uint32_t* pi;
@@ -347,11 +416,15 @@ struct PairArgs {
 };
 
 template <bool kWrite>
-__device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand) {
+__device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand, uint32_t& kept) {
     const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
     if (a.kin[lo] && a.kin[hi]) return;
     ++cand;
     if (local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
+    ++kept;
+    if (!may_act(load3(a.start, a.n, lo), load3(a.start, a.n, hi), load3(a.pos, a.n, lo), load3(a.pos, a.n, hi),
+                 a.half))
+        return;
     if (kWrite) {
         const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
         a.pi[slot] = lo;
@@ -373,9 +446,12 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const uint32_t n = a.n;
+    if (a.b.large[i] == 2) return;
+    const uint32_t slot = a.b.slot[i];
+    const int bits = a.b.bits;
     int32_t lo[3], hi[3];
     box_of(a.b, n, i, lo, hi);
-    uint32_t cand = 0;
+    uint32_t cand = 0, kept = 0;
     const bool large_i = a.b.large[i] != 0;
     if (!large_i) {
         // small-small: corners within reach of this box; the smaller REV finds the pair
@@ -383,15 +459,15 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
         for (int32_t z = lo[2] - (w[2] - 1); z <= hi[2]; ++z)
             for (int32_t y = lo[1] - (w[1] - 1); y <= hi[1]; ++y)
                 for (int32_t x = lo[0] - (w[0] - 1); x <= hi[0]; ++x) {
-                    const uint32_t slot = table_find(a.keys1, a.mask1, bin_key(x, y, z));
-                    if (slot == VX_EMPTY_U32) continue;
-                    for (uint32_t j = a.heads1[slot]; j != VX_EMPTY_U32; j = a.next1[j]) {
+                    const uint32_t hs = table_find(a.keys1, a.mask1, bin_key(slot, x, y, z, bits));
+                    if (hs == VX_EMPTY_U32) continue;
+                    for (uint32_t j = a.heads1[hs]; j != VX_EMPTY_U32; j = a.next1[j]) {
                         if (j <= i) continue;
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
                         if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] && lj[2] <= hi[2] &&
                             lo[2] <= hj[2])
-                            emit<kWrite>(a, i, j, cand);
+                            emit<kWrite>(a, i, j, cand, kept);
                     }
                 }
     }
@@ -401,22 +477,21 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
         for (int32_t z = lo[2]; z <= hi[2]; ++z)
             for (int32_t y = lo[1]; y <= hi[1]; ++y)
                 for (int32_t x = lo[0]; x <= hi[0]; ++x) {
-                    const uint32_t slot = table_find(a.keys2, a.mask2, bin_key(x, y, z));
-                    if (slot == VX_EMPTY_U32) continue;
-                    for (uint32_t e = a.heads2[slot]; e != VX_EMPTY_U32; e = a.ent_next[e]) {
+                    const uint32_t hs = table_find(a.keys2, a.mask2, bin_key(slot, x, y, z, bits));
+                    if (hs == VX_EMPTY_U32) continue;
+                    for (uint32_t e = a.heads2[hs]; e != VX_EMPTY_U32; e = a.ent_next[e]) {
                         const uint32_t j = a.ent_id[e];
                         if (j == i || (large_i && j < i)) continue;
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
                         if (x == max(lo[0], lj[0]) && y == max(lo[1], lj[1]) && z == max(lo[2], lj[2]))
-                            emit<kWrite>(a, i, j, cand);
+                            emit<kWrite>(a, i, j, cand, kept);
                     }
                 }
     }
     if (!kWrite && cand) {
-        const unsigned long long prev =
-            atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
-        (void)prev;
+        atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
+        if (kept) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), (unsigned long long)kept);
     }
 }
 
@@ -449,31 +524,7 @@ __global__ void k_classify(uint32_t count, const uint32_t* __restrict__ pi, cons
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     const uint32_t i = pi[k], j = pj[k];
-    const v3 si = load3(start, n, i), sj = load3(start, n, j), ei = load3(pos, n, i), ej = load3(pos, n, j);
-    const double d0[3] = {sj.x - si.x, sj.y - si.y, sj.z - si.z};
-    const double e[3] = {ej.x - ei.x, ej.y - ei.y, ej.z - ei.z};
-    bool near_end = true, starts_inside = true;
-    for (int t = 0; t < 3; ++t) {
-        if (!(fabs(e[t]) <= half)) near_end = false;
-        if (!(fabs(d0[t]) <= kStartTouch)) starts_inside = false;
-    }
-    bool hit = near_end;
-    if (!hit && !starts_inside) {
-        double t0 = 0.0, t1 = 1.0;
-        hit = true;
-        for (int t = 0; t < 3 && hit; ++t) {
-            const double r = e[t] - d0[t];
-            if (r == 0.0) {
-                hit = fabs(d0[t]) <= half;
-                continue;
-            }
-            const double a = (-half - d0[t]) / r, b = (half - d0[t]) / r;
-            t0 = fmax(t0, fmin(a, b));
-            t1 = fmin(t1, fmax(a, b));
-            hit = t0 <= t1;
-        }
-    }
-    live[k] = hit ? 1 : 0;
+    live[k] = may_act(load3(start, n, i), load3(start, n, j), load3(pos, n, i), load3(pos, n, j), half) ? 1 : 0;
 }
 
 __global__ void k_compact(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
@@ -698,7 +749,8 @@ __global__ void k_contact_flags(uint32_t count, const int8_t* __restrict__ code,
 __global__ void k_contact_write(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
                                 const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj,
                                 const int8_t* __restrict__ code, const uint8_t* __restrict__ impact, uint32_t* ci,
-                                uint32_t* cj, int8_t* cn, uint8_t* cm) {
+                                uint32_t* cj, int8_t* cn, uint8_t* cm, const uint32_t* __restrict__ rslot,
+                                uint32_t* slot_contacts) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count || !flag[k]) return;
     const uint32_t o = off[k];
@@ -706,6 +758,7 @@ __global__ void k_contact_write(uint32_t count, const uint8_t* __restrict__ flag
     cj[o] = pj[k];
     cn[o] = code[k];
     cm[o] = impact[k];
+    if (slot_contacts) atomicAdd(slot_contacts + rslot[pi[k]], 1u);
 }
 
 // ---- contact velocities -------------------------------------------------
@@ -921,6 +974,7 @@ struct ContactState {
     // per REV
     Boxes box{};
     double* start = nullptr;    // [3][n] previous positions when the call began
+    double* entry = nullptr;    // [3][n] positions when the call began
     double* snap = nullptr;     // [6][n] positions and previous at the start of a sweep
     double* move = nullptr;     // [n]
     double* heat = nullptr;     // [2][n]
@@ -959,6 +1013,7 @@ struct ContactState {
     uint8_t* cm = nullptr;
     uint32_t contacts = 0;
     uint32_t launches = 0;  // kernels launched by the current call
+    uint32_t* slot_contacts = nullptr;  // [pool slots] contacts per slot of the last projection
     // scalars: [0] error bits, [1..3] small extents, [4] large count, [5] changed,
     // [6..7] candidate count (u64); max movement (u64 bits of a double); the
     // host copies
@@ -1026,7 +1081,10 @@ cudaError_t ensure_state(vx_scene* s) {
     cudaError_t e = alloc(c->box.lo, 3 * n);
     if (e == cudaSuccess) e = alloc(c->box.hi, 3 * n);
     if (e == cudaSuccess) e = alloc(c->box.large, n);
+    if (e == cudaSuccess) e = alloc(c->box.slot, n);
+    if (e == cudaSuccess && s->pool_slots) e = alloc(c->slot_contacts, s->pool_slots);
     if (e == cudaSuccess) e = alloc(c->start, 3 * n);
+    if (e == cudaSuccess) e = alloc(c->entry, 3 * n);
     if (e == cudaSuccess) e = alloc(c->snap, 6 * n);
     if (e == cudaSuccess) e = alloc(c->move, n);
     if (e == cudaSuccess) e = alloc(c->heat, 2 * n);
@@ -1103,7 +1161,8 @@ int32_t read_scalars(vx_scene* s, ContactState* c, const char* what) {
     }
     const uint32_t err = c->h_scal[S_ERR];
     if (err & E_RANGE) {
-        set_error("%s: a position is non-finite or farther than %d cells from the origin", what, kCoordLimit - 2);
+        set_error("%s: a position is non-finite or too far from the origin for the bin keys (2^%d cells in a "
+                  "scene, 2^%d in a pool)", what, kSceneBits - 1, kPoolBits - 1);
         return VX_NONFINITE;
     }
     if (err & E_VOLUME) {
@@ -1147,7 +1206,7 @@ void contact_release(vx_scene* s) {
     if (!c) return;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->start, c->snap, c->move, c->heat, c->phys, c->next1,
+    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->box.slot, c->slot_contacts, c->start, c->entry, c->snap, c->move, c->heat, c->phys, c->next1,
                     c->cnt, c->off, c->parent, c->comp_cnt, c->comp_off, c->bsum, c->keys1, c->heads1, c->keys2,
                     c->heads2, c->ent_id, c->ent_next, c->pi, c->pj, c->live, c->live_off, c->live_list, c->root,
                     c->items, c->code, c->impact, c->first_code, c->first_impact, c->ci, c->cj, c->cn, c->cm,
@@ -1160,8 +1219,10 @@ void contact_release(vx_scene* s) {
 }
 
 // collision::project over the scene's positions, with its previous positions
-// as the swept starts; targeted axes have zero inverse mass.
-int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
+// as the swept starts; targeted axes have zero inverse mass. In a pool, every
+// slot taking part in the call (the tile mask) is projected on its own, and
+// slot_contacts (host, [pool slots], or null) receives the contacts per slot.
+int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_contacts) {
     const char* what = "vx_contact_project";
     vx_contact_stats st_out{};
     cudaError_t e = ensure_state(s);
@@ -1174,17 +1235,26 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     cudaStream_t st = s->stream;
     c->contacts = 0;
     c->launches = 0;
+    const bool pooled = s->pool_slots > 0;
+    if (pooled && s->pool_slots > kPoolKeySlots) {
+        set_error("%s: contact keys hold %u pool slots, the pool has %u", what, kPoolKeySlots, s->pool_slots);
+        return VX_BAD_INPUT;
+    }
+    if (slot_contacts && pooled) std::fill(slot_contacts, slot_contacts + s->pool_slots, 0u);
     if (n < 2) {
         if (out) *out = st_out;
         return VX_OK;
     }
+    RevFilter filter{};
+    if (pooled) filter = RevFilter{s->tile_on, s->tile_scene, s->pool_slot_first, s->pool_slot_revs};
+    c->box.bits = pooled ? kPoolBits : kSceneBits;
     const size_t v3b = 3 * (size_t)n * sizeof(double);
     e = cudaMemcpyAsync(c->start, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->keys1, 0xFF, (size_t)c->table1 * sizeof(unsigned long long), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->heads1, 0xFF, (size_t)c->table1 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return cuda_fail(e, what);
-    k_boxes<<<grid(n), 256, 0, st>>>(n, s->pos, c->start, c->box, c->scal);
+    k_boxes<<<grid(n), 256, 0, st>>>(n, s->pos, c->start, c->box, filter, c->scal);
     c->launches += 1;
     k_insert_corners<<<grid(n), 256, 0, st>>>(n, c->box, c->keys1, c->heads1, c->next1, c->table1 - 1, c->scal);
     c->launches += 1;
@@ -1235,117 +1305,159 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out) {
     pa.count = c->cnt;
     pa.off = c->off;
     pa.scal = c->scal;
-    e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+    pa.pos = s->pos;
+    pa.start = c->start;
+    // The projection first stores only the pairs that can act within six sweeps
+    // when no REV moves more than kSweepBound per sweep (the lattice's
+    // two-cell neighbours never can). When a sweep moves a REV farther, the
+    // call starts again from its entry state storing every pair, and then widens
+    // the bound sweep by sweep. Both ways replay the reference's sweeps exactly.
+    e = cudaMemcpyAsync(c->entry, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return cuda_fail(e, what);
-    k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
-    c->launches += 1;
-    e = scan(c, st, c->cnt, c->off, n);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_fail(e, what);
-    r = read_scalars(s, c, what);
-    if (r != VX_OK) return r;
-    const uint32_t pairs = c->h_scal[18];
-    st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
-    st_out.pairs = pairs;
-    e = ensure_pairs(c, pairs);
-    if (e != cudaSuccess) {
-        set_error("%s: %u pairs: %s", what, pairs, cudaGetErrorString(e));
-        return VX_OOM;
-    }
-    pa.pi = c->pi;
-    pa.pj = c->pj;
-    e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
-    if (e == cudaSuccess && pairs) e = cudaMemsetAsync(c->first_code, 0, pairs, st);
-    if (e != cudaSuccess) return cuda_fail(e, what);
-    if (pairs) {
-        k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
-        k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
-        c->launches += 2;
-    }
-    // the sweeps (project :51-103)
-    SweepArgs sa{};
-    sa.n = n;
-    sa.comp_off = c->comp_off;
-    sa.items = c->items;
-    sa.pi = c->pi;
-    sa.pj = c->pj;
-    sa.pos = s->pos;
-    sa.prev = s->prev;
-    sa.start = c->start;
-    sa.kin = s->kin;
-    sa.param1 = s->param1;
-    sa.tmask = s->tmask;
-    sa.move = c->move;
-    sa.code = c->code;
-    sa.impact = c->impact;
-    sa.scal = c->scal;
-    const double base_bound = 1e-3;  // M: metres a REV may move in one sweep
-    if (!pairs) st_out.sweeps = 1;   // the reference's first sweep runs over an empty list
-    for (int sweep = 0; sweep < 6 && pairs; ++sweep) {
-        st_out.sweeps += 1;
-        e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
+    uint32_t stored = 0;
+    bool full = false;
+    for (;;) {  // at most twice: bounded storage, then every pair
+        pa.half = full ? 1e300 : kCell + kSlop + 2.0 * 6.0 * kSweepBound + 1e-9;
+        pa.pi = nullptr;
+        pa.pj = nullptr;
+        e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
         if (e != cudaSuccess) return cuda_fail(e, what);
-        double bound = base_bound;
-        bool changed = false;
-        for (int attempt = 0;; ++attempt) {
-            const bool all_live = attempt >= 4;
-            const double half = all_live ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9;
-            e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
+        k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
+        c->launches += 1;
+        e = scan(c, st, c->cnt, c->off, n);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        r = read_scalars(s, c, what);
+        if (r != VX_OK) return r;
+        stored = c->h_scal[18];
+        st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
+        st_out.pairs = (uint64_t)c->h_scal[S_PAIRS_LO] | ((uint64_t)c->h_scal[S_PAIRS_HI] << 32);
+        st_out.stored = stored;
+        e = ensure_pairs(c, stored);
+        if (e != cudaSuccess) {
+            set_error("%s: %u stored pairs: %s", what, stored, cudaGetErrorString(e));
+            return VX_OOM;
+        }
+        pa.pi = c->pi;
+        pa.pj = c->pj;
+        e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+        if (e == cudaSuccess && stored) e = cudaMemsetAsync(c->first_code, 0, stored, st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        if (stored) {
+            k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
+            k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
+            c->launches += 2;
+        }
+        // the sweeps (project :51-103)
+        SweepArgs sa{};
+        sa.n = n;
+        sa.comp_off = c->comp_off;
+        sa.items = c->items;
+        sa.pi = c->pi;
+        sa.pj = c->pj;
+        sa.pos = s->pos;
+        sa.prev = s->prev;
+        sa.start = c->start;
+        sa.kin = s->kin;
+        sa.param1 = s->param1;
+        sa.tmask = s->tmask;
+        sa.move = c->move;
+        sa.code = c->code;
+        sa.impact = c->impact;
+        sa.scal = c->scal;
+        st_out.sweeps = stored ? 0 : 1;  // the reference's first sweep runs over an empty list
+        bool restart = false;
+        for (int sweep = 0; sweep < 6 && stored && !restart; ++sweep) {
+            st_out.sweeps += 1;
+            e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) return cuda_fail(e, what);
-            k_classify<<<grid(pairs), 256, 0, st>>>(pairs, c->pi, c->pj, n, s->pos, c->start, half, c->live);
-            c->launches += 1;
-            e = scan(c, st, c->live, c->live_off, pairs);
-            if (e != cudaSuccess) return cuda_fail(e, what);
-            k_compact<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->live_list);
-            c->launches += 1;
-            e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) return cuda_fail(e, what);
-            const uint32_t live = c->h_scal[18];
-            st_out.live_max = std::max(st_out.live_max, live);
-            e = components(s, c, live, c->live_list, c->pi, c->pj, c->items);
-            if (e != cudaSuccess) return cuda_fail(e, what);
-            if (live) {
-                k_sweep<<<grid(n), 256, 0, st>>>(sa);
+            double bound = kSweepBound;
+            bool changed = false;
+            for (int attempt = 0;; ++attempt) {
+                const bool all_live = full && attempt >= 4;
+                const double half = all_live ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9;
+                e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
+                if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
+                if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                k_classify<<<grid(stored), 256, 0, st>>>(stored, c->pi, c->pj, n, s->pos, c->start, half, c->live);
                 c->launches += 1;
-            }
-            k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
-            c->launches += 1;
-            r = read_scalars(s, c, what);
-            if (r != VX_OK) return r;
-            unsigned long long bits = (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
-            double moved = 0.0;
-            std::memcpy(&moved, &bits, sizeof moved);
-            changed = c->h_scal[S_CHANGED] != 0;
-            if (all_live || moved <= bound) {
+                e = scan(c, st, c->live, c->live_off, stored);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                k_compact<<<grid(stored), 256, 0, st>>>(stored, c->live, c->live_off, c->live_list);
+                c->launches += 1;
+                e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + stored, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                    st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                const uint32_t live = c->h_scal[18];
+                st_out.live_max = std::max(st_out.live_max, live);
+                e = components(s, c, live, c->live_list, c->pi, c->pj, c->items);
+                if (e != cudaSuccess) return cuda_fail(e, what);
                 if (live) {
-                    k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
-                                                        c->first_impact);
+                    k_sweep<<<grid(n), 256, 0, st>>>(sa);
                     c->launches += 1;
                 }
-                break;
+                k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
+                c->launches += 1;
+                r = read_scalars(s, c, what);
+                if (r != VX_OK) return r;
+                unsigned long long bits =
+                    (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
+                double moved = 0.0;
+                std::memcpy(&moved, &bits, sizeof moved);
+                changed = c->h_scal[S_CHANGED] != 0;
+                if (all_live || moved <= bound) {
+                    if (live) {
+                        k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
+                                                            c->first_impact);
+                        c->launches += 1;
+                    }
+                    break;
+                }
+                st_out.redone += 1;
+                if (!full) {  // start the call again from its entry state, storing every pair
+                    e = cudaMemcpyAsync(s->pos, c->entry, v3b, cudaMemcpyDeviceToDevice, st);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(s->prev, c->start, v3b, cudaMemcpyDeviceToDevice, st);
+                    if (e != cudaSuccess) return cuda_fail(e, what);
+                    restart = true;
+                    break;
+                }
+                // a REV moved farther than the bound: replay from the sweep's start
+                e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                bound = std::max(2.0 * moved, 4.0 * bound);
             }
-            // a REV moved farther than the bound: replay from the sweep's start
-            st_out.redone += 1;
-            e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
-            if (e != cudaSuccess) return cuda_fail(e, what);
-            bound = std::max(2.0 * moved, 4.0 * bound);
+            if (!restart && !changed) break;
         }
-        if (!changed) break;
+        if (!restart) break;
+        full = true;
     }
+    const uint32_t pairs = stored;
     // contacts in pair order
     if (pairs) {
+        uint32_t* per_slot = pooled && slot_contacts ? c->slot_contacts : nullptr;
+        if (per_slot) {
+            e = cudaMemsetAsync(per_slot, 0, s->pool_slots * sizeof(uint32_t), st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+        }
         k_contact_flags<<<grid(pairs), 256, 0, st>>>(pairs, c->first_code, c->live);
         c->launches += 1;
         e = scan(c, st, c->live, c->live_off, pairs);
         if (e != cudaSuccess) return cuda_fail(e, what);
         k_contact_write<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->pi, c->pj, c->first_code,
-                                                     c->first_impact, c->ci, c->cj, c->cn, c->cm);
+                                                     c->first_impact, c->ci, c->cj, c->cn, c->cm, c->box.slot,
+                                                     per_slot);
+        if (per_slot) {
+            e = cudaMemcpyAsync(slot_contacts, per_slot, s->pool_slots * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+        }
         c->launches += 1;
         e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1424,7 +1536,7 @@ extern "C" int32_t vx_contact_project(vx_scene* s, vx_contact_stats* out) {
         return VX_BAD_INPUT;
     }
     cudaSetDevice(s->device);
-    return contact_project(s, out);
+    return contact_project(s, out, nullptr);
 }
 
 extern "C" int32_t vx_contact_resolve_velocities(vx_scene* s, int32_t pre_contact, double restitution,

@@ -163,6 +163,8 @@ struct vx_scene {
     uint32_t pool_slots = 0;      // slot capacity; 0 = a single scene
     uint8_t* tile_on = nullptr;   // [tiles] 1 = tile of a slot taking part in the current call
     uint32_t* tile_scene = nullptr;  // [tiles] slot of the tile, VX_EMPTY when free
+    uint32_t* pool_slot_first = nullptr;  // [pool_slots] first tile of each slot (device)
+    uint32_t* pool_slot_revs = nullptr;   // [pool_slots] REVs of each slot (device)
     uint32_t launches = 0;        // kernels launched by the current pass
     int sm_count = 148;           // SMs of the scene's GPU
     unsigned grid32 = 0;          // grid of the FP32 / FP64 PCG kernels (0 = not yet chosen)

@@ -57,12 +57,13 @@ cudaError_t launch_scatter3(vx_scene* s, uint32_t count, const uint32_t* d_index
                             double* field);
 // connected components of the bond graph with the reference's cluster numbering (vx_clusters.cu)
 // collision::project and resolve_velocities_with_precontact (vx_contact.cu)
-int32_t contact_project(vx_scene* s, vx_contact_stats* out);
+int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_contacts);
 int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restitution, double friction,
                         vx_contact_heat* out);
 uint32_t contact_count(const vx_scene* s);
 void contact_release(vx_scene* s);
 cudaError_t launch_rest_positions(vx_scene* s);
+cudaError_t launch_rest_range(vx_scene* s, size_t first, size_t count);
 
 cudaError_t launch_rebuild_clusters(vx_scene* s);
 uint32_t cluster_scan_blocks(uint32_t n);

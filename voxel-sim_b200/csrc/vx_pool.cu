@@ -72,6 +72,7 @@ struct vx_pool {
     vx::SlotState* st = nullptr;            // device [slots]
     uint32_t* slot_first = nullptr;
     uint32_t* slot_tiles = nullptr;
+    uint32_t* slot_revs = nullptr;          // device [slots]: REVs of the slot's scene
     int32_t* active = nullptr;
     int32_t* pending = nullptr;
     unsigned long long* angle = nullptr;    // [slots]
@@ -567,7 +568,8 @@ int32_t vx_pool_create(vx_ctx* ctx, uint64_t max_revs, uint32_t max_slots, vx_po
         return o;
     };
     size_t o_on = take(p->tiles), o_ts = take(p->tiles * 4), o_st = take(max_slots * sizeof(SlotState)),
-           o_first = take(max_slots * 4), o_cnt = take(max_slots * 4), o_act = take(16), o_ang = take(max_slots * 8);
+           o_first = take(max_slots * 4), o_cnt = take(max_slots * 4), o_act = take(16), o_ang = take(max_slots * 8),
+           o_revs = take(max_slots * 4);
     cudaError_t e = cudaMalloc(&p->extra, off);
     if (e == cudaSuccess) e = cudaMemsetAsync(p->extra, 0, off, p->s.stream);
     if (e == cudaSuccess) e = cudaMallocHost(&p->h_st, max_slots * sizeof(SlotState));
@@ -582,6 +584,9 @@ int32_t vx_pool_create(vx_ctx* ctx, uint64_t max_revs, uint32_t max_slots, vx_po
     p->st = (SlotState*)(p->extra + o_st);
     p->slot_first = (uint32_t*)(p->extra + o_first);
     p->slot_tiles = (uint32_t*)(p->extra + o_cnt);
+    p->slot_revs = (uint32_t*)(p->extra + o_revs);
+    p->s.pool_slot_first = p->slot_first;
+    p->s.pool_slot_revs = p->slot_revs;
     p->active = (int32_t*)(p->extra + o_act);
     p->pending = p->active + 1;
     p->angle = (unsigned long long*)(p->extra + o_ang);
@@ -752,9 +757,13 @@ int32_t vx_pool_add(vx_pool* p, const vx_scene_desc* d, uint32_t* out_slot) {
                             cudaMemcpyHostToDevice, st);
     std::vector<uint32_t> ts(need, slot);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s->tile_scene + start, ts.data(), need * 4, cudaMemcpyHostToDevice, st);
-    uint32_t fc[2] = {start, need};
+    uint32_t fc[3] = {start, need, (uint32_t)n};
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->slot_first + slot, &fc[0], 4, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(p->slot_tiles + slot, &fc[1], 4, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p->slot_revs + slot, &fc[2], 4, cudaMemcpyHostToDevice, st);
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c)
+        e = cudaMemcpyAsync(s->prev + c * C + base, pos.data() + c * m, m * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_rest_range(s, base, m);
     if (e == cudaSuccess) e = launch_reverse_neighbors(s);
     if (e == cudaSuccess) e = launch_flags(s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -842,6 +851,33 @@ int32_t vx_pool_set_positions(vx_pool* p, uint32_t slot, const double* xyz) {
             return VX_NONFINITE;
         }
     return slot_vec(p, slot, p->s.pos, const_cast<double*>(xyz), true);
+}
+int32_t vx_pool_set_previous(vx_pool* p, uint32_t slot, const double* xyz) {
+    int32_t r = slot_ok(p, slot, xyz, __func__);
+    if (r != VX_OK) return r;
+    for (size_t t = 0; t < 3 * (size_t)p->rev_n[slot]; ++t)
+        if (!std::isfinite(xyz[t])) {
+            set_error("vx_pool_set_previous: non-finite value at %zu", t);
+            return VX_NONFINITE;
+        }
+    return slot_vec(p, slot, p->s.prev, const_cast<double*>(xyz), true);
+}
+int32_t vx_pool_get_previous(vx_pool* p, uint32_t slot, double* xyz) {
+    int32_t r = slot_ok(p, slot, xyz, __func__);
+    if (r != VX_OK) return r;
+    return slot_vec(p, slot, p->s.prev, xyz, false);
+}
+int32_t vx_pool_contact_project(vx_pool* p, const uint8_t* enabled, vx_contact_stats* out, uint32_t* slot_contacts) {
+    clear_error();
+    if (!p) {
+        set_error("vx_pool_contact_project: null pool");
+        return VX_BAD_INPUT;
+    }
+    cudaSetDevice(p->s.device);
+    std::vector<uint8_t> sel;
+    int32_t r = pool_select(p, enabled, sel);
+    if (r != VX_OK) return r;
+    return contact_project(&p->s, out, slot_contacts);
 }
 int32_t vx_pool_get_positions(vx_pool* p, uint32_t slot, double* xyz) {
     int32_t r = slot_ok(p, slot, xyz, __func__);
@@ -1060,8 +1096,9 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
                   prm->fixed_dt, prm->substeps, prm->corotation_iterations);
         return VX_BAD_INPUT;
     }
-    if (prm->contact) {
-        set_error("vx_pool_step: the contact stage runs on single scenes (vx_scene_step) only");
+    if (prm->contact && (!(prm->restitution >= 0.0 && prm->restitution <= 1.0) || !(prm->friction >= 0.0) ||
+                         !std::isfinite(prm->friction))) {
+        set_error("vx_pool_step: invalid restitution=%g or friction=%g", prm->restitution, prm->friction);
         return VX_BAD_INPUT;
     }
     cudaSetDevice(p->s.device);
@@ -1073,6 +1110,7 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
     for (uint32_t k = 0; k < S; ++k) st[k].converged = 1;
     std::vector<vx_pass_stats> ps(S);
     std::vector<double> angle(S, 0.0);
+    std::vector<uint32_t> slot_contacts(S, 0);
     int32_t worst = VX_OK;
     std::vector<uint8_t> sel;
     for (uint32_t sub = 0; sub < prm->substeps; ++sub) {
@@ -1115,6 +1153,16 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
         }
         r = pool_select(p, on.data(), sel);
         if (r != VX_OK) return r;
+        // the order of the single-scene step: velocities from the solved
+        // positions, contact projection, fracture, contact velocities
+        VX_POOL_TRY(launch_velocity(&p->s, h), "pool velocity update");
+        if (prm->contact) {  // every selected slot projected on its own; counts per slot
+            vx_contact_stats cs{};
+            r = contact_project(&p->s, &cs, slot_contacts.data());
+            if (r != VX_OK) return r;
+            for (uint32_t k = 0; k < S; ++k)
+                if (on[k]) st[k].contacts += slot_contacts[k];
+        }
         if (prm->fracture) {  // one stage over every selected slot; totals are pool-wide
             vx_dissipation d{};
             uint32_t broken = 0;
@@ -1123,7 +1171,16 @@ int32_t vx_pool_step(vx_pool* p, const uint8_t* enabled, const vx_step_params* p
             for (uint32_t k = 0; k < S; ++k)
                 if (on[k]) st[k].broken += broken;
         }
-        VX_POOL_TRY(launch_velocity(&p->s, h), "pool velocity update");
+        if (prm->contact) {  // heat totals are pool-wide, like the broken count
+            vx_contact_heat heat{};
+            r = contact_resolve(&p->s, p->s.drift, prm->restitution, prm->friction, &heat);
+            if (r != VX_OK) return r;
+            for (uint32_t k = 0; k < S; ++k)
+                if (on[k]) {
+                    st[k].restitution_heat += heat.restitution;
+                    st[k].friction_heat += heat.friction;
+                }
+        }
         VX_POOL_TRY(cudaStreamSynchronize(p->s.stream), "pool step");
     }
     if (out)

@@ -138,18 +138,22 @@ cudaError_t launch_predict(vx_scene* s, const double* gravity, double h) {
     return cudaGetLastError();
 }
 
-__global__ void k_rest_positions(size_t count, const double* __restrict__ pos, float* __restrict__ rest) {
+// rest[a][first + t] = pos[a][first + t] in f32, t < count, every axis
+__global__ void k_rest_positions(uint32_t n, size_t first, size_t count, const double* __restrict__ pos,
+                                 float* __restrict__ rest) {
     const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (t < count) rest[t] = (float)pos[t];
+    if (t >= 3 * count) return;
+    const size_t k = (t / count) * n + first + t % count;
+    rest[k] = (float)pos[k];
 }
 
 // Scene::rest_positions: the creation positions in f32 (src/scene.rs:520-522)
-cudaError_t launch_rest_positions(vx_scene* s) {
-    const size_t count = 3 * (size_t)s->n;
+cudaError_t launch_rest_range(vx_scene* s, size_t first, size_t count) {
     if (count == 0) return cudaSuccess;
-    k_rest_positions<<<(unsigned)((count + 255) / 256), 256, 0, s->stream>>>(count, s->pos, s->rest);
+    k_rest_positions<<<(unsigned)((3 * count + 255) / 256), 256, 0, s->stream>>>(s->n, first, count, s->pos, s->rest);
     return cudaGetLastError();
 }
+cudaError_t launch_rest_positions(vx_scene* s) { return launch_rest_range(s, 0, s->n); }
 
 cudaError_t launch_velocity(vx_scene* s, double h) {
     if (s->n == 0) return cudaSuccess;
@@ -233,7 +237,7 @@ extern "C" int32_t vx_scene_step(vx_scene* s, const vx_step_params* p, vx_step_s
         }
         if (p->contact) {
             vx_contact_stats cs{};
-            r = contact_project(s, &cs);
+            r = contact_project(s, &cs, nullptr);
             if (r != VX_OK) return r;
             st.contacts += cs.contacts;
         }

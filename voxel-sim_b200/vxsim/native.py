@@ -108,7 +108,7 @@ class VxStepStats(C.Structure):
 
 class VxContactStats(C.Structure):
     _fields_ = [("candidates", C.c_uint64), ("pairs", C.c_uint64), ("contacts", C.c_uint32), ("sweeps", C.c_uint32),
-                ("live_max", C.c_uint32), ("redone", C.c_uint32), ("launches", C.c_uint32)]
+                ("live_max", C.c_uint32), ("redone", C.c_uint32), ("launches", C.c_uint32), ("stored", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -587,13 +587,15 @@ def _bind_pool(L):
     L.vx_pool_add.argtypes = [C.c_void_p, C.POINTER(VxSceneDesc), C.POINTER(C.c_uint32)]
     L.vx_pool_remove.argtypes = [C.c_void_p, C.c_uint32]
     for name in ("vx_pool_set_positions", "vx_pool_get_positions", "vx_pool_get_rotations", "vx_pool_set_loads",
-                 "vx_pool_set_predicted", "vx_pool_set_velocities", "vx_pool_get_velocities"):
+                 "vx_pool_set_predicted", "vx_pool_set_velocities", "vx_pool_get_velocities",
+                 "vx_pool_set_previous", "vx_pool_get_previous"):
         getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, f64p]
     L.vx_pool_set_targets.argtypes = [C.c_void_p, C.c_uint32, u8p, f64p]
     L.vx_pool_fit_rotations.argtypes = [C.c_void_p, u8p, f64p]
     L.vx_pool_pass.argtypes = [C.c_void_p, u8p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
     L.vx_pool_bond_stress.argtypes = [C.c_void_p, C.c_uint32, f32p, f32p, u32p, C.c_uint32, u32p]
     L.vx_pool_step.argtypes = [C.c_void_p, u8p, C.POINTER(VxStepParams), C.POINTER(VxStepStats)]
+    L.vx_pool_contact_project.argtypes = [C.c_void_p, u8p, C.POINTER(VxContactStats), u32p]
     L.vx_pool_checkpoint.argtypes = [C.c_void_p, C.c_int32]
     L.vx_pool_stream.restype = C.c_void_p
     L.vx_pool_stream.argtypes = [C.c_void_p]
@@ -678,6 +680,23 @@ class DevicePool:
     def set_velocities(self, slot, v):
         x = self._v(v)
         check(load().vx_pool_set_velocities(self.h, slot, _p(x, C.c_double)))
+
+    def set_previous(self, slot, x):
+        x = self._v(x)
+        check(load().vx_pool_set_previous(self.h, slot, _p(x, C.c_double)))
+
+    def previous(self, slot):
+        out = np.zeros(3 * self.n[slot], np.float64)
+        check(load().vx_pool_get_previous(self.h, slot, _p(out, C.c_double)))
+        return out.reshape(-1, 3)
+
+    def contact_project(self, enabled=None):
+        """vx_pool_contact_project: (call statistics, contacts per slot)."""
+        m = self._mask(enabled)
+        st = VxContactStats()
+        per = np.zeros(self.slots, np.uint32)
+        check(load().vx_pool_contact_project(self.h, _p(m, C.c_uint8), C.byref(st), _p(per, C.c_uint32)))
+        return st.as_dict(), per
 
     def velocities(self, slot) -> np.ndarray:
         out = np.zeros(3 * self.n[slot], np.float64)
