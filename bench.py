@@ -521,10 +521,11 @@ def served_arm(args):
             "value": st["solves"] / out["wall_s"] * world, "unit": "solves/s", "n_gpus": world,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic",
-            "config": {"workload": "served: wood blocks pressed by a driven blade stand-in",
+            "config": {"workload": "served: wood blocks cut by a driven iron blade through contact and fracture",
                        "arrival_rate_per_s": out["arrival_rate"], "arrival_window_s": out["arrival_window_s"],
                        "steps_per_request": out["steps_per_request"], "max_slots": args.slots,
-                       "dof_range": out["dof_range"], "hbm_budget": 0.8, "parallelism": f"replicas{world}"},
+                       "dof_range": out["dof_range"], "hbm_budget": 0.8, "blade": out["blade"],
+                       "parallelism": f"replicas{world}"},
             "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"], "max_step_ms": st["max_step_ms"],
             "scene_steps_per_s": st["scene_steps"] / out["wall_s"],
             "requests": out["requests"], "completed": out["completed"], "not_converged": out["not_converged"],

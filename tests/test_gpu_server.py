@@ -101,3 +101,41 @@ def test_moving_targets_advance_with_the_tool(ctx):
     bottom = s.kinematic == 1
     assert np.array_equal(x[bottom], s.position[bottom])
     srv.close()
+
+
+def test_blade_cuts_through_contact(ctx):
+    """The served scene with a kinematic iron blade driven at 1 m/s into the
+    wood: the server steps it with contact and fracture; the blade moved by
+    the tool's advance, the wood under its edge was pushed down with it and
+    no wood REV is left inside the blade's cross-section below its edge.
+    The same request alone and in a mix ends with the same bits."""
+    from vxsim import served as V
+    rng = np.random.default_rng(21)
+    scene, blade = V.served_scene(rng, dof_lo=3e3, dof_hi=6e3)
+    other, other_blade = V.served_scene(rng, dof_lo=3e3, dof_hi=6e3)
+    p = N.step_params(1e-3, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5, gravity=(0, 0, -9.81),
+                      tolerance=1e-8, max_iterations=20000, precision=N.PRECISION_MIXED, fracture=True,
+                      contact=True)
+    steps = 20
+    srv = N.Server(ctx, p, max_slots=4, max_revs=scene.n + other.n + 4096)
+    alone = srv.wait(srv.submit(scene, steps, target_velocity=(0.0, 0.0, -1.0), moving=blade))
+    t1 = srv.submit(other, steps, target_velocity=(0.0, 0.0, -1.0), moving=other_blade)
+    t2 = srv.submit(scene, steps, target_velocity=(0.0, 0.0, -1.0), moving=blade)
+    mixed = srv.wait(t2)
+    assert srv.wait(t1)[0]["status"] in (N.VX_OK, N.VX_NOT_CONVERGED)
+    srv.close()
+    res, x = alone
+    assert res["status"] in (N.VX_OK, N.VX_NOT_CONVERGED) and res["steps_done"] == steps
+    assert np.array_equal(x, mixed[1])
+    x0 = scene.position
+    # the blade followed its targets: 20 steps of 1 mm
+    assert np.allclose(x[blade, 2] - x0[blade, 2], -0.02, atol=1e-9)
+    # wood REVs under the edge went down with it
+    edge_z = x[blade, 2].min()
+    lo = x[blade, :2].min(axis=0) - 0.004
+    hi = x[blade, :2].max(axis=0) + 0.004
+    wood = ~blade
+    under = wood & np.all((x0[:, :2] >= lo) & (x0[:, :2] <= hi), axis=1) & (x0[:, 2] > x0[wood, 2].max() - 0.025)
+    assert np.any(under) and np.min(x[under, 2] - x0[under, 2]) < -0.005
+    inside = wood & np.all((x[:, :2] > lo + 0.004) & (x[:, :2] < hi - 0.004), axis=1) & (x[:, 2] > edge_z + 0.005)
+    assert not np.any(inside)

@@ -18,17 +18,19 @@
 //
 // Projection. The reference sweeps the pairs in order, and each correction is
 // seen by the pairs after it (Gauss-Seidel). The device keeps that order
-// exactly: with a bound M on how far any REV moves during a sweep, a pair whose
-// boxes stay farther apart than the contact tests reach even after both REVs
-// move by M cannot act or report a contact in that sweep ("inert"). The other
-// ("live") pairs are grouped into connected components over shared REVs; one
-// thread replays each component's pairs in pair order, so every pair sees the
-// same positions it sees in the reference's sweep. After the sweep the largest
-// movement of any REV is checked against M; when it is larger the sweep is
-// restored and replayed with a wider bound (finally with every pair live).
-// Contact velocity resolution runs the same way over components of the
-// contact list; its sweeps stop per component when nothing changes, which is
-// what the reference's global stop does to that component.
+// exactly: with a bound M on how far any REV moves during a sweep, a pair
+// whose boxes stay farther apart than the contact tests reach even after both
+// REVs move by M cannot act or report a contact in that sweep. Each sweep
+// stores only the other pairs, which are grouped into connected components
+// over the REVs that can move; one thread replays each component's pairs in
+// pair order, so every pair sees the same positions it sees in the reference's
+// sweep. After the sweep the largest movement of any REV is checked against M;
+// when it is larger the sweep is restored and replayed with the pairs of a
+// wider bound (finally with every pair). The contacts of the sweeps are
+// merged by pair, the first one of each pair kept. Contact velocity
+// resolution runs over components of the contact list; its sweeps stop per
+// component when nothing changes, which is what the reference's global stop
+// does to that component.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -61,7 +63,7 @@ constexpr unsigned kUnionRetries = 1u << 16;
 constexpr uint64_t kMaxLargeVolume = 1ull << 24;  // bins one fast REV may sweep in a substep
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kScanBlock = 1024;
-constexpr double kSweepBound = 5e-4;  // metres a REV may move in one sweep before the call is replayed
+constexpr double kSweepBound = 5e-4;  // metres a REV may move in a sweep before it is replayed with more pairs
 
 enum : uint32_t {
     E_OK = 0,
@@ -513,26 +515,6 @@ __global__ void k_sort_segments(uint32_t n, const uint32_t* __restrict__ off, ui
 
 // ---- projection sweeps -----------------------------------------------------
 
-// A pair is live when, with both REVs moved by at most M, one of the three
-// tests can still answer: its end separation within H = CELL + slop + 2M (+ a
-// rounding margin) on every axis, or (unless the starts already overlap) its
-// relative path from the start separation to the end one meeting the box of
-// half-width H.
-__global__ void k_classify(uint32_t count, const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj, uint32_t n,
-                           const double* __restrict__ pos, const double* __restrict__ start, double half,
-                           uint8_t* __restrict__ live) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    const uint32_t i = pi[k], j = pj[k];
-    live[k] = may_act(load3(start, n, i), load3(start, n, j), load3(pos, n, i), load3(pos, n, j), half) ? 1 : 0;
-}
-
-__global__ void k_compact(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
-                          uint32_t* __restrict__ out) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < count && flag[k]) out[off[k]] = k;
-}
-
 __global__ void k_iota(uint32_t n, uint32_t* __restrict__ v) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
@@ -684,7 +666,7 @@ __device__ bool separate(const SweepArgs& a, uint32_t i, uint32_t j, int code, d
     return true;
 }
 
-// One thread replays one component's live pairs in pair order.
+// One thread replays one component's pairs in pair order.
 __global__ void k_sweep(SweepArgs a) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= a.n) return;
@@ -727,38 +709,79 @@ __global__ void k_max_move(uint32_t n, const double* __restrict__ move, unsigned
     if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
-// The first contact of each pair over the sweeps is kept (the reference sorts
-// the pushed contacts by pair and keeps one per pair).
-__global__ void k_merge(uint32_t count, const uint32_t* __restrict__ live_list, const int8_t* __restrict__ code,
-                        const uint8_t* __restrict__ impact, int8_t* __restrict__ first_code,
-                        uint8_t* __restrict__ first_impact) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const uint32_t k = live_list[t];
-    if (code[k] && !first_code[k]) {
-        first_code[k] = code[k];
-        first_impact[k] = impact[k];
-    }
-}
-
-__global__ void k_contact_flags(uint32_t count, const int8_t* __restrict__ code, uint8_t* __restrict__ flag) {
+// This sweep's contacts, in pair order: key (i << 32 | j), normal code, impact.
+__global__ void k_sweep_contact_flags(uint32_t count, const int8_t* __restrict__ code, uint8_t* __restrict__ flag) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < count) flag[k] = code[k] != 0;
 }
-
-__global__ void k_contact_write(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
-                                const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj,
-                                const int8_t* __restrict__ code, const uint8_t* __restrict__ impact, uint32_t* ci,
-                                uint32_t* cj, int8_t* cn, uint8_t* cm, const uint32_t* __restrict__ rslot,
-                                uint32_t* slot_contacts) {
+__global__ void k_sweep_contact_write(uint32_t count, const uint8_t* __restrict__ flag, const uint32_t* __restrict__ off,
+                                      const uint32_t* __restrict__ pi, const uint32_t* __restrict__ pj,
+                                      const int8_t* __restrict__ code, const uint8_t* __restrict__ impact,
+                                      unsigned long long* key, int8_t* cn, uint8_t* cm) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count || !flag[k]) return;
     const uint32_t o = off[k];
-    ci[o] = pi[k];
-    cj[o] = pj[k];
+    key[o] = ((unsigned long long)pi[k] << 32) | pj[k];
     cn[o] = code[k];
     cm[o] = impact[k];
-    if (slot_contacts) atomicAdd(slot_contacts + rslot[pi[k]], 1u);
+}
+
+// First index of v[0, n) not below key (v ascending).
+__device__ __forceinline__ uint32_t lower_bound(const unsigned long long* v, uint32_t n, unsigned long long key) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (v[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The recorded contacts keep each pair's first contact over the sweeps (the
+// reference sorts the pushed contacts by pair and keeps one per pair). A
+// sweep's list B joins the recorded list A (both ascending): B's pairs already
+// in A are dropped, the rest are merged in by rank.
+__global__ void k_new_contacts(uint32_t nb, const unsigned long long* __restrict__ bkey, uint32_t na,
+                               const unsigned long long* __restrict__ akey, uint8_t* __restrict__ keep) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const uint32_t at = lower_bound(akey, na, bkey[b]);
+    keep[b] = !(at < na && akey[at] == bkey[b]);
+}
+__global__ void k_merge_recorded(uint32_t na, const unsigned long long* __restrict__ akey,
+                                 const int8_t* __restrict__ acn, const uint8_t* __restrict__ acm, uint32_t nb,
+                                 const unsigned long long* __restrict__ bkey, const int8_t* __restrict__ bcn,
+                                 const uint8_t* __restrict__ bcm, const uint8_t* __restrict__ keep,
+                                 const uint32_t* __restrict__ boff, unsigned long long* okey, int8_t* ocn,
+                                 uint8_t* ocm) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < na) {  // kept B entries before it: B's kept prefix up to its first key not below A's
+        const uint32_t o = t + boff[lower_bound(bkey, nb, akey[t])];
+        okey[o] = akey[t];
+        ocn[o] = acn[t];
+        ocm[o] = acm[t];
+    } else if (t < na + nb) {
+        const uint32_t b = t - na;
+        if (!keep[b]) return;
+        const uint32_t o = boff[b] + lower_bound(akey, na, bkey[b]);
+        okey[o] = bkey[b];
+        ocn[o] = bcn[b];
+        ocm[o] = bcm[b];
+    }
+}
+
+__global__ void k_contacts_out(uint32_t count, const unsigned long long* __restrict__ key,
+                               const int8_t* __restrict__ rcn, const uint8_t* __restrict__ rcm, uint32_t* ci,
+                               uint32_t* cj, int8_t* cn, uint8_t* cm, const uint32_t* __restrict__ rslot,
+                               uint32_t* slot_contacts) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t i = (uint32_t)(key[k] >> 32);
+    ci[k] = i;
+    cj[k] = (uint32_t)key[k];
+    cn[k] = rcn[k];
+    cm[k] = rcm[k];
+    if (slot_contacts) atomicAdd(slot_contacts + rslot[i], 1u);
 }
 
 // ---- contact velocities -------------------------------------------------
@@ -974,7 +997,6 @@ struct ContactState {
     // per REV
     Boxes box{};
     double* start = nullptr;    // [3][n] previous positions when the call began
-    double* entry = nullptr;    // [3][n] positions when the call began
     double* snap = nullptr;     // [6][n] positions and previous at the start of a sweep
     double* move = nullptr;     // [n]
     double* heat = nullptr;     // [2][n]
@@ -997,16 +1019,23 @@ struct ContactState {
     // per pair
     uint32_t* pi = nullptr;
     uint32_t* pj = nullptr;
-    uint8_t* live = nullptr;
-    uint32_t* live_off = nullptr;  // [cap + 1]
-    uint32_t* live_list = nullptr;
     uint32_t* root = nullptr;
     uint32_t* items = nullptr;
     int8_t* code = nullptr;
     uint8_t* impact = nullptr;
-    int8_t* first_code = nullptr;
-    uint8_t* first_impact = nullptr;
-    // contacts
+    uint8_t* sw_flag = nullptr;     // [cap] this sweep's contact flags
+    uint32_t* sw_off = nullptr;     // [cap + 1]
+    // contacts: this sweep's list, the recorded list (two buffers), the output
+    size_t contact_cap = 0;
+    unsigned long long* sw_key = nullptr;
+    int8_t* sw_cn = nullptr;
+    uint8_t* sw_cm = nullptr;
+    uint8_t* sw_keep = nullptr;
+    uint32_t* sw_koff = nullptr;   // [contact_cap + 1]
+    unsigned long long* rec_key[2] = {nullptr, nullptr};
+    int8_t* rec_cn[2] = {nullptr, nullptr};
+    uint8_t* rec_cm[2] = {nullptr, nullptr};
+    size_t rec_cap[2] = {0, 0};
     uint32_t* ci = nullptr;
     uint32_t* cj = nullptr;
     int8_t* cn = nullptr;
@@ -1084,7 +1113,6 @@ cudaError_t ensure_state(vx_scene* s) {
     if (e == cudaSuccess) e = alloc(c->box.slot, n);
     if (e == cudaSuccess && s->pool_slots) e = alloc(c->slot_contacts, s->pool_slots);
     if (e == cudaSuccess) e = alloc(c->start, 3 * n);
-    if (e == cudaSuccess) e = alloc(c->entry, 3 * n);
     if (e == cudaSuccess) e = alloc(c->snap, 6 * n);
     if (e == cudaSuccess) e = alloc(c->move, n);
     if (e == cudaSuccess) e = alloc(c->heat, 2 * n);
@@ -1107,27 +1135,65 @@ cudaError_t ensure_state(vx_scene* s) {
 cudaError_t ensure_pairs(ContactState* c, size_t want) {
     if (want <= c->pair_cap && c->pi) return cudaSuccess;
     size_t cap = std::max<size_t>(want + want / 4, 4096);
-    void* ptrs[] = {c->pi, c->pj, c->live, c->live_off, c->live_list, c->root, c->items,
-                    c->code, c->impact, c->first_code, c->first_impact, c->ci, c->cj, c->cn, c->cm};
+    void* ptrs[] = {c->pi, c->pj, c->root, c->items, c->code, c->impact, c->sw_flag, c->sw_off};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    c->pi = c->pj = c->root = c->items = c->sw_off = nullptr;
+    c->impact = c->sw_flag = nullptr;
+    c->code = nullptr;
     c->pair_cap = 0;
     cudaError_t e = alloc(c->pi, cap);
     if (e == cudaSuccess) e = alloc(c->pj, cap);
-    if (e == cudaSuccess) e = alloc(c->live, cap);
-    if (e == cudaSuccess) e = alloc(c->live_off, cap + 1);
-    if (e == cudaSuccess) e = alloc(c->live_list, cap);
     if (e == cudaSuccess) e = alloc(c->root, cap);
     if (e == cudaSuccess) e = alloc(c->items, cap);
     if (e == cudaSuccess) e = alloc(c->code, cap);
     if (e == cudaSuccess) e = alloc(c->impact, cap);
-    if (e == cudaSuccess) e = alloc(c->first_code, cap);
-    if (e == cudaSuccess) e = alloc(c->first_impact, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_flag, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_off, cap + 1);
+    if (e == cudaSuccess) c->pair_cap = cap;
+    return e;
+}
+
+// The output contact list and the per-sweep list: want entries.
+cudaError_t ensure_contacts(ContactState* c, size_t want) {
+    if (want <= c->contact_cap && c->ci) return cudaSuccess;
+    size_t cap = std::max<size_t>(want + want / 4, 4096);
+    void* own[] = {c->sw_key, c->sw_cn, c->sw_cm, c->sw_keep, c->sw_koff, c->ci, c->cj, c->cn, c->cm};
+    for (void* p : own)
+        if (p) cudaFree(p);
+    c->sw_key = nullptr;
+    c->sw_cn = c->cn = nullptr;
+    c->sw_cm = c->sw_keep = c->cm = nullptr;
+    c->sw_koff = c->ci = c->cj = nullptr;
+    c->contact_cap = 0;
+    cudaError_t e = alloc(c->sw_key, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_cn, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_cm, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_keep, cap);
+    if (e == cudaSuccess) e = alloc(c->sw_koff, cap + 1);
     if (e == cudaSuccess) e = alloc(c->ci, cap);
     if (e == cudaSuccess) e = alloc(c->cj, cap);
     if (e == cudaSuccess) e = alloc(c->cn, cap);
     if (e == cudaSuccess) e = alloc(c->cm, cap);
-    if (e == cudaSuccess) c->pair_cap = cap;
+    if (e == cudaSuccess) c->contact_cap = cap;
+    return e;
+}
+
+// Recorded-contact buffer b can hold want entries (its contents are not kept).
+cudaError_t ensure_recorded(ContactState* c, int b, size_t want) {
+    if (want <= c->rec_cap[b] && c->rec_key[b]) return cudaSuccess;
+    size_t cap = std::max<size_t>(want + want / 4, 4096);
+    if (c->rec_key[b]) cudaFree(c->rec_key[b]);
+    if (c->rec_cn[b]) cudaFree(c->rec_cn[b]);
+    if (c->rec_cm[b]) cudaFree(c->rec_cm[b]);
+    c->rec_key[b] = nullptr;
+    c->rec_cn[b] = nullptr;
+    c->rec_cm[b] = nullptr;
+    c->rec_cap[b] = 0;
+    cudaError_t e = alloc(c->rec_key[b], cap);
+    if (e == cudaSuccess) e = alloc(c->rec_cn[b], cap);
+    if (e == cudaSuccess) e = alloc(c->rec_cm[b], cap);
+    if (e == cudaSuccess) c->rec_cap[b] = cap;
     return e;
 }
 
@@ -1206,10 +1272,12 @@ void contact_release(vx_scene* s) {
     if (!c) return;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->box.slot, c->slot_contacts, c->start, c->entry, c->snap, c->move, c->heat, c->phys, c->next1,
+    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->box.slot, c->slot_contacts, c->start, c->snap, c->move, c->heat, c->phys, c->next1,
                     c->cnt, c->off, c->parent, c->comp_cnt, c->comp_off, c->bsum, c->keys1, c->heads1, c->keys2,
-                    c->heads2, c->ent_id, c->ent_next, c->pi, c->pj, c->live, c->live_off, c->live_list, c->root,
-                    c->items, c->code, c->impact, c->first_code, c->first_impact, c->ci, c->cj, c->cn, c->cm,
+                    c->heads2, c->ent_id, c->ent_next, c->pi, c->pj, c->root,
+                    c->items, c->code, c->impact, c->sw_flag, c->sw_off, c->sw_key, c->sw_cn, c->sw_cm,
+                    c->sw_keep, c->sw_koff, c->rec_key[0], c->rec_key[1], c->rec_cn[0], c->rec_cn[1],
+                    c->rec_cm[0], c->rec_cm[1], c->ci, c->cj, c->cn, c->cm,
                     c->scal, c->max_move, c->heat_sum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1307,164 +1375,169 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
     pa.scal = c->scal;
     pa.pos = s->pos;
     pa.start = c->start;
-    // The projection first stores only the pairs that can act within six sweeps
-    // when no REV moves more than kSweepBound per sweep (the lattice's
-    // two-cell neighbours never can). When a sweep moves a REV farther, the
-    // call starts again from its entry state storing every pair, and then widens
-    // the bound sweep by sweep. Both ways replay the reference's sweeps exactly.
-    e = cudaMemcpyAsync(c->entry, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
-    if (e != cudaSuccess) return cuda_fail(e, what);
-    uint32_t stored = 0;
-    bool full = false;
-    for (;;) {  // at most twice: bounded storage, then every pair
-        pa.half = full ? 1e300 : kCell + kSlop + 2.0 * 6.0 * kSweepBound + 1e-9;
+    // Each sweep stores only the pairs that can act in it when no REV moves
+    // more than the sweep's bound M (first kSweepBound): the lattice's two-cell
+    // neighbours never can. When a REV moves farther, the sweep is restored and
+    // replayed with the pairs of a wider bound, and after four widenings with
+    // every pair. The replay is exact at any bound.
+    bool first_generation = true;
+    auto generate = [&](double half, uint32_t* out_stored) -> int32_t {
+        pa.half = half;
         pa.pi = nullptr;
         pa.pj = nullptr;
-        e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
-        if (e != cudaSuccess) return cuda_fail(e, what);
+        cudaError_t ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+        if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
+        if (ge != cudaSuccess) return cuda_fail(ge, what);
         k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
         c->launches += 1;
-        e = scan(c, st, c->cnt, c->off, n);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        if (e != cudaSuccess) return cuda_fail(e, what);
-        r = read_scalars(s, c, what);
-        if (r != VX_OK) return r;
-        stored = c->h_scal[18];
-        st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
-        st_out.pairs = (uint64_t)c->h_scal[S_PAIRS_LO] | ((uint64_t)c->h_scal[S_PAIRS_HI] << 32);
-        st_out.stored = stored;
-        e = ensure_pairs(c, stored);
-        if (e != cudaSuccess) {
-            set_error("%s: %u stored pairs: %s", what, stored, cudaGetErrorString(e));
+        ge = scan(c, st, c->cnt, c->off, n);
+        if (ge == cudaSuccess)
+            ge = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (ge != cudaSuccess) return cuda_fail(ge, what);
+        int32_t gr = read_scalars(s, c, what);
+        if (gr != VX_OK) return gr;
+        const uint32_t stored = c->h_scal[18];
+        if (first_generation) {  // the candidate and pair counts do not depend on the bound
+            st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
+            st_out.pairs = (uint64_t)c->h_scal[S_PAIRS_LO] | ((uint64_t)c->h_scal[S_PAIRS_HI] << 32);
+            first_generation = false;
+        }
+        st_out.stored = std::max<uint64_t>(st_out.stored, stored);
+        ge = ensure_pairs(c, stored);
+        if (ge != cudaSuccess) {
+            set_error("%s: %u stored pairs: %s", what, stored, cudaGetErrorString(ge));
             return VX_OOM;
         }
         pa.pi = c->pi;
         pa.pj = c->pj;
-        e = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
-        if (e == cudaSuccess && stored) e = cudaMemsetAsync(c->first_code, 0, stored, st);
-        if (e != cudaSuccess) return cuda_fail(e, what);
         if (stored) {
+            ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
+            if (ge != cudaSuccess) return cuda_fail(ge, what);
             k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
             k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
             c->launches += 2;
         }
-        // the sweeps (project :51-103)
-        SweepArgs sa{};
-        sa.n = n;
-        sa.comp_off = c->comp_off;
-        sa.items = c->items;
-        sa.pi = c->pi;
-        sa.pj = c->pj;
-        sa.pos = s->pos;
-        sa.prev = s->prev;
-        sa.start = c->start;
-        sa.kin = s->kin;
-        sa.param1 = s->param1;
-        sa.tmask = s->tmask;
-        sa.move = c->move;
-        sa.code = c->code;
-        sa.impact = c->impact;
-        sa.scal = c->scal;
-        st_out.sweeps = stored ? 0 : 1;  // the reference's first sweep runs over an empty list
-        bool restart = false;
-        for (int sweep = 0; sweep < 6 && stored && !restart; ++sweep) {
-            st_out.sweeps += 1;
-            e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
+        *out_stored = stored;
+        return VX_OK;
+    };
+    SweepArgs sa{};  // the pair arrays are bound after each generation, which may reallocate them
+    sa.n = n;
+    sa.comp_off = c->comp_off;
+    sa.pos = s->pos;
+    sa.prev = s->prev;
+    sa.start = c->start;
+    sa.kin = s->kin;
+    sa.param1 = s->param1;
+    sa.tmask = s->tmask;
+    sa.move = c->move;
+    sa.scal = c->scal;
+    uint32_t recorded = 0;
+    int cur = 0;
+    for (int sweep = 0; sweep < 6; ++sweep) {  // the sweeps (project :51-103)
+        st_out.sweeps += 1;
+        e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        double bound = kSweepBound;
+        bool changed = false;
+        uint32_t stored = 0;
+        for (int attempt = 0;; ++attempt) {
+            const bool all_pairs = attempt >= 4;
+            r = generate(all_pairs ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9, &stored);
+            if (r != VX_OK) return r;
+            e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
             if (e != cudaSuccess) return cuda_fail(e, what);
-            double bound = kSweepBound;
-            bool changed = false;
-            for (int attempt = 0;; ++attempt) {
-                const bool all_live = full && attempt >= 4;
-                const double half = all_live ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9;
-                e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
-                if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
-                if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
-                if (e != cudaSuccess) return cuda_fail(e, what);
-                k_classify<<<grid(stored), 256, 0, st>>>(stored, c->pi, c->pj, n, s->pos, c->start, half, c->live);
+            st_out.live_max = std::max(st_out.live_max, stored);
+            sa.pi = c->pi;
+            sa.pj = c->pj;
+            sa.items = c->items;
+            sa.code = c->code;
+            sa.impact = c->impact;
+            e = components(s, c, stored, nullptr, c->pi, c->pj, c->items);
+            if (e != cudaSuccess) return cuda_fail(e, what);
+            if (stored) {
+                k_sweep<<<grid(n), 256, 0, st>>>(sa);
                 c->launches += 1;
-                e = scan(c, st, c->live, c->live_off, stored);
-                if (e != cudaSuccess) return cuda_fail(e, what);
-                k_compact<<<grid(stored), 256, 0, st>>>(stored, c->live, c->live_off, c->live_list);
-                c->launches += 1;
-                e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + stored, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                    st);
-                if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-                if (e != cudaSuccess) return cuda_fail(e, what);
-                const uint32_t live = c->h_scal[18];
-                st_out.live_max = std::max(st_out.live_max, live);
-                e = components(s, c, live, c->live_list, c->pi, c->pj, c->items);
-                if (e != cudaSuccess) return cuda_fail(e, what);
-                if (live) {
-                    k_sweep<<<grid(n), 256, 0, st>>>(sa);
-                    c->launches += 1;
-                }
-                k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
-                c->launches += 1;
-                r = read_scalars(s, c, what);
-                if (r != VX_OK) return r;
-                unsigned long long bits =
-                    (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
-                double moved = 0.0;
-                std::memcpy(&moved, &bits, sizeof moved);
-                changed = c->h_scal[S_CHANGED] != 0;
-                if (all_live || moved <= bound) {
-                    if (live) {
-                        k_merge<<<grid(live), 256, 0, st>>>(live, c->live_list, c->code, c->impact, c->first_code,
-                                                            c->first_impact);
-                        c->launches += 1;
-                    }
-                    break;
-                }
-                st_out.redone += 1;
-                if (!full) {  // start the call again from its entry state, storing every pair
-                    e = cudaMemcpyAsync(s->pos, c->entry, v3b, cudaMemcpyDeviceToDevice, st);
-                    if (e == cudaSuccess) e = cudaMemcpyAsync(s->prev, c->start, v3b, cudaMemcpyDeviceToDevice, st);
-                    if (e != cudaSuccess) return cuda_fail(e, what);
-                    restart = true;
-                    break;
-                }
-                // a REV moved farther than the bound: replay from the sweep's start
-                e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
-                if (e == cudaSuccess)
-                    e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
-                if (e != cudaSuccess) return cuda_fail(e, what);
-                bound = std::max(2.0 * moved, 4.0 * bound);
             }
-            if (!restart && !changed) break;
-        }
-        if (!restart) break;
-        full = true;
-    }
-    const uint32_t pairs = stored;
-    // contacts in pair order
-    if (pairs) {
-        uint32_t* per_slot = pooled && slot_contacts ? c->slot_contacts : nullptr;
-        if (per_slot) {
-            e = cudaMemsetAsync(per_slot, 0, s->pool_slots * sizeof(uint32_t), st);
+            k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
+            c->launches += 1;
+            r = read_scalars(s, c, what);
+            if (r != VX_OK) return r;
+            unsigned long long bits = (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
+            double moved = 0.0;
+            std::memcpy(&moved, &bits, sizeof moved);
+            changed = c->h_scal[S_CHANGED] != 0;
+            if (all_pairs || moved <= bound) break;
+            // a REV moved farther than the bound: replay from the sweep's start
+            st_out.redone += 1;
+            e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) return cuda_fail(e, what);
+            bound = std::max(2.0 * moved, 4.0 * bound);
         }
-        k_contact_flags<<<grid(pairs), 256, 0, st>>>(pairs, c->first_code, c->live);
-        c->launches += 1;
-        e = scan(c, st, c->live, c->live_off, pairs);
-        if (e != cudaSuccess) return cuda_fail(e, what);
-        k_contact_write<<<grid(pairs), 256, 0, st>>>(pairs, c->live, c->live_off, c->pi, c->pj, c->first_code,
-                                                     c->first_impact, c->ci, c->cj, c->cn, c->cm, c->box.slot,
-                                                     per_slot);
-        if (per_slot) {
-            e = cudaMemcpyAsync(slot_contacts, per_slot, s->pool_slots * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (stored) {  // this sweep's contacts join the recorded ones
+            k_sweep_contact_flags<<<grid(stored), 256, 0, st>>>(stored, c->code, c->sw_flag);
+            c->launches += 1;
+            e = scan(c, st, c->sw_flag, c->sw_off, stored);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&c->h_scal[18], c->sw_off + stored, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return cuda_fail(e, what);
+            const uint32_t nb = c->h_scal[18];
+            if (nb) {
+                e = ensure_contacts(c, std::max<size_t>(nb, recorded));
+                if (e == cudaSuccess) e = ensure_recorded(c, 1 - cur, (size_t)recorded + nb);
+                if (e != cudaSuccess) {
+                    set_error("%s: %u contacts: %s", what, recorded + nb, cudaGetErrorString(e));
+                    return VX_OOM;
+                }
+                k_sweep_contact_write<<<grid(stored), 256, 0, st>>>(stored, c->sw_flag, c->sw_off, c->pi, c->pj, c->code,
+                                                                    c->impact, c->sw_key, c->sw_cn, c->sw_cm);
+                k_new_contacts<<<grid(nb), 256, 0, st>>>(nb, c->sw_key, recorded, c->rec_key[cur], c->sw_keep);
+                c->launches += 2;
+                e = scan(c, st, c->sw_keep, c->sw_koff, nb);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(&c->h_scal[19], c->sw_koff + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                k_merge_recorded<<<grid((size_t)recorded + nb), 256, 0, st>>>(
+                    recorded, c->rec_key[cur], c->rec_cn[cur], c->rec_cm[cur], nb, c->sw_key, c->sw_cn, c->sw_cm,
+                    c->sw_keep, c->sw_koff, c->rec_key[1 - cur], c->rec_cn[1 - cur], c->rec_cm[1 - cur]);
+                c->launches += 1;
+                e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess) return cuda_fail(e, what);
+                recorded += c->h_scal[19];
+                cur = 1 - cur;
+            }
         }
-        c->launches += 1;
-        e = cudaMemcpyAsync(&c->h_scal[18], c->live_off + pairs, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return cuda_fail(e, what);
-        c->contacts = c->h_scal[18];
+        if (!changed) break;
     }
-    st_out.contacts = c->contacts;
+    // the recorded contacts, sorted by pair
+    uint32_t* per_slot = pooled && slot_contacts ? c->slot_contacts : nullptr;
+    if (per_slot) {
+        e = cudaMemsetAsync(per_slot, 0, s->pool_slots * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+    }
+    if (recorded) {
+        e = ensure_contacts(c, recorded);
+        if (e != cudaSuccess) {
+            set_error("%s: %u contacts: %s", what, recorded, cudaGetErrorString(e));
+            return VX_OOM;
+        }
+        k_contacts_out<<<grid(recorded), 256, 0, st>>>(recorded, c->rec_key[cur], c->rec_cn[cur], c->rec_cm[cur], c->ci,
+                                                       c->cj, c->cn, c->cm, c->box.slot, per_slot);
+        c->launches += 1;
+    }
+    if (per_slot) {
+        e = cudaMemcpyAsync(slot_contacts, per_slot, s->pool_slots * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+    }
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    c->contacts = recorded;
+    st_out.contacts = recorded;
     st_out.launches = c->launches;
     if (out) *out = st_out;
     return VX_OK;
@@ -1483,6 +1556,9 @@ int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restituti
     cudaStream_t st = s->stream;
     vx_contact_heat heat{};
     if (count && n) {
+        // the component scratch (root, items) is pair-sized: it must hold the contacts
+        e = ensure_pairs(c, count);
+        if (e != cudaSuccess) return cuda_fail(e, what);
         const size_t v3b = 3 * (size_t)n * sizeof(double);
         e = cudaMemcpyAsync(c->phys, pre_contact ? pre_contact : s->vel, v3b, cudaMemcpyDeviceToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
@@ -1524,6 +1600,15 @@ int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restituti
 }
 
 uint32_t contact_count(const vx_scene* s) { return s->contact ? s->contact->contacts : 0; }
+
+// Device bytes of the contact buffers that scale with the REV count (the
+// pair buffers grow with the stored pairs, usually a small share).
+uint64_t contact_state_bytes(uint32_t n) {
+    const uint64_t m = n ? n : 1;
+    const uint64_t per_rev = 6 * 4 + 1 + 4 + 3 * 8 * 3 + 6 * 8 + 8 + 2 * 8 + 4 * 7;  // boxes .. component offsets
+    const uint64_t table = pow2_at_least(2 * m);
+    return per_rev * m + table * (8 + 4);
+}
 
 }  // namespace vx
 
@@ -1599,6 +1684,7 @@ extern "C" int32_t vx_scene_set_contacts(vx_scene* s, uint32_t count, const uint
     }
     cudaSetDevice(s->device);
     cudaError_t e = ensure_state(s);
+    if (e == cudaSuccess) e = ensure_contacts(s->contact, count);
     if (e == cudaSuccess) e = ensure_pairs(s->contact, count);
     if (e != cudaSuccess) return cuda_fail(e, "vx_scene_set_contacts");
     ContactState* c = s->contact;

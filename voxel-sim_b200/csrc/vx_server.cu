@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "vx_internal.h"
+#include "vx_kernels.h"
 
 namespace {
 
@@ -243,7 +244,9 @@ int32_t vx_server_create(vx_ctx* ctx, const vx_server_config* cfg, vx_server** o
         }
         const double budget = std::min(cfg->hbm_fraction * (double)total_b, 0.95 * (double)free_b);
         const uint64_t probe = 1ull << 20;
-        const double per_rev = (double)vx_pool_footprint_bytes(probe, cfg->max_slots) / (double)probe;
+        double per_rev = (double)vx_pool_footprint_bytes(probe, cfg->max_slots) / (double)probe;
+        // the contact stage's buffers scale with the pool's REV capacity too
+        if (cfg->step.contact) per_rev += (double)vx::contact_state_bytes((uint32_t)probe) / (double)probe;
         revs = (uint64_t)(budget / per_rev) / 256 * 256;
         if (revs > 0x7FFFFF00ull) revs = 0x7FFFFF00ull;
     }

@@ -2,15 +2,17 @@
 
 Each request is a wood block built as in the batched workload (a union of
 1-4 axis-aligned boxes spanning the cube; size log-uniform over 1k-2M DOF,
-grain random) whose bottom layer is clamped and whose top face is pressed by
-a blade (a 2 x 20 REV footprint of a 2 x 20 x 40 iron blade, centred on the
-top face, with a one-REV bevel: the two rows of its edge) driven into the
-block at 1 m/s. The blade itself is not simulated: contact with it is the
-prescribed displacement of the wood REVs under its edge, which are targeted
-and advance at the blade speed every step (tools and contact projection are
-outside the elastic path). Each request runs 100 fixed steps of 1 ms with
+grain random) whose bottom layer is clamped, with a 2 x 20 x 40 iron blade
+standing on the centre of its top face. The blade is kinematic REVs whose
+targets advance at 1 m/s into the block; its lowest row is one REV thick
+(the bevel). The blade pushes the wood through the contact stage of the step
+(collision::project and the contact velocities), and the wood's bonds go
+through the fracture stage. Each request runs 100 fixed steps of 1 ms with
 its state resident on the device; admission is capped by the pool, sized at
-80% of the device memory.
+80% of the device memory together with the contact buffers.
+
+`blade="targets"` builds the earlier stand-in instead: no blade REVs, the
+wood REVs under the blade's edge are targeted and driven at the blade speed.
 """
 from __future__ import annotations
 
@@ -23,10 +25,10 @@ from . import native as N
 from . import scenes as S
 
 
-def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6) -> tuple:
+def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6, blade: str = "contact") -> tuple:
     """(scene, moving mask) for one request. The boxes are drawn as fractions of
     the cube edge, then the edge is chosen so the union holds about the drawn
-    REV count (DOF / 3)."""
+    REV count (DOF / 3) of wood."""
     revs = math.exp(rng.uniform(math.log(dof_lo / 3.0), math.log(dof_hi / 3.0)))
     boxes = []
     for _ in range(int(rng.integers(1, 5))):
@@ -51,27 +53,49 @@ def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6) -> tuple:
     cells = cells[np.lexsort((cells[:, 0], cells[:, 1], cells[:, 2]))]
     table = S.wood_config_materials()
     g = S.random_unit_vectors(rng, 1)[0]
-    n = len(cells)
-    s = S.from_cells(cells, 1, table, fiber=np.tile(g, (n, 1)), anisotropy=1.0)
-    s.fix_voxels(np.nonzero(cells[:, 2] == 0)[0])
-    # blade edge: 2 rows (the bevel) x 20 REVs along y, centred over the top face's cells
     top = cells[:, 2] == edge - 1
     cx, cy = int(np.round(cells[top, 0].mean())), int(np.round(cells[top, 1].mean()))
-    under = top & (cells[:, 0] >= cx) & (cells[:, 0] <= cx + 1) & (cells[:, 1] >= cy - 10) & (cells[:, 1] < cy + 10)
-    s.target_mask[under] = 7
-    s.target[under] = s.position[under]
-    s.meta.update(workload="served", edge=edge, dt=1e-3, substeps=1, gravity=(0, 0, -9.81))
-    return s, under
+    n_wood = len(cells)
+    if blade == "targets":
+        s = S.from_cells(cells, 1, table, fiber=np.tile(g, (n_wood, 1)), anisotropy=1.0)
+        s.fix_voxels(np.nonzero(cells[:, 2] == 0)[0])
+        # the wood under the blade's edge: 2 rows x 20 REVs along y
+        under = top & (cells[:, 0] >= cx) & (cells[:, 0] <= cx + 1) & (cells[:, 1] >= cy - 10) & (cells[:, 1] < cy + 10)
+        s.target_mask[under] = 7
+        s.target[under] = s.position[under]
+        s.meta.update(workload="served", edge=edge, dt=1e-3, substeps=1, gravity=(0, 0, -9.81), wood_revs=n_wood)
+        return s, under
+    # the blade: 2 (x) x 20 (y) x 40 (z) iron REVs on the top face, lowest row 1 REV thick
+    bx, by, bz = np.meshgrid(np.arange(cx, cx + 2), np.arange(cy - 10, cy + 10), np.arange(edge, edge + 40),
+                             indexing="ij")
+    bcells = np.stack([bx.ravel(), by.ravel(), bz.ravel()], axis=1).astype(np.int32)
+    bcells = bcells[(bcells[:, 2] > edge) | (bcells[:, 0] == cx)]
+    bcells = bcells[np.lexsort((bcells[:, 0], bcells[:, 1], bcells[:, 2]))]
+    all_cells = np.concatenate([cells, bcells])
+    n = len(all_cells)
+    is_blade = np.arange(n) >= n_wood
+    mats = np.where(is_blade, 2, 1).astype(np.uint32)
+    fib = np.tile(np.array([0, 0, 1], np.float32), (n, 1))
+    fib[:n_wood] = g
+    s = S.from_cells(all_cells, mats, table, kinematic=is_blade.astype(np.uint8), fiber=fib,
+                     anisotropy=np.where(is_blade, 0.0, 1.0).astype(np.float32))
+    s.fix_voxels(np.nonzero(all_cells[:n_wood, 2] == 0)[0])
+    s.target_mask[is_blade] = 7
+    s.target[is_blade] = s.position[is_blade]
+    s.meta.update(workload="served", edge=edge, dt=1e-3, substeps=1, gravity=(0, 0, -9.81), wood_revs=n_wood)
+    return s, is_blade
 
 
 def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps: int = 100,
                max_slots: int = 256, templates: int = 16, seed: int = 77, drain: float = 60.0,
-               blade_speed: float = 1.0, hbm_fraction: float = 0.8, tolerance: float = 1e-8) -> dict:
+               blade_speed: float = 1.0, hbm_fraction: float = 0.8, tolerance: float = 1e-8,
+               blade: str = "contact") -> dict:
     rng = np.random.default_rng(seed)
-    pool = [served_scene(rng) for _ in range(templates)]
+    pool = [served_scene(rng, blade=blade) for _ in range(templates)]
+    real = blade == "contact"
     params = N.step_params(1e-3, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5,
                            gravity=(0.0, 0.0, -9.81), tolerance=tolerance, max_iterations=20000,
-                           precision=N.PRECISION_MIXED)
+                           precision=N.PRECISION_MIXED, fracture=real, contact=real)
     srv = N.Server(ctx, params, max_slots=max_slots, hbm_fraction=hbm_fraction)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * duration * 2) + 16))
     arrivals = arrivals[arrivals < duration]
@@ -84,7 +108,7 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
             time.sleep(t - now)
         scene, moving = pool[k]
         tickets.append(srv.submit(scene, steps, target_velocity=(0.0, 0.0, -blade_speed), moving=moving))
-        sizes.append(scene.n)
+        sizes.append(scene.meta["wood_revs"])
     submit_s = time.perf_counter() - t0
     results = []
     deadline = time.perf_counter() + drain
@@ -99,6 +123,7 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
     done = [r for r in results if r["status"] in (N.VX_OK, N.VX_NOT_CONVERGED)]
     return {
         "requests": len(tickets), "completed": len(done), "arrival_rate": rate, "arrival_window_s": duration,
+        "blade": blade,
         "submit_s": submit_s, "wall_s": wall, "steps_per_request": steps,
         "dof_range": [3 * min(sizes) if sizes else 0, 3 * max(sizes) if sizes else 0],
         "templates": templates, "stats": st,
