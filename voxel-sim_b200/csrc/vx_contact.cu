@@ -63,7 +63,8 @@ constexpr unsigned kUnionRetries = 1u << 16;
 constexpr uint64_t kMaxLargeVolume = 1ull << 24;  // bins one fast REV may sweep in a substep
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kScanBlock = 1024;
-constexpr double kSweepBound = 5e-4;  // metres a REV may move in a sweep before it is replayed with more pairs
+constexpr double kSweepBound = 5e-4;  // metres a REV may first move in a sweep before it is replayed with more pairs
+constexpr int kMaxAttempts = 8;       // replays of a sweep with wider bounds before every pair is stored
 
 enum : uint32_t {
     E_OK = 0,
@@ -74,7 +75,10 @@ enum : uint32_t {
 };
 
 // scalars in ContactState::scal
-enum { S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_PAIRS_LO = 8, S_PAIRS_HI = 9 };
+enum {
+    S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_PAIRS_LO = 8, S_PAIRS_HI = 9,
+    S_MOVED = 10  // a REV moved farther than its bound in the last sweep
+};
 
 // Which scene a REV belongs to. A single scene is slot 0 for every REV. In a
 // pool, REVs of free tiles, of slots not taking part in the call, and the
@@ -214,9 +218,9 @@ __device__ __forceinline__ double inverse_mass(const uint8_t* kin, const float4*
     return 1.0 / (double)param1[i].w;
 }
 
-// True when the pair can act or report a contact while each REV moves at
-// most M: its end separation within half = CELL + slop + 2M (+ a rounding
-// margin) on every axis, or, unless the starts already overlap (swept_normal
+// True when the pair can act or report a contact while its REVs move at most
+// m_i and m_j: its end separation within half = CELL + slop + m_i + m_j (+ a
+// rounding margin) on every axis, or, unless the starts already overlap (swept_normal
 // then answers nothing), its relative path from the start separation to the
 // end one meeting the box of that half-width.
 __device__ bool may_act(v3 si, v3 sj, v3 ei, v3 ej, double half) {
@@ -407,9 +411,10 @@ struct PairArgs {
     const uint32_t* ent_next;
     uint32_t mask2;
     int32_t wx, wy, wz;  // largest small extent per axis
-    const double* pos;   // current positions
-    const double* start; // swept starts
-    double half;         // pairs that cannot act within this reach are not stored
+    const double* pos;    // current positions
+    const double* start;  // swept starts
+    const double* bound;  // per REV: how far it may move in this sweep
+    bool all;             // store every pair (the last resort of a sweep)
     uint32_t* count;     // per owner: pairs (count pass) / cursor (write pass)
     const uint32_t* off;
     uint32_t* pi;
@@ -424,8 +429,8 @@ __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, 
     ++cand;
     if (local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
     ++kept;
-    if (!may_act(load3(a.start, a.n, lo), load3(a.start, a.n, hi), load3(a.pos, a.n, lo), load3(a.pos, a.n, hi),
-                 a.half))
+    if (!a.all && !may_act(load3(a.start, a.n, lo), load3(a.start, a.n, hi), load3(a.pos, a.n, lo),
+                           load3(a.pos, a.n, hi), kCell + kSlop + a.bound[lo] + a.bound[hi] + 1e-9))
         return;
     if (kWrite) {
         const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
@@ -702,11 +707,24 @@ __global__ void k_sweep(SweepArgs a) {
     if (changed) atomicOr(a.scal + S_CHANGED, 1u);
 }
 
-__global__ void k_max_move(uint32_t n, const double* __restrict__ move, unsigned long long* out) {
+// Movement bounds at the start of a sweep: REVs that cannot move keep 0.
+__global__ void k_init_bounds(uint32_t n, const uint8_t* __restrict__ kin, const uint8_t* __restrict__ tmask,
+                              double base, double* __restrict__ bound) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) bound[i] = movable(kin, tmask, i) ? base : 0.0;
+}
+
+// After a sweep: a REV that moved farther than its bound gets a wider one and
+// the sweep must be replayed (flag); the others keep theirs.
+__global__ void k_check_bounds(uint32_t n, const double* __restrict__ move, double* __restrict__ bound,
+                               uint32_t* __restrict__ flag) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double m = move[i];
-    if (m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    if (m > bound[i]) {
+        bound[i] = fmax(2.0 * m, 4.0 * bound[i]);
+        atomicOr(flag, 1u);
+    }
 }
 
 // This sweep's contacts, in pair order: key (i << 32 | j), normal code, impact.
@@ -998,7 +1016,8 @@ struct ContactState {
     Boxes box{};
     double* start = nullptr;    // [3][n] previous positions when the call began
     double* snap = nullptr;     // [6][n] positions and previous at the start of a sweep
-    double* move = nullptr;     // [n]
+    double* move = nullptr;     // [n] summed corrections of the sweep
+    double* bound = nullptr;    // [n] how far each REV may move in the sweep
     double* heat = nullptr;     // [2][n]
     double* phys = nullptr;     // [3][n]
     uint32_t* next1 = nullptr;  // [n]
@@ -1047,7 +1066,6 @@ struct ContactState {
     // [6..7] candidate count (u64); max movement (u64 bits of a double); the
     // host copies
     uint32_t* scal = nullptr;
-    unsigned long long* max_move = nullptr;
     double* heat_sum = nullptr;  // [2]
     uint32_t* h_scal = nullptr;  // pinned [32]: [0, 16) the scalars, [16, 18) max movement, [18] a count
 };
@@ -1115,6 +1133,7 @@ cudaError_t ensure_state(vx_scene* s) {
     if (e == cudaSuccess) e = alloc(c->start, 3 * n);
     if (e == cudaSuccess) e = alloc(c->snap, 6 * n);
     if (e == cudaSuccess) e = alloc(c->move, n);
+    if (e == cudaSuccess) e = alloc(c->bound, n);
     if (e == cudaSuccess) e = alloc(c->heat, 2 * n);
     if (e == cudaSuccess) e = alloc(c->phys, 3 * n);
     if (e == cudaSuccess) e = alloc(c->next1, n);
@@ -1126,7 +1145,6 @@ cudaError_t ensure_state(vx_scene* s) {
     if (e == cudaSuccess) e = alloc(c->keys1, c->table1);
     if (e == cudaSuccess) e = alloc(c->heads1, c->table1);
     if (e == cudaSuccess) e = alloc(c->scal, 16);
-    if (e == cudaSuccess) e = alloc(c->max_move, 1);
     if (e == cudaSuccess) e = alloc(c->heat_sum, 2);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_scal, 32 * sizeof(uint32_t));
     return e;
@@ -1218,8 +1236,6 @@ cudaError_t ensure_large(ContactState* c, size_t entries) {
 
 int32_t read_scalars(vx_scene* s, ContactState* c, const char* what) {
     cudaError_t e = cudaMemcpyAsync(c->h_scal, c->scal, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c->h_scal + 16, c->max_move, sizeof(unsigned long long),
-                                              cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
         set_error("%s: %s", what, cudaGetErrorString(e));
@@ -1272,13 +1288,13 @@ void contact_release(vx_scene* s) {
     if (!c) return;
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->box.slot, c->slot_contacts, c->start, c->snap, c->move, c->heat, c->phys, c->next1,
+    void* ptrs[] = {c->box.lo, c->box.hi, c->box.large, c->box.slot, c->slot_contacts, c->start, c->snap, c->move, c->bound, c->heat, c->phys, c->next1,
                     c->cnt, c->off, c->parent, c->comp_cnt, c->comp_off, c->bsum, c->keys1, c->heads1, c->keys2,
                     c->heads2, c->ent_id, c->ent_next, c->pi, c->pj, c->root,
                     c->items, c->code, c->impact, c->sw_flag, c->sw_off, c->sw_key, c->sw_cn, c->sw_cm,
                     c->sw_keep, c->sw_koff, c->rec_key[0], c->rec_key[1], c->rec_cn[0], c->rec_cn[1],
                     c->rec_cm[0], c->rec_cm[1], c->ci, c->cj, c->cn, c->cm,
-                    c->scal, c->max_move, c->heat_sum};
+                    c->scal, c->heat_sum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -1375,14 +1391,16 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
     pa.scal = c->scal;
     pa.pos = s->pos;
     pa.start = c->start;
-    // Each sweep stores only the pairs that can act in it when no REV moves
-    // more than the sweep's bound M (first kSweepBound): the lattice's two-cell
-    // neighbours never can. When a REV moves farther, the sweep is restored and
-    // replayed with the pairs of a wider bound, and after four widenings with
-    // every pair. The replay is exact at any bound.
+    // Each sweep stores only the pairs that can act in it while every REV
+    // moves at most its bound (kSweepBound for REVs that can move, 0 for the
+    // others): the lattice's two-cell neighbours never can. When a REV moves
+    // farther, its bound is widened and the sweep is restored and replayed;
+    // after kMaxAttempts tries every pair is stored. The replay is exact with
+    // any bounds.
     bool first_generation = true;
-    auto generate = [&](double half, uint32_t* out_stored) -> int32_t {
-        pa.half = half;
+    pa.bound = c->bound;
+    auto generate = [&](bool all, uint32_t* out_stored) -> int32_t {
+        pa.all = all;
         pa.pi = nullptr;
         pa.pj = nullptr;
         cudaError_t ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
@@ -1438,16 +1456,17 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         e = cudaMemcpyAsync(c->snap, s->pos, v3b, cudaMemcpyDeviceToDevice, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(c->snap + 3 * (size_t)n, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return cuda_fail(e, what);
-        double bound = kSweepBound;
+        k_init_bounds<<<grid(n), 256, 0, st>>>(n, s->kin, s->tmask, kSweepBound, c->bound);
+        c->launches += 1;
         bool changed = false;
         uint32_t stored = 0;
         for (int attempt = 0;; ++attempt) {
-            const bool all_pairs = attempt >= 4;
-            r = generate(all_pairs ? 1e300 : kCell + kSlop + 2.0 * bound + 1e-9, &stored);
+            const bool all_pairs = attempt >= kMaxAttempts;
+            r = generate(all_pairs, &stored);
             if (r != VX_OK) return r;
             e = cudaMemsetAsync(c->scal + S_CHANGED, 0, sizeof(uint32_t), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->scal + S_MOVED, 0, sizeof(uint32_t), st);
             if (e == cudaSuccess) e = cudaMemsetAsync(c->move, 0, (size_t)n * sizeof(double), st);
-            if (e == cudaSuccess) e = cudaMemsetAsync(c->max_move, 0, sizeof(unsigned long long), st);
             if (e != cudaSuccess) return cuda_fail(e, what);
             st_out.live_max = std::max(st_out.live_max, stored);
             sa.pi = c->pi;
@@ -1461,22 +1480,18 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
                 k_sweep<<<grid(n), 256, 0, st>>>(sa);
                 c->launches += 1;
             }
-            k_max_move<<<grid(n), 256, 0, st>>>(n, c->move, c->max_move);
+            k_check_bounds<<<grid(n), 256, 0, st>>>(n, c->move, c->bound, c->scal + S_MOVED);
             c->launches += 1;
             r = read_scalars(s, c, what);
             if (r != VX_OK) return r;
-            unsigned long long bits = (unsigned long long)c->h_scal[16] | ((unsigned long long)c->h_scal[17] << 32);
-            double moved = 0.0;
-            std::memcpy(&moved, &bits, sizeof moved);
             changed = c->h_scal[S_CHANGED] != 0;
-            if (all_pairs || moved <= bound) break;
-            // a REV moved farther than the bound: replay from the sweep's start
+            if (all_pairs || !c->h_scal[S_MOVED]) break;
+            // a REV moved farther than its bound: replay from the sweep's start
             st_out.redone += 1;
             e = cudaMemcpyAsync(s->pos, c->snap, v3b, cudaMemcpyDeviceToDevice, st);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(s->prev, c->snap + 3 * (size_t)n, v3b, cudaMemcpyDeviceToDevice, st);
             if (e != cudaSuccess) return cuda_fail(e, what);
-            bound = std::max(2.0 * moved, 4.0 * bound);
         }
         if (stored) {  // this sweep's contacts join the recorded ones
             k_sweep_contact_flags<<<grid(stored), 256, 0, st>>>(stored, c->code, c->sw_flag);
