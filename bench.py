@@ -344,8 +344,21 @@ def our_arm(args):
     # end to end through the C ABI with host buffers (pinned staging inside the library)
     e2e = None
     if not args.no_e2e:
-        x0 = np.ascontiguousarray(scene.position)
-        q0 = np.ascontiguousarray(scene.rotation)
+        # the step's inputs and outputs in page-locked host memory, as an engine
+        # keeps its staging buffers; the library copies them by DMA
+        torch_types = {np.float64: torch.float64, np.float32: torch.float32, np.uint8: torch.uint8}
+
+        def pinned(a, dtype):
+            t = torch.empty(np.asarray(a).size, dtype=torch_types[dtype], pin_memory=True)
+            view = t.numpy()
+            view[:] = np.asarray(a, dtype).reshape(-1)
+            return t, view
+
+        keep = [pinned(scene.position, np.float64), pinned(scene.rotation, np.float64), pinned(pred, np.float64),
+                pinned(scene.target_mask, np.uint8), pinned(scene.target, np.float64),
+                pinned(scene.loads, np.float64), pinned(np.zeros(3 * scene.n), np.float64),
+                pinned(np.zeros(3 * scene.n), np.float32)]
+        x0, q0, pred_h, mask_h, target_h, loads_h, x_out, ratio_out = [v for _, v in keep]
         e2e_ms, e2e_it = 0.0, 0
         h2d = scene.n * (24 * 4 + 32 + 1)
         d2h = scene.n * (24 + 12)
@@ -357,9 +370,9 @@ def our_arm(args):
             e0.record(ext)
             ds.set_positions(x0)
             ds.set_rotations(q0)
-            ds.set_predicted(pred)
-            ds.set_targets(scene.target_mask, scene.target)
-            ds.set_loads(scene.loads)
+            ds.set_predicted(pred_h)
+            ds.set_targets(mask_h, target_h)
+            ds.set_loads(loads_h)
             ds.fit_rotations()
             it = 0
             for p in range(passes):
@@ -367,8 +380,8 @@ def our_arm(args):
                 it += st["iterations"]
                 if p + 1 < passes:
                     ds.fit_rotations()
-            out = ds.bond_stress(with_force=False)
-            xs = ds.positions()
+            out = ds.bond_stress(with_force=False, ratio_out=ratio_out)
+            xs = ds.positions(out=x_out)
             e1.record(ext)
             e1.synchronize()
             e2e_ms += e0.elapsed_time(e1)

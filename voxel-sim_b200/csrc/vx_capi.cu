@@ -102,7 +102,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->barrier = A.take<unsigned>(4);
     s->zp32 = A.take<float>(6 * m);
     s->nbcode = A.take<uint32_t>(3 * m);
-    s->nbcode_bad = A.take<uint32_t>(1);
+    s->nbcode_bad = A.take<uint32_t>(2);  // [0] neighbour deltas out of range, [1] upload check
 }
 
 uint64_t scene_bytes(uint32_t n, uint32_t material_count) {
@@ -125,24 +125,84 @@ static int32_t cuda_fail(cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(_e, what); \
     } while (0)
 
-// AoS (n x 3) host doubles -> SoA [3][n] device doubles through the pinned stage
-static int32_t upload_vec3(vx_scene* s, double* dst, const double* src) {
-    size_t n = s->n;
-    double* tmp = s->h_stage;
-    VX_TRY(cudaStreamSynchronize(s->stream), "upload sync");  // the stage may still feed a copy
-    for (size_t i = 0; i < n; ++i)
-        for (int c = 0; c < 3; ++c) tmp[c * n + i] = src[3 * i + c];
-    VX_TRY(cudaMemcpyAsync(dst, tmp, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream), "upload");
+// AoS (n x 3) <-> SoA [3][n] on the device: the host only makes contiguous
+// copies, and one kernel reorders.
+__global__ void k_aos_to_soa(size_t n, const double* __restrict__ aos, double* __restrict__ soa) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;  // t = 3 i + c, coalesced reads
+    if (t < 3 * n) soa[(t % 3) * n + t / 3] = aos[t];
+}
+__global__ void k_soa_to_aos(size_t n, const double* __restrict__ soa, double* __restrict__ aos) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;  // t = 3 i + c, coalesced writes
+    if (t < 3 * n) aos[t] = soa[(t % 3) * n + t / 3];
+}
+// Counts the non-finite values of v[count] into *bad.
+__global__ void k_count_nonfinite(size_t count, const double* __restrict__ v, uint32_t* bad) {
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const bool nf = t < count && !isfinite(v[t]);
+    const unsigned ballot = __ballot_sync(0xffffffffu, nf);
+    if ((threadIdx.x & 31) == 0 && ballot) atomicAdd(bad, (uint32_t)__popc(ballot));
+}
+
+// Page-locked host memory (cudaMallocHost or registered) is copied by DMA
+// directly; other host memory goes through the scene's pinned stage.
+static bool is_pinned(const void* p) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+// Host bytes -> device (through the stage unless the source is pinned).
+static cudaError_t host_to_device(vx_scene* s, void* dst, const void* src, size_t bytes) {
+    if (is_pinned(src)) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->stream);
+    cudaError_t e = cudaStreamSynchronize(s->stream);  // the stage may still feed a copy
+    if (e != cudaSuccess) return e;
+    std::memcpy(s->h_stage, src, bytes);
+    return cudaMemcpyAsync(dst, s->h_stage, bytes, cudaMemcpyHostToDevice, s->stream);
+}
+// Device bytes -> host; returns after the copy has landed.
+static cudaError_t device_to_host(vx_scene* s, void* dst, const void* src, size_t bytes) {
+    if (is_pinned(dst)) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->stream);
+        return e == cudaSuccess ? cudaStreamSynchronize(s->stream) : e;
+    }
+    cudaError_t e = cudaMemcpyAsync(s->h_stage, src, bytes, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e == cudaSuccess) std::memcpy(dst, s->h_stage, bytes);
+    return e;
+}
+
+// AoS host doubles -> SoA device doubles. The transit buffer is the FP64
+// residual vector r64, which holds nothing between solves (every host call on
+// a scene runs on its stream, between solves). With check_finite, nothing is
+// written and VX_NONFINITE is returned when a value is not finite.
+static int32_t upload_vec3(vx_scene* s, double* dst, const double* src, bool check_finite = false,
+                           const char* what = "upload") {
+    const size_t n = s->n, bytes = 3 * n * sizeof(double);
+    if (n == 0) return VX_OK;
+    VX_TRY(host_to_device(s, s->r64, src, bytes), what);
+    if (check_finite) {
+        VX_TRY(cudaMemsetAsync(s->nbcode_bad + 1, 0, sizeof(uint32_t), s->stream), what);
+        k_count_nonfinite<<<(unsigned)((3 * n + 255) / 256), 256, 0, s->stream>>>(3 * n, s->r64, s->nbcode_bad + 1);
+        uint32_t bad = 0;
+        VX_TRY(device_to_host(s, &bad, s->nbcode_bad + 1, sizeof(uint32_t)), what);
+        if (bad) {
+            set_error("%s: %u non-finite values", what, bad);
+            return VX_NONFINITE;
+        }
+    }
+    k_aos_to_soa<<<(unsigned)((3 * n + 255) / 256), 256, 0, s->stream>>>(n, s->r64, dst);
+    VX_TRY(cudaGetLastError(), "upload reorder");
     VX_TRY(cudaStreamSynchronize(s->stream), "upload sync");
     return VX_OK;
 }
 static int32_t download_vec3(vx_scene* s, double* dst, const double* src) {
-    size_t n = s->n;
-    double* tmp = s->h_stage;
-    VX_TRY(cudaMemcpyAsync(tmp, src, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream), "download");
-    VX_TRY(cudaStreamSynchronize(s->stream), "download sync");
-    for (size_t i = 0; i < n; ++i)
-        for (int c = 0; c < 3; ++c) dst[3 * i + c] = tmp[c * n + i];
+    const size_t n = s->n, bytes = 3 * n * sizeof(double);
+    if (n == 0) return VX_OK;
+    k_soa_to_aos<<<(unsigned)((3 * n + 255) / 256), 256, 0, s->stream>>>(n, src, s->r64);
+    VX_TRY(cudaGetLastError(), "download reorder");
+    VX_TRY(device_to_host(s, dst, s->r64, bytes), "download");
     return VX_OK;
 }
 
@@ -463,12 +523,7 @@ int32_t vx_scene_destroy(vx_scene* s) {
 
 int32_t vx_scene_set_positions(vx_scene* s, const double* xyz) {
     VX_CHECK_SCENE(s, xyz);
-    for (size_t t = 0; t < 3 * (size_t)s->n; ++t)
-        if (!std::isfinite(xyz[t])) {
-            set_error("vx_scene_set_positions: non-finite value at %zu", t);
-            return VX_NONFINITE;
-        }
-    return upload_vec3(s, s->pos, xyz);
+    return upload_vec3(s, s->pos, xyz, true, "vx_scene_set_positions");
 }
 int32_t vx_scene_get_positions(vx_scene* s, double* xyz) {
     VX_CHECK_SCENE(s, xyz);
@@ -476,19 +531,15 @@ int32_t vx_scene_get_positions(vx_scene* s, double* xyz) {
 }
 int32_t vx_scene_set_rotations(vx_scene* s, const double* q) {
     VX_CHECK_SCENE(s, q);
-    VX_TRY(cudaStreamSynchronize(s->stream), "upload");
-    std::memcpy(s->h_stage, q, (size_t)s->n * sizeof(double4));
-    VX_TRY(cudaMemcpyAsync(s->rot, s->h_stage, (size_t)s->n * sizeof(double4), cudaMemcpyHostToDevice, s->stream),
-           "upload");
+    if (s->n == 0) return VX_OK;
+    VX_TRY(host_to_device(s, s->rot, q, (size_t)s->n * sizeof(double4)), "upload");
     VX_TRY(cudaStreamSynchronize(s->stream), "upload");
     return VX_OK;
 }
 int32_t vx_scene_get_rotations(vx_scene* s, double* q) {
     VX_CHECK_SCENE(s, q);
-    VX_TRY(cudaMemcpyAsync(s->h_stage, s->rot, (size_t)s->n * sizeof(double4), cudaMemcpyDeviceToHost, s->stream),
-           "download");
-    VX_TRY(cudaStreamSynchronize(s->stream), "download");
-    std::memcpy(q, s->h_stage, (size_t)s->n * sizeof(double4));
+    if (s->n == 0) return VX_OK;
+    VX_TRY(device_to_host(s, q, s->rot, (size_t)s->n * sizeof(double4)), "download");
     return VX_OK;
 }
 int32_t vx_scene_set_targets(vx_scene* s, const uint8_t* mask, const double* xyz) {
@@ -505,12 +556,7 @@ int32_t vx_scene_set_targets(vx_scene* s, const uint8_t* mask, const double* xyz
 }
 int32_t vx_scene_set_velocities(vx_scene* s, const double* xyz) {
     VX_CHECK_SCENE(s, xyz);
-    for (size_t t = 0; t < 3 * (size_t)s->n; ++t)
-        if (!std::isfinite(xyz[t])) {
-            set_error("vx_scene_set_velocities: non-finite value at %zu", t);
-            return VX_NONFINITE;
-        }
-    return upload_vec3(s, s->vel, xyz);
+    return upload_vec3(s, s->vel, xyz, true, "vx_scene_set_velocities");
 }
 int32_t vx_scene_get_velocities(vx_scene* s, double* xyz) {
     VX_CHECK_SCENE(s, xyz);

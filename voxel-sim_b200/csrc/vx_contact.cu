@@ -415,6 +415,7 @@ struct PairArgs {
     const double* start;  // swept starts
     const double* bound;  // per REV: how far it may move in this sweep
     bool all;             // store every pair (the last resort of a sweep)
+    bool count_pairs;     // count candidates and pairs (the call's first generation)
     uint32_t* count;     // per owner: pairs (count pass) / cursor (write pass)
     const uint32_t* off;
     uint32_t* pi;
@@ -426,12 +427,18 @@ template <bool kWrite>
 __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand, uint32_t& kept) {
     const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
     if (a.kin[lo] && a.kin[hi]) return;
-    ++cand;
-    if (local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
-    ++kept;
-    if (!a.all && !may_act(load3(a.start, a.n, lo), load3(a.start, a.n, hi), load3(a.pos, a.n, lo),
-                           load3(a.pos, a.n, hi), kCell + kSlop + a.bound[lo] + a.bound[hi] + 1e-9))
-        return;
+    auto acts = [&] {
+        return a.all || may_act(load3(a.start, a.n, lo), load3(a.start, a.n, hi), load3(a.pos, a.n, lo),
+                                load3(a.pos, a.n, hi), kCell + kSlop + a.bound[lo] + a.bound[hi] + 1e-9);
+    };
+    if (a.count_pairs) {  // every candidate through the lattice test, for the counts
+        ++cand;
+        if (local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
+        ++kept;
+        if (!acts()) return;
+    } else {  // the cheaper test first: most candidates cannot act
+        if (!acts() || local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
+    }
     if (kWrite) {
         const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
         a.pi[slot] = lo;
@@ -1401,6 +1408,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
     pa.bound = c->bound;
     auto generate = [&](bool all, uint32_t* out_stored) -> int32_t {
         pa.all = all;
+        pa.count_pairs = first_generation;
         pa.pi = nullptr;
         pa.pj = nullptr;
         cudaError_t ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);

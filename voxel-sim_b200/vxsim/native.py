@@ -349,8 +349,11 @@ class DeviceScene:
         x = self._vec(x)
         check(load().vx_scene_set_positions(self.h, _p(x, C.c_double)))
 
-    def positions(self) -> np.ndarray:
-        out = np.zeros(3 * self.n, np.float64)
+    def positions(self, out=None) -> np.ndarray:
+        """Positions (n, 3); `out` (a C-contiguous float64 array of 3n values,
+        pinned for a direct copy) receives them when given."""
+        out = np.zeros(3 * self.n, np.float64) if out is None else out
+        assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.size == 3 * self.n
         check(load().vx_scene_get_positions(self.h, _p(out, C.c_double)))
         return out.reshape(-1, 3)
 
@@ -518,9 +521,9 @@ class DeviceScene:
         check(load().vx_scene_update_velocities(self.h, len(idx), _p(idx, C.c_uint32), _p(val, C.c_double),
                                                 1 if add else 0))
 
-    def bond_stress(self, with_force=True, with_ratio=True, cap=None):
+    def bond_stress(self, with_force=True, with_ratio=True, cap=None, ratio_out=None):
         m = 3 * self.n
-        ratio = np.zeros(m, np.float32) if with_ratio else None
+        ratio = (np.zeros(m, np.float32) if ratio_out is None else ratio_out) if with_ratio else None
         force = np.zeros(3 * m, np.float32) if with_force else None
         cap = m if cap is None else cap
         near = np.zeros(max(cap, 1), np.uint32)
