@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--drain", type=float, default=60.0, help="served: seconds to wait for completions")
     ap.add_argument("--request-steps", type=int, default=100, help="served: fixed steps per request")
     ap.add_argument("--slots", type=int, default=256, help="served: resident scenes at most")
+    ap.add_argument("--lanes", type=int, default=3, help="served: pools by scene size, each with its own stream")
     ap.add_argument("--scenes", type=int, default=512, help="batched: scenes per batch")
     ap.add_argument("--fp64-sample", type=int, default=None,
                     help="batched: scenes timed in the plain FP64 single-scene form (default all)")
@@ -524,6 +525,7 @@ def served_arm(args):
     clocks = ClockSampler(local)
     clocks.start()
     out = V.run_served(ctx, rate=args.rate, duration=args.window, steps=args.request_steps, max_slots=args.slots,
+                       lanes=args.lanes,
                        drain=args.drain, tolerance=args.tolerance, seed=77 + rank)
     clk = clocks.stop()
     st = out["stats"]
@@ -538,6 +540,7 @@ def served_arm(args):
                        "arrival_rate_per_s": out["arrival_rate"], "arrival_window_s": out["arrival_window_s"],
                        "steps_per_request": out["steps_per_request"], "max_slots": args.slots,
                        "dof_range": out["dof_range"], "hbm_budget": 0.8, "blade": out["blade"],
+                       "lanes": out["lanes"],
                        "parallelism": f"replicas{world}"},
             "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"], "max_step_ms": st["max_step_ms"],
             "scene_steps_per_s": st["scene_steps"] / out["wall_s"],

@@ -515,6 +515,12 @@ typedef struct vx_server_config {
     double hbm_fraction;          /* budget used when max_revs == 0 (for example 0.8) */
     uint32_t max_slots;           /* resident scenes at most */
     vx_step_params step;          /* the step every scene runs (pass.precision VX_PRECISION_MIXED) */
+    uint32_t lanes;               /* 0 or 1: one pool. 2..4: one pool, stream and thread per size
+                                     class, so small scenes step in short rounds beside large ones */
+    uint32_t lane_max_revs[3];    /* REV bound of every lane but the last (0 = 16384, 131072,
+                                     1048576); the slots are split evenly, a lane but the last gets
+                                     room for its slots' largest scenes (at most a quarter of the
+                                     REV budget) and the last lane the rest */
 } vx_server_config;
 
 typedef struct vx_request_plan {

@@ -139,3 +139,28 @@ def test_blade_cuts_through_contact(ctx):
     assert np.any(under) and np.min(x[under, 2] - x0[under, 2]) < -0.005
     inside = wood & np.all((x[:, :2] > lo + 0.004) & (x[:, :2] < hi - 0.004), axis=1) & (x[:, 2] > edge_z + 0.005)
     assert not np.any(inside)
+
+
+def test_lanes_route_by_size_and_keep_results(ctx):
+    """Two lanes (scenes up to 2,000 REVs, and larger): every request ends with
+    the same bits as on a one-lane server, and the small scenes finish while
+    the large ones still run their own rounds."""
+    sc = scenes()
+    sizes = [s.n for s in sc]
+    assert min(sizes) <= 2000 < max(sizes), sizes
+    cap = sum(sizes) + 8192
+
+    def run(lanes):
+        srv = N.Server(ctx, step(), max_slots=8, max_revs=4 * cap, lanes=lanes, lane_max_revs=(2000, 0, 0))
+        tickets = [srv.submit(s, steps=3) for s in sc]
+        out = [srv.wait(t) for t in tickets]
+        st = srv.stats()
+        srv.close()
+        return out, st
+
+    one, _ = run(1)
+    two, st = run(2)
+    assert st["completed"] == len(sc) and st["failed"] == 0
+    for (r1, x1), (r2, x2) in zip(one, two):
+        assert r1["status"] == r2["status"] == N.VX_OK and r2["steps_done"] == 3
+        assert np.array_equal(x1, x2)

@@ -1,6 +1,13 @@
-// vx_server.cu — the served form: a host thread that keeps scenes resident in
-// one pool, admits new requests at round boundaries as slots and memory free
-// up, and steps every resident scene together (include/vxcorot.h).
+// vx_server.cu — the served form: host threads that keep scenes resident in
+// pools, admit new requests at round boundaries as slots and memory free up,
+// and step every resident scene of a pool together (include/vxcorot.h).
+//
+// With several lanes, requests are routed by size: each lane has its own pool,
+// stream and thread, and steps only scenes up to its REV bound. A round lasts
+// as long as its largest scene needs, so a small scene in its own lane runs
+// short rounds, concurrently on the GPU with the long rounds of the large
+// scenes, instead of waiting for them. A scene's result does not depend on
+// its lane (pool slots keep per-scene scalars).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -33,6 +40,7 @@ struct Request {
     std::vector<vx_material> mats;
     vx_request_plan plan{};
     int state = 0;  // 0 queued, 1 resident, 2 finished
+    uint32_t lane = 0;
     uint32_t slot = 0;
     vx_request_result res{};
     std::vector<double> final_pos;
@@ -68,18 +76,27 @@ std::vector<T> copy_of(const T* p, size_t count) {
 
 }  // namespace
 
+// One pool with its own thread; its queue and slots are guarded by the
+// server's mutex.
+struct Lane {
+    vx_pool* pool = nullptr;
+    uint64_t max_scene_revs = 0;  // largest scene routed here (the last lane: no bound)
+    uint64_t pool_revs = 0, pool_bytes = 0;
+    uint32_t max_slots = 0;
+    std::thread worker;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::vector<std::shared_ptr<Request>> slots;
+};
+
 struct vx_server {
     vx_ctx* ctx = nullptr;
     int device = 0;
-    vx_pool* pool = nullptr;
     vx_server_config cfg{};
     uint64_t pool_revs = 0, pool_bytes = 0;
-    std::thread worker;
+    std::vector<std::unique_ptr<Lane>> lanes;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     bool stop = false;
-    std::deque<std::shared_ptr<Request>> queue;
-    std::vector<std::shared_ptr<Request>> slots;
     std::unordered_map<uint64_t, std::shared_ptr<Request>> live;
     uint64_t next_ticket = 1;
     // statistics (under mu)
@@ -89,21 +106,21 @@ struct vx_server {
     std::vector<float> latency_ms;
     Clock::time_point start = Clock::now();
 
-    void run();
-    void finish(const std::shared_ptr<Request>& r, int32_t status, bool download);
+    void run(Lane& L);
+    void finish(Lane& L, const std::shared_ptr<Request>& r, int32_t status, bool download);
 };
 
 // Ends a resident request: final positions, slot freed, waiter woken.
-void vx_server::finish(const std::shared_ptr<Request>& r, int32_t status, bool download) {
+void vx_server::finish(Lane& L, const std::shared_ptr<Request>& r, int32_t status, bool download) {
     if (download && r->n) {
         r->final_pos.assign(3 * (size_t)r->n, 0.0);
-        if (vx_pool_get_positions(pool, r->slot, r->final_pos.data()) != VX_OK && status == VX_OK)
+        if (vx_pool_get_positions(L.pool, r->slot, r->final_pos.data()) != VX_OK && status == VX_OK)
             status = VX_CUDA_ERROR;
     }
-    vx_pool_remove(pool, r->slot);
+    vx_pool_remove(L.pool, r->slot);
     const Clock::time_point now = Clock::now();
     std::lock_guard<std::mutex> g(mu);
-    slots[r->slot].reset();
+    L.slots[r->slot].reset();
     if (status == VX_OK && r->res.status != VX_OK) status = r->res.status;
     r->res.status = status;
     r->res.run_s = seconds(r->admitted, now);
@@ -113,9 +130,12 @@ void vx_server::finish(const std::shared_ptr<Request>& r, int32_t status, bool d
     cv_done.notify_all();
 }
 
-void vx_server::run() {
+void vx_server::run(Lane& L) {
     cudaSetDevice(device);
-    const uint32_t S = cfg.max_slots;
+    const uint32_t S = L.max_slots;
+    vx_pool* pool = L.pool;
+    std::deque<std::shared_ptr<Request>>& queue = L.queue;
+    std::vector<std::shared_ptr<Request>>& slots = L.slots;
     std::vector<uint8_t> enabled(S);
     std::vector<double> delta(3 * (size_t)S);
     std::vector<vx_step_stats> st(S);
@@ -213,7 +233,7 @@ void vx_server::run() {
                 if (r->res.steps_done >= r->plan.steps) done.push_back(r);
             }
         }
-        for (const auto& r : done) finish(r, fatal ? rs : VX_OK, !fatal);
+        for (const auto& r : done) finish(L, r, fatal ? rs : VX_OK, !fatal);
     }
 }
 
@@ -250,20 +270,54 @@ int32_t vx_server_create(vx_ctx* ctx, const vx_server_config* cfg, vx_server** o
         revs = (uint64_t)(budget / per_rev) / 256 * 256;
         if (revs > 0x7FFFFF00ull) revs = 0x7FFFFF00ull;
     }
+    // lanes: the REV budget and the slots split by scene size
+    const uint32_t nl = std::min<uint32_t>(std::max<uint32_t>(cfg->lanes, 1u), 4u);
+    const uint64_t default_bounds[3] = {1ull << 14, 1ull << 17, 1ull << 20};
+    std::vector<uint64_t> bound(nl, ~0ull), lane_revs(nl, 0);
+    std::vector<uint32_t> lane_slots(nl, cfg->max_slots / nl);
+    lane_slots[nl - 1] += cfg->max_slots % nl;
+    uint64_t given = 0;
+    for (uint32_t k = 0; k + 1 < nl; ++k) {
+        bound[k] = cfg->lane_max_revs[k] ? cfg->lane_max_revs[k] : default_bounds[k];
+        if (lane_slots[k] == 0 || (k > 0 && bound[k] <= bound[k - 1])) {
+            vx::set_error("vx_server_create: %u lanes need at least as many slots and increasing REV bounds", nl);
+            return VX_BAD_INPUT;
+        }
+        // room for a full set of the lane's largest scenes, at most a quarter of the budget
+        lane_revs[k] = std::min<uint64_t>((uint64_t)lane_slots[k] * ((bound[k] + 255) / 256 * 256), revs / 4) / 256 * 256;
+        given += lane_revs[k];
+    }
+    if (given >= revs) {
+        vx::set_error("vx_server_create: a pool of %llu REVs is too small for %u lanes", (unsigned long long)revs, nl);
+        return VX_BAD_INPUT;
+    }
+    lane_revs[nl - 1] = (revs - given) / 256 * 256;
     vx_server* s = new (std::nothrow) vx_server();
     if (!s) return VX_OOM;
     s->ctx = ctx;
     s->device = ctx->device;
     s->cfg = *cfg;
-    s->pool_revs = revs;
-    s->pool_bytes = vx_pool_footprint_bytes(revs, cfg->max_slots);
-    int32_t r = vx_pool_create(ctx, revs, cfg->max_slots, &s->pool);
-    if (r != VX_OK) {
-        delete s;
-        return r;
+    for (uint32_t k = 0; k < nl; ++k) {
+        auto L = std::make_unique<Lane>();
+        L->max_scene_revs = bound[k];
+        L->max_slots = lane_slots[k];
+        L->pool_revs = lane_revs[k];
+        L->pool_bytes = vx_pool_footprint_bytes(lane_revs[k], lane_slots[k]);
+        int32_t r = vx_pool_create(ctx, lane_revs[k], lane_slots[k], &L->pool);
+        if (r != VX_OK) {
+            for (auto& M : s->lanes) vx_pool_destroy(M->pool);
+            delete s;
+            return r;
+        }
+        L->slots.assign(lane_slots[k], nullptr);
+        s->pool_revs += L->pool_revs;
+        s->pool_bytes += L->pool_bytes;
+        s->lanes.push_back(std::move(L));
     }
-    s->slots.assign(cfg->max_slots, nullptr);
-    s->worker = std::thread([s] { s->run(); });
+    for (auto& L : s->lanes) {
+        Lane* lp = L.get();
+        L->worker = std::thread([s, lp] { s->run(*lp); });
+    }
     *out = s;
     return VX_OK;
 }
@@ -281,10 +335,12 @@ int32_t vx_server_submit(vx_server* s, const vx_scene_desc* d, const uint8_t* ma
             vx::set_error("vx_server_submit: non-finite target velocity");
             return VX_NONFINITE;
         }
+    uint32_t lane = 0;
+    while (lane + 1 < s->lanes.size() && d->n > s->lanes[lane]->max_scene_revs) ++lane;
     const uint64_t need = (d->n + 255ull) / 256 * 256;
-    if (need > s->pool_revs) {
-        vx::set_error("vx_server_submit: scene of %u REVs exceeds the pool capacity of %llu", d->n,
-                      (unsigned long long)s->pool_revs);
+    if (need > s->lanes[lane]->pool_revs) {
+        vx::set_error("vx_server_submit: scene of %u REVs exceeds the capacity of its lane's pool, %llu REVs", d->n,
+                      (unsigned long long)s->lanes[lane]->pool_revs);
         return VX_OOM;
     }
     auto r = std::make_shared<Request>();
@@ -308,13 +364,14 @@ int32_t vx_server_submit(vx_server* s, const vx_scene_desc* d, const uint8_t* ma
     r->tmask = copy_of(mask, n);
     r->target = copy_of(target, 3 * n);
     r->plan = *plan;
+    r->lane = lane;
     r->res.n = d->n;
     r->res.status = VX_OK;
     r->submitted = Clock::now();
     std::lock_guard<std::mutex> g(s->mu);
     r->ticket = s->next_ticket++;
     s->live[r->ticket] = r;
-    s->queue.push_back(r);
+    s->lanes[lane]->queue.push_back(r);
     ++s->submitted;
     *out_ticket = r->ticket;
     s->cv_work.notify_all();
@@ -353,9 +410,11 @@ int32_t vx_server_get_stats(vx_server* s, vx_server_stats* out) {
     o.submitted = s->submitted;
     o.completed = s->completed;
     o.failed = s->failed;
-    o.resident = (uint32_t)std::count_if(s->slots.begin(), s->slots.end(),
-                                         [](const std::shared_ptr<Request>& p) { return (bool)p; });
-    o.queued = (uint32_t)s->queue.size();
+    for (const auto& L : s->lanes) {
+        o.resident += (uint32_t)std::count_if(L->slots.begin(), L->slots.end(),
+                                              [](const std::shared_ptr<Request>& p) { return (bool)p; });
+        o.queued += (uint32_t)L->queue.size();
+    }
     o.rounds = s->rounds;
     o.scene_steps = s->scene_steps;
     o.solves = s->solves;
@@ -387,8 +446,10 @@ int32_t vx_server_destroy(vx_server* s) {
         s->stop = true;
         s->cv_work.notify_all();
     }
-    if (s->worker.joinable()) s->worker.join();
-    if (s->pool) vx_pool_destroy(s->pool);
+    for (auto& L : s->lanes)
+        if (L->worker.joinable()) L->worker.join();
+    for (auto& L : s->lanes)
+        if (L->pool) vx_pool_destroy(L->pool);
     delete s;
     return VX_OK;
 }

@@ -136,7 +136,7 @@ class VxTuneResult(C.Structure):
 
 class VxServerConfig(C.Structure):
     _fields_ = [("max_revs", C.c_uint64), ("hbm_fraction", C.c_double), ("max_slots", C.c_uint32),
-                ("step", VxStepParams)]
+                ("step", VxStepParams), ("lanes", C.c_uint32), ("lane_max_revs", C.c_uint32 * 3)]
 
 
 class VxRequestPlan(C.Structure):
@@ -760,15 +760,16 @@ class DevicePool:
 
 
 class Server:
-    """The served form (vx_server): a native thread keeps scenes resident in one
-    pool, admits submissions at round boundaries and steps all resident scenes
-    together."""
+    """The served form (vx_server): native threads keep scenes resident in
+    pools, admit submissions at round boundaries and step all resident scenes
+    of a pool together. With lanes > 1 the scenes are routed by size to one
+    pool per lane (REV bounds lane_max_revs, 0 = the defaults)."""
 
     def __init__(self, ctx: Context, step: VxStepParams, max_slots: int = 64, max_revs: int = 0,
-                 hbm_fraction: float = 0.8):
+                 hbm_fraction: float = 0.8, lanes: int = 1, lane_max_revs=(0, 0, 0)):
         self.ctx = ctx
         self.h = C.c_void_p()
-        cfg = VxServerConfig(max_revs, hbm_fraction, max_slots, step)
+        cfg = VxServerConfig(max_revs, hbm_fraction, max_slots, step, lanes, (C.c_uint32 * 3)(*lane_max_revs))
         check(load().vx_server_create(ctx.h, C.byref(cfg), C.byref(self.h)))
         self.n = {}
 

@@ -8,8 +8,10 @@ targets advance at 1 m/s into the block; its lowest row is one REV thick
 (the bevel). The blade pushes the wood through the contact stage of the step
 (collision::project and the contact velocities), and the wood's bonds go
 through the fracture stage. Each request runs 100 fixed steps of 1 ms with
-its state resident on the device; admission is capped by the pool, sized at
-80% of the device memory together with the contact buffers.
+its state resident on the device; admission is capped by the pools, sized at
+80% of the device memory together with the contact buffers. The server runs
+three lanes by scene size (up to 16,384 REVs, up to 131,072, larger), each
+with its own pool, stream and thread.
 
 `blade="targets"` builds the earlier stand-in instead: no blade REVs, the
 wood REVs under the blade's edge are targeted and driven at the blade speed.
@@ -89,14 +91,14 @@ def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6, blade: str = "co
 def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps: int = 100,
                max_slots: int = 256, templates: int = 16, seed: int = 77, drain: float = 60.0,
                blade_speed: float = 1.0, hbm_fraction: float = 0.8, tolerance: float = 1e-8,
-               blade: str = "contact") -> dict:
+               blade: str = "contact", lanes: int = 3) -> dict:
     rng = np.random.default_rng(seed)
     pool = [served_scene(rng, blade=blade) for _ in range(templates)]
     real = blade == "contact"
     params = N.step_params(1e-3, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5,
                            gravity=(0.0, 0.0, -9.81), tolerance=tolerance, max_iterations=20000,
                            precision=N.PRECISION_MIXED, fracture=real, contact=real)
-    srv = N.Server(ctx, params, max_slots=max_slots, hbm_fraction=hbm_fraction)
+    srv = N.Server(ctx, params, max_slots=max_slots, hbm_fraction=hbm_fraction, lanes=lanes)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * duration * 2) + 16))
     arrivals = arrivals[arrivals < duration]
     picks = rng.integers(0, templates, size=len(arrivals))
@@ -123,7 +125,7 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
     done = [r for r in results if r["status"] in (N.VX_OK, N.VX_NOT_CONVERGED)]
     return {
         "requests": len(tickets), "completed": len(done), "arrival_rate": rate, "arrival_window_s": duration,
-        "blade": blade,
+        "blade": blade, "lanes": lanes,
         "submit_s": submit_s, "wall_s": wall, "steps_per_request": steps,
         "dof_range": [3 * min(sizes) if sizes else 0, 3 * max(sizes) if sizes else 0],
         "templates": templates, "stats": st,
