@@ -62,6 +62,7 @@ int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restituti
                         vx_contact_heat* out);
 uint32_t contact_count(const vx_scene* s);
 uint64_t contact_state_bytes(uint32_t n);
+int32_t pool_stream_priority(vx_pool* p, int priority);
 void contact_release(vx_scene* s);
 cudaError_t launch_rest_positions(vx_scene* s);
 cudaError_t launch_rest_range(vx_scene* s, size_t first, size_t count);

@@ -519,6 +519,24 @@ int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint
 
 using namespace vx;
 
+namespace vx {
+// Replaces an idle pool's stream by one of the given priority (lower numbers
+// run first when the GPU is shared). Only before the pool captures graphs.
+int32_t pool_stream_priority(vx_pool* p, int priority) {
+    cudaSetDevice(p->s.device);
+    cudaStream_t fresh = nullptr;
+    cudaError_t e = cudaStreamSynchronize(p->s.stream);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&fresh, cudaStreamNonBlocking, priority);
+    if (e != cudaSuccess) {
+        set_error("pool stream priority: %s", cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    cudaStreamDestroy(p->s.stream);
+    p->s.stream = fresh;
+    return VX_OK;
+}
+}  // namespace vx
+
 extern "C" {
 
 uint64_t vx_pool_footprint_bytes(uint64_t max_revs, uint32_t max_slots) {

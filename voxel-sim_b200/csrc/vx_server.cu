@@ -6,8 +6,9 @@
 // stream and thread, and steps only scenes up to its REV bound. A round lasts
 // as long as its largest scene needs, so a small scene in its own lane runs
 // short rounds, concurrently on the GPU with the long rounds of the large
-// scenes, instead of waiting for them. A scene's result does not depend on
-// its lane (pool slots keep per-scene scalars).
+// scenes, instead of waiting for them; the lanes of smaller scenes get higher
+// stream priorities. A scene's result does not depend on its lane (pool slots
+// keep per-scene scalars).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -304,6 +305,14 @@ int32_t vx_server_create(vx_ctx* ctx, const vx_server_config* cfg, vx_server** o
         L->pool_revs = lane_revs[k];
         L->pool_bytes = vx_pool_footprint_bytes(lane_revs[k], lane_slots[k]);
         int32_t r = vx_pool_create(ctx, lane_revs[k], lane_slots[k], &L->pool);
+        if (r == VX_OK && nl > 1) {
+            // the lane of the smallest scenes runs first when the lanes share the GPU
+            int least = 0, greatest = 0;
+            cudaDeviceGetStreamPriorityRange(&least, &greatest);
+            const int prio = std::max(greatest, std::min(least, greatest + (int)k * (least - greatest) / (int)(nl - 1)));
+            r = vx::pool_stream_priority(L->pool, prio);
+            if (r != VX_OK) vx_pool_destroy(L->pool);
+        }
         if (r != VX_OK) {
             for (auto& M : s->lanes) vx_pool_destroy(M->pool);
             delete s;
