@@ -338,9 +338,9 @@ typedef struct vx_contact_stats {
     uint32_t contacts;
     uint32_t sweeps;
     uint32_t live_max;    /* most pairs replayed in one sweep */
-    uint32_t redone;      /* sweeps replayed because a REV moved farther than the bound */
+    uint32_t redone;      /* sweeps replayed because a REV moved farther than its bound */
     uint32_t launches;    /* kernels launched by the call */
-    uint64_t stored;      /* pairs kept for the sweeps: those that can act within them */
+    uint64_t stored;      /* most pairs stored for one sweep: those that can act in it */
 } vx_contact_stats;
 typedef struct vx_contact_heat {
     double restitution;  /* J, kinetic loss of the normal impulses */
