@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--edge", type=int, default=None)
     ap.add_argument("--passes", type=int, default=None)
     ap.add_argument("--tolerance", type=float, default=1e-8)
+    ap.add_argument("--inner-tolerance", type=float, default=0.0,
+                    help="relative tolerance of each FP32 inner solve (0 = the library's default)")
     ap.add_argument("--max-iterations", type=int, default=50000)
     ap.add_argument("--cpu-iterations", type=int, default=40, help="PCG iterations per CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -262,7 +264,8 @@ def our_arm(args):
         launches = 1
         worst = 0.0
         for p in range(passes):
-            st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision)
+            st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision,
+                                      inner_tolerance=args.inner_tolerance)
             it += st["iterations"]
             launches += st["kernel_launches"]
             worst = max(worst, st["true_residual"])
@@ -377,7 +380,8 @@ def our_arm(args):
             ds.fit_rotations()
             it = 0
             for p in range(passes):
-                st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision)
+                st = ds.corotational_pass(h, args.tolerance, args.max_iterations, precision=precision,
+                                      inner_tolerance=args.inner_tolerance)
                 it += st["iterations"]
                 if p + 1 < passes:
                     ds.fit_rotations()
