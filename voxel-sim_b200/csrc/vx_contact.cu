@@ -77,8 +77,13 @@ enum : uint32_t {
 // scalars in ContactState::scal
 enum {
     S_ERR = 0, S_EXT = 1, S_LARGE = 4, S_CHANGED = 5, S_CAND_LO = 6, S_CAND_HI = 7, S_PAIRS_LO = 8, S_PAIRS_HI = 9,
-    S_MOVED = 10  // a REV moved farther than its bound in the last sweep
+    S_MOVED = 10,     // a REV moved farther than its bound in the last sweep
+    S_CMIN = 11,      // [3] smallest small-box corner per axis, biased by kCornerBias
+    S_CMAX = 14,      // [3] largest small-box corner per axis, biased
+    kScalars = 24,    // device words; the host copy holds them and, from kHostCount, counts
+    kHostCount = 28
 };
+constexpr int32_t kCornerBias = 1 << 30;
 
 // Which scene a REV belongs to. A single scene is slot 0 for every REV. In a
 // pool, REVs of free tiles, of slots not taking part in the call, and the
@@ -336,8 +341,32 @@ __global__ void k_boxes(uint32_t n, const double* __restrict__ pos, const double
     if (large) {
         atomicAdd(scal + S_LARGE, 1u);
     } else {
-        for (int t = 0; t < 3; ++t) atomicMax(scal + S_EXT + t, (uint32_t)ext[t]);
+        for (int t = 0; t < 3; ++t) {
+            atomicMax(scal + S_EXT + t, (uint32_t)ext[t]);
+            const uint32_t corner = (uint32_t)(b.lo[(size_t)t * n + i] + kCornerBias);
+            atomicMin(scal + S_CMIN + t, corner);
+            atomicMax(scal + S_CMAX + t, corner);
+        }
     }
+}
+
+// The corner grid of a single scene: when the small boxes' corners fill a
+// compact box, chains hang off a dense array indexed by the corner itself.
+struct CornerGrid {
+    uint32_t* heads;   // [nx * ny * nz], null: the hash is used
+    int32_t x0, y0, z0;
+    uint32_t nx, ny, nz;
+};
+__device__ __forceinline__ uint32_t grid_cell(const CornerGrid& g, int32_t x, int32_t y, int32_t z) {
+    const uint32_t dx = (uint32_t)(x - g.x0), dy = (uint32_t)(y - g.y0), dz = (uint32_t)(z - g.z0);
+    if (dx >= g.nx || dy >= g.ny || dz >= g.nz) return VX_EMPTY_U32;  // also catches x < x0 (wraps)
+    return dx + g.nx * (dy + g.ny * dz);
+}
+__global__ void k_insert_corners_dense(uint32_t n, Boxes b, CornerGrid g, uint32_t* next) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || b.large[i]) return;
+    const uint32_t cell = grid_cell(g, b.lo[i], b.lo[(size_t)n + i], b.lo[2 * (size_t)n + i]);
+    next[i] = atomicExch(g.heads + cell, i);  // every small corner lies inside the grid
 }
 
 // Small boxes: chain REVs by box corner.
@@ -401,10 +430,11 @@ struct PairArgs {
     const float* rest;
     const uint32_t* nbr;
     const uint32_t* rev;
-    const unsigned long long* keys1;  // corner table
+    const unsigned long long* keys1;  // corner table (when grid.heads is null)
     const uint32_t* heads1;
     const uint32_t* next1;
     uint32_t mask1;
+    CornerGrid grid;                  // dense corner grid of a single scene
     const unsigned long long* keys2;  // large-box table (mask2 = 0: none)
     const uint32_t* heads2;
     const uint32_t* ent_id;
@@ -473,9 +503,17 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
         for (int32_t z = lo[2] - (w[2] - 1); z <= hi[2]; ++z)
             for (int32_t y = lo[1] - (w[1] - 1); y <= hi[1]; ++y)
                 for (int32_t x = lo[0] - (w[0] - 1); x <= hi[0]; ++x) {
-                    const uint32_t hs = table_find(a.keys1, a.mask1, bin_key(slot, x, y, z, bits));
-                    if (hs == VX_EMPTY_U32) continue;
-                    for (uint32_t j = a.heads1[hs]; j != VX_EMPTY_U32; j = a.next1[j]) {
+                    uint32_t head;
+                    if (a.grid.heads) {
+                        const uint32_t cell = grid_cell(a.grid, x, y, z);
+                        if (cell == VX_EMPTY_U32) continue;
+                        head = a.grid.heads[cell];
+                    } else {
+                        const uint32_t hs = table_find(a.keys1, a.mask1, bin_key(slot, x, y, z, bits));
+                        if (hs == VX_EMPTY_U32) continue;
+                        head = a.heads1[hs];
+                    }
+                    for (uint32_t j = head; j != VX_EMPTY_U32; j = a.next1[j]) {
                         if (j <= i) continue;
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
@@ -1034,6 +1072,8 @@ struct ContactState {
     uint32_t* comp_cnt = nullptr;  // [n + 1]
     uint32_t* comp_off = nullptr;  // [n + 1]
     uint32_t* bsum = nullptr;      // scan block sums
+    uint32_t* grid_heads = nullptr;  // dense corner grid of a single scene
+    size_t grid_cap = 0;
     size_t bsum_cap = 0;
     unsigned long long* keys1 = nullptr;
     uint32_t* heads1 = nullptr;
@@ -1151,7 +1191,7 @@ cudaError_t ensure_state(vx_scene* s) {
     if (e == cudaSuccess) e = alloc(c->comp_off, n + 1);
     if (e == cudaSuccess) e = alloc(c->keys1, c->table1);
     if (e == cudaSuccess) e = alloc(c->heads1, c->table1);
-    if (e == cudaSuccess) e = alloc(c->scal, 16);
+    if (e == cudaSuccess) e = alloc(c->scal, kScalars);
     if (e == cudaSuccess) e = alloc(c->heat_sum, 2);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_scal, 32 * sizeof(uint32_t));
     return e;
@@ -1242,7 +1282,7 @@ cudaError_t ensure_large(ContactState* c, size_t entries) {
 }
 
 int32_t read_scalars(vx_scene* s, ContactState* c, const char* what) {
-    cudaError_t e = cudaMemcpyAsync(c->h_scal, c->scal, 16 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    cudaError_t e = cudaMemcpyAsync(c->h_scal, c->scal, kScalars * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
         set_error("%s: %s", what, cudaGetErrorString(e));
@@ -1301,7 +1341,7 @@ void contact_release(vx_scene* s) {
                     c->items, c->code, c->impact, c->sw_flag, c->sw_off, c->sw_key, c->sw_cn, c->sw_cm,
                     c->sw_keep, c->sw_koff, c->rec_key[0], c->rec_key[1], c->rec_cn[0], c->rec_cn[1],
                     c->rec_cm[0], c->rec_cm[1], c->ci, c->cj, c->cn, c->cm,
-                    c->scal, c->heat_sum};
+                    c->scal, c->heat_sum, c->grid_heads};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -1341,15 +1381,41 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
     c->box.bits = pooled ? kPoolBits : kSceneBits;
     const size_t v3b = 3 * (size_t)n * sizeof(double);
     e = cudaMemcpyAsync(c->start, s->prev, v3b, cudaMemcpyDeviceToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->keys1, 0xFF, (size_t)c->table1 * sizeof(unsigned long long), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->heads1, 0xFF, (size_t)c->table1 * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, kScalars * sizeof(uint32_t), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scal + S_CMIN, 0xFF, 3 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return cuda_fail(e, what);
     k_boxes<<<grid(n), 256, 0, st>>>(n, s->pos, c->start, c->box, filter, c->scal);
     c->launches += 1;
-    k_insert_corners<<<grid(n), 256, 0, st>>>(n, c->box, c->keys1, c->heads1, c->next1, c->table1 - 1, c->scal);
-    c->launches += 1;
     int32_t r = read_scalars(s, c, what);
+    if (r != VX_OK) return r;
+    // Corners of a single scene that fill a compact box go into a dense grid;
+    // the others (pools, sparse scenes) into the hash.
+    CornerGrid cgrid{};
+    uint64_t cells = 0;
+    if (!pooled && c->h_scal[S_CMIN] <= c->h_scal[S_CMAX]) {
+        cells = 1;
+        for (int t = 0; t < 3; ++t) cells *= (uint64_t)(c->h_scal[S_CMAX + t] - c->h_scal[S_CMIN + t]) + 1;
+    }
+    if (cells && cells <= 8ull * n + 4096 && cells < (1ull << 31)) {  // 32-bit cell indices
+        e = grow(c->grid_heads, c->grid_cap, cells);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->grid_heads, 0xFF, cells * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        cgrid.heads = c->grid_heads;
+        cgrid.x0 = (int32_t)(c->h_scal[S_CMIN] - (uint32_t)kCornerBias);
+        cgrid.y0 = (int32_t)(c->h_scal[S_CMIN + 1] - (uint32_t)kCornerBias);
+        cgrid.z0 = (int32_t)(c->h_scal[S_CMIN + 2] - (uint32_t)kCornerBias);
+        cgrid.nx = c->h_scal[S_CMAX] - c->h_scal[S_CMIN] + 1;
+        cgrid.ny = c->h_scal[S_CMAX + 1] - c->h_scal[S_CMIN + 1] + 1;
+        cgrid.nz = c->h_scal[S_CMAX + 2] - c->h_scal[S_CMIN + 2] + 1;
+        k_insert_corners_dense<<<grid(n), 256, 0, st>>>(n, c->box, cgrid, c->next1);
+    } else {
+        e = cudaMemsetAsync(c->keys1, 0xFF, (size_t)c->table1 * sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->heads1, 0xFF, (size_t)c->table1 * sizeof(uint32_t), st);
+        if (e != cudaSuccess) return cuda_fail(e, what);
+        k_insert_corners<<<grid(n), 256, 0, st>>>(n, c->box, c->keys1, c->heads1, c->next1, c->table1 - 1, c->scal);
+    }
+    c->launches += 1;
+    r = read_scalars(s, c, what);
     if (r != VX_OK) return r;
     const uint32_t large = c->h_scal[S_LARGE];
     uint32_t mask2 = 0;
@@ -1359,12 +1425,12 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         e = scan(c, st, c->cnt, c->off, n);
         uint32_t entries = 0;
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            e = cudaMemcpyAsync(&c->h_scal[kHostCount], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return cuda_fail(e, what);
         r = read_scalars(s, c, what);
         if (r != VX_OK) return r;
-        entries = c->h_scal[18];
+        entries = c->h_scal[kHostCount];
         e = ensure_large(c, entries);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->keys2, 0xFF, (size_t)c->table2 * sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->heads2, 0xFF, (size_t)c->table2 * sizeof(uint32_t), st);
@@ -1385,6 +1451,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
     pa.heads1 = c->heads1;
     pa.next1 = c->next1;
     pa.mask1 = c->table1 - 1;
+    pa.grid = cgrid;
     pa.keys2 = c->keys2;
     pa.heads2 = c->heads2;
     pa.ent_id = c->ent_id;
@@ -1418,11 +1485,11 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         c->launches += 1;
         ge = scan(c, st, c->cnt, c->off, n);
         if (ge == cudaSuccess)
-            ge = cudaMemcpyAsync(&c->h_scal[18], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            ge = cudaMemcpyAsync(&c->h_scal[kHostCount], c->off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (ge != cudaSuccess) return cuda_fail(ge, what);
         int32_t gr = read_scalars(s, c, what);
         if (gr != VX_OK) return gr;
-        const uint32_t stored = c->h_scal[18];
+        const uint32_t stored = c->h_scal[kHostCount];
         if (first_generation) {  // the candidate and pair counts do not depend on the bound
             st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
             st_out.pairs = (uint64_t)c->h_scal[S_PAIRS_LO] | ((uint64_t)c->h_scal[S_PAIRS_HI] << 32);
@@ -1506,10 +1573,10 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
             c->launches += 1;
             e = scan(c, st, c->sw_flag, c->sw_off, stored);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(&c->h_scal[18], c->sw_off + stored, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+                e = cudaMemcpyAsync(&c->h_scal[kHostCount], c->sw_off + stored, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return cuda_fail(e, what);
-            const uint32_t nb = c->h_scal[18];
+            const uint32_t nb = c->h_scal[kHostCount];
             if (nb) {
                 e = ensure_contacts(c, std::max<size_t>(nb, recorded));
                 if (e == cudaSuccess) e = ensure_recorded(c, 1 - cur, (size_t)recorded + nb);
@@ -1523,7 +1590,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
                 c->launches += 2;
                 e = scan(c, st, c->sw_keep, c->sw_koff, nb);
                 if (e == cudaSuccess)
-                    e = cudaMemcpyAsync(&c->h_scal[19], c->sw_koff + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+                    e = cudaMemcpyAsync(&c->h_scal[kHostCount + 1], c->sw_koff + nb, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
                 if (e != cudaSuccess) return cuda_fail(e, what);
                 k_merge_recorded<<<grid((size_t)recorded + nb), 256, 0, st>>>(
                     recorded, c->rec_key[cur], c->rec_cn[cur], c->rec_cm[cur], nb, c->sw_key, c->sw_cn, c->sw_cm,
@@ -1531,7 +1598,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
                 c->launches += 1;
                 e = cudaStreamSynchronize(st);
                 if (e != cudaSuccess) return cuda_fail(e, what);
-                recorded += c->h_scal[19];
+                recorded += c->h_scal[kHostCount + 1];
                 cur = 1 - cur;
             }
         }
@@ -1584,7 +1651,7 @@ int32_t contact_resolve(vx_scene* s, const double* pre_contact, double restituti
         if (e != cudaSuccess) return cuda_fail(e, what);
         const size_t v3b = 3 * (size_t)n * sizeof(double);
         e = cudaMemcpyAsync(c->phys, pre_contact ? pre_contact : s->vel, v3b, cudaMemcpyDeviceToDevice, st);
-        if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, 16 * sizeof(uint32_t), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->scal, 0, kScalars * sizeof(uint32_t), st);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->heat, 0, 2 * (size_t)n * sizeof(double), st);
         if (e == cudaSuccess) e = components(s, c, count, nullptr, c->ci, c->cj, c->items);
         if (e != cudaSuccess) return cuda_fail(e, what);
