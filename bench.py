@@ -613,17 +613,27 @@ def contact_arm(args):
         launches += stats["launches"]
     clk = clocks.stop()
     ms = total_ms / args.steps
-    # end to end: host positions in, projection, contacts and positions out
+    # end to end: host positions and previous positions in (page-locked), the
+    # projection, contacts and positions out
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        v = t.numpy()
+        v[:] = a.reshape(-1)
+        return t, v
+
+    keep = [pinned(pos), pinned(prev), pinned(np.zeros(pos.size))]
+    pos_h, prev_h, out_h = (v for _, v in keep)
     e2e_ms = 0.0
     reps = max(1, min(args.steps, 3))
     for k in range(reps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(ext)
-        reset()
+        ds.set_positions(pos_h)
+        ds.set_previous(prev_h)
         ds.contact_project()
         c = ds.contacts()
-        x = ds.positions()
+        x = ds.positions(out=out_h)
         e1.record(ext)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)

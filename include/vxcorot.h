@@ -332,6 +332,9 @@ int32_t vx_scene_get_bond_state(vx_scene* scene, float* plastic_strain, float* d
  * rest positions that decide the intact-lattice pairs are the positions the
  * scene was created with.
  */
+/* Previous positions of every REV, xyz[3n] (AoS): the swept starts of the
+   next contact projection. A page-locked buffer is copied directly. */
+int32_t vx_scene_set_previous(vx_scene* scene, const double* xyz);
 typedef struct vx_contact_stats {
     uint64_t candidates;  /* pairs whose swept boxes share a bin, one REV not kinematic */
     uint64_t pairs;       /* after the intact-lattice filter */

@@ -81,6 +81,7 @@ def test_shim_argument_checks_need_no_device(lib):
 def test_null_handles_are_rejected(lib):
     assert lib.vx_corotational_pass(None, None, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_set_positions(None, None) == N.VX_BAD_INPUT
+    assert lib.vx_scene_set_previous(None, None) == N.VX_BAD_INPUT
     assert lib.vx_ctx_create(0, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_step(None, None, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_update_velocities(None, 0, None, None, 0) == N.VX_BAD_INPUT

@@ -60,6 +60,21 @@ def _check_project(ctx, s, pos, prev, tmask=None):
     return d, st, oc
 
 
+def test_set_previous_writes_every_rev(ctx):
+    s = S.from_cells(S.grid_cells(4, 3, 2), M.component_id("iron"), M.table())
+    rng = np.random.default_rng(3)
+    prev = s.position + rng.normal(0, 1e-3, s.position.shape)
+    d = N.DeviceScene(ctx, s)
+    d.set_previous(prev)
+    assert np.array_equal(d.read_field(N.FIELD_PREVIOUS), prev)
+    assert np.array_equal(d.positions(), s.position)
+    bad = prev.copy()
+    bad[5, 1] = np.nan
+    with pytest.raises(N.VxError):
+        d.set_previous(bad)
+    d.close()
+
+
 def test_rotated_continuum_has_no_internal_contacts(ctx):
     s = S.scene_new((3, 3, 3))
     c, sn = math.cos(0.37), math.sin(0.37)
@@ -114,6 +129,16 @@ def test_rubble_projection_matches_the_oracle(ctx, seed):
     s, pos, prev = _rubble(seed)
     d, st, oc = _check_project(ctx, s, pos, prev)
     assert st["contacts"] > 50 and st["sweeps"] >= 2
+    d.close()
+
+
+def test_staging_overflow_writes_in_a_second_pass(ctx):
+    # an unbonded 14^3 pile stores about 13 pairs per REV, more than the
+    # initial staging list (n / 4 + 4096): the first generation writes its pairs
+    # in a second pass, later ones fit the grown list
+    s, pos, prev = _rubble(5, n_side=14, jitter=0.2, speed=0.1)
+    d, st, oc = _check_project(ctx, s, pos, prev)
+    assert st["stored"] > s.n // 4 + 4096 and st["sweeps"] >= 2
     d.close()
 
 

@@ -525,6 +525,10 @@ int32_t vx_scene_set_positions(vx_scene* s, const double* xyz) {
     VX_CHECK_SCENE(s, xyz);
     return upload_vec3(s, s->pos, xyz, true, "vx_scene_set_positions");
 }
+int32_t vx_scene_set_previous(vx_scene* s, const double* xyz) {
+    VX_CHECK_SCENE(s, xyz);
+    return upload_vec3(s, s->prev, xyz, true, "vx_scene_set_previous");
+}
 int32_t vx_scene_get_positions(vx_scene* s, double* xyz) {
     VX_CHECK_SCENE(s, xyz);
     return download_vec3(s, xyz, s->pos);

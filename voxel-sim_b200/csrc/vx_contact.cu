@@ -80,6 +80,7 @@ enum {
     S_MOVED = 10,     // a REV moved farther than its bound in the last sweep
     S_CMIN = 11,      // [3] smallest small-box corner per axis, biased by kCornerBias
     S_CMAX = 14,      // [3] largest small-box corner per axis, biased
+    S_STAGE = 17,     // pairs appended to the staging list by one generation
     kScalars = 24,    // device words; the host copy holds them and, from kHostCount, counts
     kHostCount = 28
 };
@@ -446,14 +447,21 @@ struct PairArgs {
     const double* bound;  // per REV: how far it may move in this sweep
     bool all;             // store every pair (the last resort of a sweep)
     bool count_pairs;     // count candidates and pairs (the call's first generation)
-    uint32_t* count;     // per owner: pairs (count pass) / cursor (write pass)
+    uint32_t* count;     // per owner: pairs (count and append passes) / cursor (write pass)
+    uint2* stage;         // append pass: (owner, partner) of every stored pair, in no order
+    uint32_t stage_cap;
     const uint32_t* off;
     uint32_t* pi;
     uint32_t* pj;
     uint32_t* scal;
 };
 
-template <bool kWrite>
+// k_pairs passes: count each owner's stored pairs and append them to the
+// staging list; or, when that list overflowed, write them into the owners'
+// segments in a second pass.
+enum { kAppendPass = 0, kWritePass = 1 };
+
+template <int kMode>
 __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand, uint32_t& kept) {
     const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
     if (a.kin[lo] && a.kin[hi]) return;
@@ -469,12 +477,23 @@ __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, 
     } else {  // the cheaper test first: most candidates cannot act
         if (!acts() || local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
     }
-    if (kWrite) {
+    if (kMode == kWritePass) {
         const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
         a.pi[slot] = lo;
         a.pj[slot] = hi;
-    } else {
-        atomicAdd(a.count + lo, 1u);
+        return;
+    }
+    atomicAdd(a.count + lo, 1u);
+    if (kMode == kAppendPass) {
+        // one atomic per group of lanes emitting together
+        const unsigned act = __activemask();
+        const unsigned lane = threadIdx.x & 31;
+        const int leader = __ffs(act) - 1;
+        uint32_t base = 0;
+        if ((int)lane == leader) base = atomicAdd(a.scal + S_STAGE, (uint32_t)__popc(act));
+        base = __shfl_sync(act, base, leader);
+        const uint32_t k = base + (uint32_t)__popc(act & ((1u << lane) - 1u));
+        if (k < a.stage_cap) a.stage[k] = make_uint2(lo, hi);
     }
 }
 
@@ -485,7 +504,7 @@ __device__ __forceinline__ void box_of(const Boxes& b, uint32_t n, uint32_t i, i
     }
 }
 
-template <bool kWrite>
+template <int kMode>
 __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
@@ -519,7 +538,7 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                         box_of(a.b, n, j, lj, hj);
                         if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] && lj[2] <= hi[2] &&
                             lo[2] <= hj[2])
-                            emit<kWrite>(a, i, j, cand, kept);
+                            emit<kMode>(a, i, j, cand, kept);
                     }
                 }
     }
@@ -537,14 +556,26 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
                         if (x == max(lo[0], lj[0]) && y == max(lo[1], lj[1]) && z == max(lo[2], lj[2]))
-                            emit<kWrite>(a, i, j, cand, kept);
+                            emit<kMode>(a, i, j, cand, kept);
                     }
                 }
     }
-    if (!kWrite && cand) {
+    if (kMode != kWritePass && cand) {
         atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
         if (kept) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), (unsigned long long)kept);
     }
+}
+
+// Staged pairs into their owners' segments (cursor zeroed; the segment sort
+// then fixes the order).
+__global__ void k_stage_scatter(uint32_t count, const uint2* __restrict__ stage, const uint32_t* __restrict__ off,
+                                uint32_t* cursor, uint32_t* pi, uint32_t* pj) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint2 p = stage[k];
+    const uint32_t slot = off[p.x] + atomicAdd(cursor + p.x, 1u);
+    pi[slot] = p.x;
+    pj[slot] = p.y;
 }
 
 // Sorts each REV's pair segment by partner (insertion sort; segments are short).
@@ -1074,6 +1105,8 @@ struct ContactState {
     uint32_t* bsum = nullptr;      // scan block sums
     uint32_t* grid_heads = nullptr;  // dense corner grid of a single scene
     size_t grid_cap = 0;
+    uint2* stage = nullptr;          // stored pairs of the append pass
+    size_t stage_cap = 0;
     size_t bsum_cap = 0;
     unsigned long long* keys1 = nullptr;
     uint32_t* heads1 = nullptr;
@@ -1192,6 +1225,7 @@ cudaError_t ensure_state(vx_scene* s) {
     if (e == cudaSuccess) e = alloc(c->keys1, c->table1);
     if (e == cudaSuccess) e = alloc(c->heads1, c->table1);
     if (e == cudaSuccess) e = alloc(c->scal, kScalars);
+    if (e == cudaSuccess) e = grow(c->stage, c->stage_cap, n / 4 + 4096);
     if (e == cudaSuccess) e = alloc(c->heat_sum, 2);
     if (e == cudaSuccess) e = cudaMallocHost(&c->h_scal, 32 * sizeof(uint32_t));
     return e;
@@ -1341,7 +1375,7 @@ void contact_release(vx_scene* s) {
                     c->items, c->code, c->impact, c->sw_flag, c->sw_off, c->sw_key, c->sw_cn, c->sw_cm,
                     c->sw_keep, c->sw_koff, c->rec_key[0], c->rec_key[1], c->rec_cn[0], c->rec_cn[1],
                     c->rec_cm[0], c->rec_cm[1], c->ci, c->cj, c->cn, c->cm,
-                    c->scal, c->heat_sum, c->grid_heads};
+                    c->scal, c->heat_sum, c->grid_heads, c->stage};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -1478,10 +1512,13 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         pa.count_pairs = first_generation;
         pa.pi = nullptr;
         pa.pj = nullptr;
+        pa.stage = c->stage;
+        pa.stage_cap = (uint32_t)std::min<size_t>(c->stage_cap, 0xffffffffu);
         cudaError_t ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
         if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
+        if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_STAGE, 0, sizeof(uint32_t), st);
         if (ge != cudaSuccess) return cuda_fail(ge, what);
-        k_pairs<false><<<grid(n), 256, 0, st>>>(pa);
+        k_pairs<kAppendPass><<<grid(n), 256, 0, st>>>(pa);
         c->launches += 1;
         ge = scan(c, st, c->cnt, c->off, n);
         if (ge == cudaSuccess)
@@ -1506,9 +1543,20 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         if (stored) {
             ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
             if (ge != cudaSuccess) return cuda_fail(ge, what);
-            k_pairs<true><<<grid(n), 256, 0, st>>>(pa);
+            if (stored <= c->stage_cap) {  // every stored pair was staged
+                k_stage_scatter<<<grid(stored), 256, 0, st>>>(stored, c->stage, c->off, c->cnt, c->pi, c->pj);
+            } else {  // the staging list overflowed: write the pairs in a second pass
+                k_pairs<kWritePass><<<grid(n), 256, 0, st>>>(pa);
+            }
             k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
             c->launches += 2;
+        }
+        if (stored > c->stage_cap) {  // room for this many next time
+            ge = grow(c->stage, c->stage_cap, (size_t)stored + stored / 2 + 4096);
+            if (ge != cudaSuccess) {
+                set_error("%s: a staging list of %u pairs: %s", what, stored, cudaGetErrorString(ge));
+                return VX_OOM;
+            }
         }
         *out_stored = stored;
         return VX_OK;
@@ -1697,7 +1745,8 @@ uint64_t contact_state_bytes(uint32_t n) {
     const uint64_t m = n ? n : 1;
     const uint64_t per_rev = 6 * 4 + 1 + 4 + 3 * 8 * 3 + 6 * 8 + 8 + 2 * 8 + 4 * 7;  // boxes .. component offsets
     const uint64_t table = pow2_at_least(2 * m);
-    return per_rev * m + table * (8 + 4);
+    const uint64_t stage = (m / 4 + 4096) * 8;  // the initial staging list
+    return per_rev * m + table * (8 + 4) + stage;
 }
 
 }  // namespace vx

@@ -202,7 +202,8 @@ def load(path: Path | None = None):
     L.vx_scene_footprint_bytes.restype = C.c_uint64
     L.vx_scene_footprint_bytes.argtypes = [C.c_uint32]
     for name in ("vx_scene_set_positions", "vx_scene_get_positions", "vx_scene_set_rotations",
-                 "vx_scene_get_rotations", "vx_scene_set_loads", "vx_scene_set_predicted"):
+                 "vx_scene_get_rotations", "vx_scene_set_loads", "vx_scene_set_predicted",
+                 "vx_scene_set_previous"):
         getattr(L, name).argtypes = [C.c_void_p, f64p]
     L.vx_scene_set_targets.argtypes = [C.c_void_p, u8p, f64p]
     L.vx_scene_set_bonds.argtypes = [C.c_void_p, u32p, f32p, f32p, f32p]
@@ -348,6 +349,11 @@ class DeviceScene:
     def set_positions(self, x):
         x = self._vec(x)
         check(load().vx_scene_set_positions(self.h, _p(x, C.c_double)))
+
+    def set_previous(self, xyz):
+        """Previous positions (the contact projection's swept starts) of every REV."""
+        x = self._vec(xyz)
+        check(load().vx_scene_set_previous(self.h, _p(x, C.c_double)))
 
     def positions(self, out=None) -> np.ndarray:
         """Positions (n, 3); `out` (a C-contiguous float64 array of 3n values,
