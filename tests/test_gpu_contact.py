@@ -75,6 +75,17 @@ def test_set_previous_writes_every_rev(ctx):
     d.close()
 
 
+@pytest.mark.parametrize("count", [0, 1])
+def test_contact_on_empty_and_single_rev_scenes(ctx, count):
+    s = S.from_cells(np.zeros((count, 3), np.int32), M.component_id("iron"), M.table())
+    d = N.DeviceScene(ctx, s)
+    st = d.contact_project()
+    assert st["candidates"] == 0 and st["pairs"] == 0 and st["contacts"] == 0
+    assert len(d.contacts()) == 0
+    assert d.resolve_contact_velocities(0.1, 0.35) == (0.0, 0.0)
+    d.close()
+
+
 def test_rotated_continuum_has_no_internal_contacts(ctx):
     s = S.scene_new((3, 3, 3))
     c, sn = math.cos(0.37), math.sin(0.37)

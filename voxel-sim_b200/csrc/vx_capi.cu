@@ -70,6 +70,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->d64 = A.take<double>(6 * m);
     s->dinv64 = A.take<double>(6 * m);
     s->d32 = A.take<float>(6 * m);
+    s->mh2_32 = A.take<float>(m);
     s->dinv32 = A.take<float>(6 * m);
     s->b64 = A.take<double>(3 * m);
     s->x64 = A.take<double>(3 * m);

@@ -154,16 +154,18 @@ struct RevOut {
     float* d32;
     float* dinv32;
     double* b64;
+    float* mh2;
 };
 
 // One thread per REV: D = m/h^2 I + sum K_e, b = (pred - x) m/h^2 + load +- f_e,
-// then b *= free and D = P D P + (I - P).
+// then b *= free and D = P D P + (I - P); m/h^2 also in FP32 for the FP32 operator.
 __global__ void k_assemble_revs(SceneView s, BondArrays b, RevOut o, double h, int reuse) {
     const uint32_t n = s.n;
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !tile_active(s.tile_on, i)) return;
     size_t m3n = 3 * (size_t)n;
     double m = (double)s.param1[i].w / (h * h);
+    o.mh2[i] = (float)m;
     double D[6] = {m, m, m, 0.0, 0.0, 0.0};
     v3 x = load3(s.pos, n, i);
     v3 p = load3(s.pred, n, i);
@@ -209,7 +211,7 @@ cudaError_t launch_assembly(vx_scene* s, double h, bool reuse_preconditioner) {
     size_t m = 3 * (size_t)s->n;
     cudaMemsetAsync(s->bond_count, 0, sizeof(uint32_t), s->stream);
     k_assemble_bonds<<<(unsigned)((m + 255) / 256), 256, 0, s->stream>>>(v, s->bonds, s->bond_count);
-    RevOut o{s->d64, s->dinv64, s->d32, s->dinv32, s->b64};
+    RevOut o{s->d64, s->dinv64, s->d32, s->dinv32, s->b64, s->mh2_32};
     k_assemble_revs<<<(s->n + 255) / 256, 256, 0, s->stream>>>(v, s->bonds, o, h, reuse_preconditioner ? 1 : 0);
     return cudaGetLastError();
 }

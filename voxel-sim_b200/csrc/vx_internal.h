@@ -113,6 +113,7 @@ struct vx_scene {
     double* d64;                  // [6][n] projected diagonal block
     double* dinv64;               // [6][n]
     float* d32;
+    float* mh2_32;  // [n] m/h^2 of the last assembly: the FP32 operator's mass term
     float* dinv32;
     double* b64;                  // [3][n]
 

@@ -9,7 +9,8 @@
 //
 // One iteration is two grid-stride kernels sized to fill the GPU once:
 //   k_matvec  p_new = z + beta p_old (ping-pong buffers, formed for the REV and,
-//             on the fly, for its six neighbours) and Ap = D p - P sum K p_nbr;
+//             on the fly, for its six neighbours) and Ap (apply_row: in FP64
+//             D p - P sum K p_nbr, in FP32 the same operator built from m/h^2);
 //             writes per-block partials of p.Ap.
 //   k_update  x += alpha p, r -= alpha Ap, z = D^-1 r; writes per-block partials
 //             of r.z and r.r.
@@ -234,7 +235,7 @@ __global__ void k_accumulate(uint32_t n, double* __restrict__ x64, const float* 
 
 // ---- drivers ------------------------------------------------------------------------------
 static IterArgs<double> args64(vx_scene* s, int ping) {
-    IterArgs<double> a;
+    IterArgs<double> a{};
     a.n = s->n;
     a.kn = s->n;
     a.flags = s->flags;
@@ -257,7 +258,7 @@ static IterArgs<double> args64(vx_scene* s, int ping) {
 }
 
 static IterArgs<float> args32(vx_scene* s, int ping) {
-    IterArgs<float> a;
+    IterArgs<float> a{};
     a.n = s->n;
     a.kn = kstride32(s->n);
     a.flags = s->flags;
@@ -266,6 +267,7 @@ static IterArgs<float> args32(vx_scene* s, int ping) {
     a.Dinv = s->dinv32;
     a.nbr = s->nbr;
     a.rev = s->rev;
+    a.mh2 = s->mh2_32;
     a.z_in = s->z32;
     a.p_old = s->p32[ping];
     a.p_new = s->p32[ping ^ 1];

@@ -5,10 +5,12 @@
 // block of 512 threads per SM owns a contiguous range of REVs for the whole
 // inner solve. Shared memory holds, per REV of the range, the stiffness of its
 // three owned bonds, the pair (z, p_old) as float4 + float2 records, its six
-// neighbour deltas as int16 and its free-axis flags, so an in-range neighbour
-// costs two vector loads from shared memory and no index load. x, r, p and Ap
-// live in registers of the owning thread; the diagonal block and its inverse
-// are read from L2 (issued before the grid wait when registers allow).
+// neighbour deltas as int16, its mass term m/h^2 and its free-axis flags, so an
+// in-range neighbour costs two vector loads from shared memory and no index
+// load. x, r, p and Ap live in registers of the owning thread. The operator is
+// the FP32 row of apply_row (vx_pcg_core.cuh): the diagonal comes from the
+// mass term and the bonds, so only its inverse is read from L2 (issued before
+// the grid wait when registers allow).
 // Neighbours outside the range are read from the global copy of (z, p_old),
 // which every block republishes once per iteration. An iteration is the
 // recurrence of k_matvec/k_update in vx_pcg.cu (src/solver.rs:1833-1911) with
@@ -34,15 +36,15 @@ namespace {
 
 constexpr int kPThreads = 512;
 // shared memory per REV: K float4[3] + float2[3], (z, p_old) float4 + float2,
-// three delta words and one flag byte
-constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 1;
+// three delta words, the mass term and one flag byte
+constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 4 + 1;
 
 struct PersistArgs {
     uint32_t n;
     uint32_t cap;  // REVs per block (contiguous range)
     uint32_t kn;   // REV stride of the per-axis K arrays
     const uint8_t* flags;
-    const float* D;
+    const float* mh2;           // m/h^2 [n]
     const float* K;
     const float* Dinv;
     const uint32_t* code;       // [3][n] neighbour deltas
@@ -144,9 +146,10 @@ __device__ __forceinline__ F3 smul(const Sym<float>& s, F3 v) {
 __device__ __forceinline__ Sym<float> sym_of(float4 a, float2 b) { return {a.x, a.y, a.z, a.w, b.x, b.y}; }
 __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-// R REVs per thread. With R <= 2 the diagonal block and its inverse are loaded
-// into registers before each grid wait, so their L2 latency overlaps the wait;
-// at R = 4 the registers are not there and they are loaded where used.
+// R REVs per thread. With R <= 2 the inverse diagonal block is loaded into
+// registers before the grid wait of the matvec phase, so its L2 latency
+// overlaps the wait; at R = 4 the registers are not there and it is loaded
+// where used.
 template <int R>
 __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) {
     constexpr bool kPrefetch = R <= 2;
@@ -160,7 +163,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     float2* sK2 = reinterpret_cast<float2*>(sZP4 + cap);       // [3][cap] (xz, yz)
     float2* sZP2 = sK2 + 3 * cap;                              // [cap] (p_old.y, p_old.z)
     uint32_t* sNB = reinterpret_cast<uint32_t*>(sZP2 + cap);   // [3][cap] neighbour deltas
-    uint8_t* sFL = reinterpret_cast<uint8_t*>(sNB + 3 * cap);  // [cap] free-axis flags
+    float* sM = reinterpret_cast<float*>(sNB + 3 * cap);       // [cap] m/h^2
+    uint8_t* sFL = reinterpret_cast<uint8_t*>(sM + cap);       // [cap] free-axis flags
     const uint32_t lo = blockIdx.x * cap;
     const uint32_t cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
 
@@ -173,11 +177,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             sK2[ax * cap + li] = __ldg(reinterpret_cast<const float2*>(kb + 4 * (size_t)a.kn) + i);
             sNB[ax * cap + li] = __ldg(a.code + (size_t)ax * n + i);
         }
+        sM[li] = __ldg(a.mh2 + i);
         sFL[li] = __ldg(a.flags + i);
     }
 
     float x[R][3], r[R][3], p[R][3], ap[R][3];
-    Sym<float> dreg[kPrefetch ? R : 1], ireg[kPrefetch ? R : 1];
+    Sym<float> ireg[kPrefetch ? R : 1];
     double scale = 1.0;
     {
         double rn = *a.scale_from;
@@ -201,7 +206,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             a.zp4[i] = q4, a.zp2[i] = q2;
             acc[0] += (double)dot3(rr, z);
             acc[1] += (double)dot3(rr, rr);
-            if constexpr (kPrefetch) dreg[k] = load_sym(a.D, n, i);
         }
     }
     unsigned long long seq = 1;
@@ -228,7 +232,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
 
     while (!done) {
         const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
-        // ---- matvec phase: p = z + beta p_old, Ap = D p - P sum K p_nbr ----
+        // ---- matvec phase: p = z + beta p_old,
+        //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
         double pap[1] = {0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
@@ -246,11 +251,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             const float4 o4 = sZP4[li];
             const float2 o2 = sZP2[li];
             const F3 pi = {fmaf(beta, o4.w, o4.x), fmaf(beta, o2.x, o4.y), fmaf(beta, o2.y, o4.z)};
-            Sym<float> Dm;
-            if constexpr (kPrefetch) Dm = dreg[k];
-            else Dm = load_sym(a.D, n, i);
-            F3 y = smul(Dm, pi);
-            F3 s = {0.f, 0.f, 0.f};
+            const float mh = sM[li];
+            F3 s = {mh * pi.x, mh * pi.y, mh * pi.z};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
                 const bool ok = dl[t] != 0;
@@ -273,14 +275,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                 } else {
                     Kb = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
                 }
-                const float m = ok ? 1.f : 0.f;
-                const F3 pn = {m * fmaf(beta, q4.w, q4.x), m * fmaf(beta, q2.x, q4.y), m * fmaf(beta, q2.y, q4.z)};
-                const F3 kv = smul(Kb, pn);
+                const F3 pn = {fmaf(beta, q4.w, q4.x), fmaf(beta, q2.x, q4.y), fmaf(beta, q2.y, q4.z)};
+                const F3 d = ok ? F3{pi.x - pn.x, pi.y - pn.y, pi.z - pn.z} : F3{0.f, 0.f, 0.f};
+                const F3 kv = smul(Kb, d);
                 s.x += kv.x, s.y += kv.y, s.z += kv.z;
             }
-            if (fl & 1) y.x -= s.x;
-            if (fl & 2) y.y -= s.y;
-            if (fl & 4) y.z -= s.z;
+            const F3 y = {(fl & 1) ? s.x : pi.x, (fl & 2) ? s.y : pi.y, (fl & 4) ? s.z : pi.z};
             p[k][0] = pi.x, p[k][1] = pi.y, p[k][2] = pi.z;
             ap[k][0] = y.x, ap[k][1] = y.y, ap[k][2] = y.z;
             pap[0] += (double)dot3(pi, y);
@@ -327,7 +327,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             a.zp4[i] = q4, a.zp2[i] = q2;
             au[0] += (double)dot3(rr, z);
             au[1] += (double)dot3(rr, rr);
-            if constexpr (kPrefetch) dreg[k] = load_sym(a.D, n, i);  // in flight during the wait below
         }
         double tu[2];
         if (!grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu)) {
@@ -418,7 +417,7 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     a.cap = s->persist_cap;
     a.kn = kstride32(s->n);
     a.flags = s->flags;
-    a.D = s->d32;
+    a.mh2 = s->mh2_32;
     a.K = s->bonds.k32;
     a.Dinv = s->dinv32;
     a.code = s->nbcode;

@@ -371,6 +371,7 @@ IterArgs<float> pool_args32(vx_scene* s, int ping) {
     a.Dinv = s->dinv32;
     a.nbr = s->nbr;
     a.rev = s->rev;
+    a.mh2 = s->mh2_32;
     a.z_in = s->z32;
     a.p_old = s->p32[ping];
     a.p_new = s->p32[ping ^ 1];
