@@ -139,7 +139,7 @@ typedef struct vx_pass_params {
     int32_t reuse_preconditioner;/* 1: keep the block-Jacobi inverse of the previous pass
                                     (CPU path, src/solver.rs:554 and :1639) */
     double inner_tolerance;      /* MIXED only: relative target of each FP32 inner solve
-                                    (0 = default 1e-4) */
+                                    (0 = default 1e-5) */
     uint32_t max_outer;          /* MIXED only: refinement cap (0 = default 30) */
     int32_t kernel;              /* MIXED only: VX_KERNEL_AUTO / _STREAMING / _PERSISTENT */
 } vx_pass_params;

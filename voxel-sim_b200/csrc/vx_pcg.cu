@@ -443,7 +443,7 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
         out->converged = 1;
         return VX_OK;
     }
-    if (inner_tolerance <= 0.0) inner_tolerance = 1e-4;
+    if (inner_tolerance <= 0.0) inner_tolerance = 1e-5;
     if (max_outer == 0) max_outer = 30;
     cudaMemsetAsync(s->x64, 0, 3 * (size_t)s->n * sizeof(double), s->stream);
     uint32_t used = 0;

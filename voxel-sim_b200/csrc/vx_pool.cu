@@ -355,7 +355,7 @@ PoolArgs pool_args(vx_pool* p, const vx_pass_params* prm) {
     P.active = p->active;
     P.pending = p->pending;
     P.tolerance = prm ? prm->tolerance : 0.0;
-    P.inner_tolerance = prm && prm->inner_tolerance > 0.0 ? prm->inner_tolerance : 1e-4;
+    P.inner_tolerance = prm && prm->inner_tolerance > 0.0 ? prm->inner_tolerance : 1e-5;
     P.max_iterations = prm ? prm->max_iterations : 0;
     P.max_outer = prm && prm->max_outer ? prm->max_outer : 30;
     return P;
