@@ -447,7 +447,7 @@ struct PairArgs {
     const double* bound;  // per REV: how far it may move in this sweep
     bool all;             // store every pair (the last resort of a sweep)
     bool count_pairs;     // count candidates and pairs (the call's first generation)
-    uint32_t* count;     // per owner: pairs (count and append passes) / cursor (write pass)
+    uint32_t* count;     // per owner: pairs (append pass) / cursor (write pass)
     uint2* stage;         // append pass: (owner, partner) of every stored pair, in no order
     uint32_t stage_cap;
     const uint32_t* off;
@@ -484,8 +484,7 @@ __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, 
         return;
     }
     atomicAdd(a.count + lo, 1u);
-    if (kMode == kAppendPass) {
-        // one atomic per group of lanes emitting together
+    {  // append pass: one atomic per group of lanes emitting together
         const unsigned act = __activemask();
         const unsigned lane = threadIdx.x & 31;
         const int leader = __ffs(act) - 1;
