@@ -503,24 +503,35 @@ __device__ __forceinline__ void box_of(const Boxes& b, uint32_t n, uint32_t i, i
     }
 }
 
-template <int kMode>
+// kLanes threads per REV share the rows of the REV's probe range, so a small
+// scene, which has too few REVs to fill the GPU, examines a REV's candidates in
+// parallel. Emission order does not matter: pairs are counted by atomics and
+// each segment is sorted afterwards. Measured per projection: the 32^3 block
+// 0.712 ms with one thread per REV, 0.645 with 2, 0.630 with 4, 0.693 with 8;
+// the 64^3 block 1.132, 1.206, 1.362 and 1.821 ms.
+constexpr uint32_t kPairSmallScene = 65536;  // REVs below which four threads share a REV
+
+template <int kMode, int kLanes>
 __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = (uint32_t)(gid / kLanes);
+    const int32_t t = (int32_t)(gid % kLanes);
     const uint32_t n = a.n;
-    if (a.b.large[i] == 2) return;
-    const uint32_t slot = a.b.slot[i];
-    const int bits = a.b.bits;
-    int32_t lo[3], hi[3];
-    box_of(a.b, n, i, lo, hi);
     uint32_t cand = 0, kept = 0;
-    const bool large_i = a.b.large[i] != 0;
-    if (!large_i) {
-        // small-small: corners within reach of this box; the smaller REV finds the pair
-        const int32_t w[3] = {a.wx, a.wy, a.wz};
-        for (int32_t z = lo[2] - (w[2] - 1); z <= hi[2]; ++z)
-            for (int32_t y = lo[1] - (w[1] - 1); y <= hi[1]; ++y)
-                for (int32_t x = lo[0] - (w[0] - 1); x <= hi[0]; ++x) {
+    if (i < n && a.b.large[i] != 2) {  // no early return: the whole warp sums the counts below
+        const uint32_t slot = a.b.slot[i];
+        const int bits = a.b.bits;
+        int32_t lo[3], hi[3];
+        box_of(a.b, n, i, lo, hi);
+        const bool large_i = a.b.large[i] != 0;
+        if (!large_i) {
+            // small-small: corners within reach of this box; the smaller REV finds the pair
+            const int32_t w[3] = {a.wx, a.wy, a.wz};
+            const int32_t x0 = lo[0] - (w[0] - 1), y0 = lo[1] - (w[1] - 1), z0 = lo[2] - (w[2] - 1);
+            const int32_t ny = hi[1] - y0 + 1, rows = ny * (hi[2] - z0 + 1);
+            for (int32_t r = t; r < rows; r += kLanes) {
+                const int32_t z = z0 + r / ny, y = y0 + r % ny;
+                for (int32_t x = x0; x <= hi[0]; ++x) {
                     uint32_t head;
                     if (a.grid.heads) {
                         const uint32_t cell = grid_cell(a.grid, x, y, z);
@@ -535,17 +546,19 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                         if (j <= i) continue;
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
-                        if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] && lj[2] <= hi[2] &&
-                            lo[2] <= hj[2])
+                        if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] &&
+                            lj[2] <= hi[2] && lo[2] <= hj[2])
                             emit<kMode>(a, i, j, cand, kept);
                     }
                 }
-    }
-    if (a.mask2) {
-        // pairs with large boxes: the bins of this box, each pair counted at the
-        // lowest corner of the two boxes' intersection
-        for (int32_t z = lo[2]; z <= hi[2]; ++z)
-            for (int32_t y = lo[1]; y <= hi[1]; ++y)
+            }
+        }
+        if (a.mask2) {
+            // pairs with large boxes: the bins of this box, each pair counted at the
+            // lowest corner of the two boxes' intersection
+            const int32_t ny = hi[1] - lo[1] + 1, rows = ny * (hi[2] - lo[2] + 1);
+            for (int32_t r = t; r < rows; r += kLanes) {
+                const int32_t z = lo[2] + r / ny, y = lo[1] + r % ny;
                 for (int32_t x = lo[0]; x <= hi[0]; ++x) {
                     const uint32_t hs = table_find(a.keys2, a.mask2, bin_key(slot, x, y, z, bits));
                     if (hs == VX_EMPTY_U32) continue;
@@ -558,10 +571,16 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                             emit<kMode>(a, i, j, cand, kept);
                     }
                 }
+            }
+        }
     }
-    if (kMode != kWritePass && cand) {
-        atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
-        if (kept) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), (unsigned long long)kept);
+    if (kMode != kWritePass) {  // one pair of atomics per warp
+        cand = __reduce_add_sync(0xffffffffu, cand);
+        kept = __reduce_add_sync(0xffffffffu, kept);
+        if ((threadIdx.x & 31) == 0 && cand) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
+            if (kept) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), (unsigned long long)kept);
+        }
     }
 }
 
@@ -1517,7 +1536,8 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
         if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_STAGE, 0, sizeof(uint32_t), st);
         if (ge != cudaSuccess) return cuda_fail(ge, what);
-        k_pairs<kAppendPass><<<grid(n), 256, 0, st>>>(pa);
+        if (n < kPairSmallScene) k_pairs<kAppendPass, 4><<<grid((size_t)n * 4), 256, 0, st>>>(pa);
+        else k_pairs<kAppendPass, 1><<<grid(n), 256, 0, st>>>(pa);
         c->launches += 1;
         ge = scan(c, st, c->cnt, c->off, n);
         if (ge == cudaSuccess)
@@ -1545,7 +1565,8 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
             if (stored <= c->stage_cap) {  // every stored pair was staged
                 k_stage_scatter<<<grid(stored), 256, 0, st>>>(stored, c->stage, c->off, c->cnt, c->pi, c->pj);
             } else {  // the staging list overflowed: write the pairs in a second pass
-                k_pairs<kWritePass><<<grid(n), 256, 0, st>>>(pa);
+                if (n < kPairSmallScene) k_pairs<kWritePass, 4><<<grid((size_t)n * 4), 256, 0, st>>>(pa);
+                else k_pairs<kWritePass, 1><<<grid(n), 256, 0, st>>>(pa);
             }
             k_sort_segments<<<grid(n), 256, 0, st>>>(n, c->off, c->pj);
             c->launches += 2;
