@@ -306,47 +306,58 @@ struct Boxes {
     int bits;        // key coordinate bits
 };
 
+// The extents, corner bounds and counts are reduced per warp first (min, max
+// and sums do not depend on order), then one lane updates the scalars.
 __global__ void k_boxes(uint32_t n, const double* __restrict__ pos, const double* __restrict__ start, Boxes b,
                         RevFilter f, uint32_t* __restrict__ scal) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t slot = rev_slot(f, i);
-    b.slot[i] = slot;
-    if (slot == VX_EMPTY_U32) {
-        b.large[i] = 2;
-        for (int t = 0; t < 3; ++t) b.lo[(size_t)t * n + i] = b.hi[(size_t)t * n + i] = 0;
-        return;
-    }
-    // |bin| stays 8 below the key range, so corner probes (reach 3) stay inside it
-    const double limit = (double)((1 << (b.bits - 1)) - 8);
-    bool large = false, bad = false;
-    int32_t ext[3];
-    for (int t = 0; t < 3; ++t) {
-        const double s = start[(size_t)t * n + i], p = pos[(size_t)t * n + i];
-        const double a = fmin(s, p) / kCell - kBinHalf, c = fmax(s, p) / kCell + kBinHalf;
-        if (!(fabs(a) < limit) || !(fabs(c) < limit)) {
-            bad = true;
-            b.lo[(size_t)t * n + i] = 0;
-            b.hi[(size_t)t * n + i] = 0;
-            ext[t] = 1;
-            continue;
+    bool small = false, large = false, bad = false;
+    int32_t ext[3] = {0, 0, 0}, lo[3] = {0, 0, 0};
+    if (i < n) {  // no early return: the whole warp takes part in the reductions below
+        const uint32_t slot = rev_slot(f, i);
+        b.slot[i] = slot;
+        if (slot == VX_EMPTY_U32) {
+            b.large[i] = 2;
+            for (int t = 0; t < 3; ++t) b.lo[(size_t)t * n + i] = b.hi[(size_t)t * n + i] = 0;
+        } else {
+            // |bin| stays 8 below the key range, so corner probes (reach 3) stay inside it
+            const double limit = (double)((1 << (b.bits - 1)) - 8);
+            for (int t = 0; t < 3; ++t) {
+                const double s = start[(size_t)t * n + i], p = pos[(size_t)t * n + i];
+                const double a = fmin(s, p) / kCell - kBinHalf, c = fmax(s, p) / kCell + kBinHalf;
+                if (!(fabs(a) < limit) || !(fabs(c) < limit)) {
+                    bad = true;
+                    b.lo[(size_t)t * n + i] = 0;
+                    b.hi[(size_t)t * n + i] = 0;
+                    ext[t] = 1;
+                    continue;
+                }
+                lo[t] = (int32_t)floor(a);
+                const int32_t hi = (int32_t)floor(c);
+                b.lo[(size_t)t * n + i] = lo[t];
+                b.hi[(size_t)t * n + i] = hi;
+                ext[t] = hi - lo[t] + 1;
+                if (ext[t] > kSmallExtent) large = true;
+            }
+            b.large[i] = large ? 1 : 0;
+            small = !large;
         }
-        const int32_t lo = (int32_t)floor(a), hi = (int32_t)floor(c);
-        b.lo[(size_t)t * n + i] = lo;
-        b.hi[(size_t)t * n + i] = hi;
-        ext[t] = hi - lo + 1;
-        if (ext[t] > kSmallExtent) large = true;
     }
-    if (bad) atomicOr(scal + S_ERR, E_RANGE);
-    b.large[i] = large ? 1 : 0;
-    if (large) {
-        atomicAdd(scal + S_LARGE, 1u);
-    } else {
+    const unsigned full = 0xffffffffu, lane = threadIdx.x & 31;
+    if (__any_sync(full, bad) && lane == 0) atomicOr(scal + S_ERR, E_RANGE);
+    const unsigned large_count = __reduce_add_sync(full, large ? 1u : 0u);
+    if (lane == 0 && large_count) atomicAdd(scal + S_LARGE, large_count);
+    if (__any_sync(full, small)) {
         for (int t = 0; t < 3; ++t) {
-            atomicMax(scal + S_EXT + t, (uint32_t)ext[t]);
-            const uint32_t corner = (uint32_t)(b.lo[(size_t)t * n + i] + kCornerBias);
-            atomicMin(scal + S_CMIN + t, corner);
-            atomicMax(scal + S_CMAX + t, corner);
+            const uint32_t corner = (uint32_t)(lo[t] + kCornerBias);
+            const uint32_t e_max = __reduce_max_sync(full, small ? (uint32_t)ext[t] : 0u);
+            const uint32_t c_min = __reduce_min_sync(full, small ? corner : 0xffffffffu);
+            const uint32_t c_max = __reduce_max_sync(full, small ? corner : 0u);
+            if (lane == 0) {
+                atomicMax(scal + S_EXT + t, e_max);
+                atomicMin(scal + S_CMIN + t, c_min);
+                atomicMax(scal + S_CMAX + t, c_max);
+            }
         }
     }
 }
