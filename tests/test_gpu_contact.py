@@ -86,6 +86,58 @@ def test_contact_on_empty_and_single_rev_scenes(ctx, count):
     d.close()
 
 
+def _loose(count):
+    """count unbonded iron REVs in a row along x."""
+    cells = np.zeros((count, 3), np.int32)
+    cells[:, 0] = 2 * np.arange(count)
+    s = S.from_cells(cells, M.component_id("iron"), M.table())
+    s.neighbor[:] = S.EMPTY
+    return s
+
+
+def test_position_outside_the_bin_key_range_is_reported(ctx):
+    s = _loose(2)
+    d = N.DeviceScene(ctx, s)
+    far = s.position.copy()
+    far[1, 0] = 2.0e4  # 2e6 cells: beyond the 2^20 cells of a scene's bin keys
+    d.set_positions(far)
+    d.set_previous(far)
+    with pytest.raises(N.VxError) as e:
+        d.contact_project()
+    assert e.value.status == N.VX_NONFINITE
+    d.set_positions(s.position)  # the scene stays usable
+    d.set_previous(s.position)
+    st = d.contact_project()  # two cells apart: a candidate pair, no contact
+    assert st["candidates"] == 1 and st["contacts"] == 0
+    d.close()
+
+
+def test_sweep_beyond_the_volume_limit_is_reported(ctx):
+    s = _loose(2)
+    d = N.DeviceScene(ctx, s)
+    pos = s.position.copy()
+    pos[0] += 3.0  # 302^3 bins, above the 2^24 one REV may sweep
+    d.set_positions(pos)
+    d.set_previous(s.position)
+    with pytest.raises(N.VxError) as e:
+        d.contact_project()
+    assert e.value.status == N.VX_BAD_INPUT
+    d.close()
+
+
+def test_sweeps_beyond_the_total_volume_limit_are_reported(ctx):
+    s = _loose(20)
+    d = N.DeviceScene(ctx, s)
+    pos = s.position + 2.5  # 252^3 bins each, under the per-REV limit; 20 of them above 2^28
+    d.set_positions(pos)
+    d.set_previous(s.position)
+    with pytest.raises(N.VxError) as e:
+        d.contact_project()
+    assert e.value.status == N.VX_BAD_INPUT
+    assert "together" in str(e.value)
+    d.close()
+
+
 def test_rotated_continuum_has_no_internal_contacts(ctx):
     s = S.scene_new((3, 3, 3))
     c, sn = math.cos(0.37), math.sin(0.37)

@@ -61,6 +61,8 @@ constexpr uint32_t kPoolKeySlots = 1u << (64 - 3 * kPoolBits);
 constexpr unsigned kProbeLimit = 1u << 20;
 constexpr unsigned kUnionRetries = 1u << 16;
 constexpr uint64_t kMaxLargeVolume = 1ull << 24;  // bins one fast REV may sweep in a substep
+constexpr uint64_t kMaxLargeEntries = 1ull << 28;  // bins all fast REVs together may sweep (32-bit scan)
+constexpr uint64_t kMaxStoredPairs = 1ull << 31;   // pairs one sweep may store (32-bit scan)
 constexpr unsigned long long kEmptyKey = ~0ull;
 constexpr unsigned kScanBlock = 1024;
 constexpr double kSweepBound = 5e-4;  // metres a REV may first move in a sweep before it is replayed with more pairs
@@ -81,6 +83,8 @@ enum {
     S_CMIN = 11,      // [3] smallest small-box corner per axis, biased by kCornerBias
     S_CMAX = 14,      // [3] largest small-box corner per axis, biased
     S_STAGE = 17,     // pairs appended to the staging list by one generation
+    S_LVOL = 18,      // [2] bins of all large boxes together (u64)
+    S_STORED = 20,    // [2] pairs stored by one generation (u64)
     kScalars = 24,    // device words; the host copy holds them and, from kHostCount, counts
     kHostCount = 28
 };
@@ -408,6 +412,7 @@ __global__ void k_large_volume(uint32_t n, Boxes b, uint32_t* vol, uint32_t* sca
             atomicOr(scal + S_ERR, E_VOLUME);
             v = 0;
         }
+        if (v) atomicAdd(reinterpret_cast<unsigned long long*>(scal + S_LVOL), (unsigned long long)v);
     }
     vol[i] = (uint32_t)v;
 }
@@ -467,13 +472,20 @@ struct PairArgs {
     uint32_t* scal;
 };
 
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // k_pairs passes: count each owner's stored pairs and append them to the
 // staging list; or, when that list overflowed, write them into the owners'
 // segments in a second pass.
 enum { kAppendPass = 0, kWritePass = 1 };
 
 template <int kMode>
-__device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand, uint32_t& kept) {
+__device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, uint32_t& cand, uint32_t& kept,
+                                     uint32_t& stored) {
     const uint32_t lo = i < j ? i : j, hi = i < j ? j : i;
     if (a.kin[lo] && a.kin[hi]) return;
     auto acts = [&] {
@@ -488,6 +500,7 @@ __device__ __forceinline__ void emit(const PairArgs& a, uint32_t i, uint32_t j, 
     } else {  // the cheaper test first: most candidates cannot act
         if (!acts() || local_continuum(a.rest, a.nbr, a.rev, a.n, lo, hi)) return;
     }
+    ++stored;
     if (kMode == kWritePass) {
         const uint32_t slot = a.off[lo] + atomicAdd(a.count + lo, 1u);
         a.pi[slot] = lo;
@@ -528,7 +541,7 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
     const uint32_t i = (uint32_t)(gid / kLanes);
     const int32_t t = (int32_t)(gid % kLanes);
     const uint32_t n = a.n;
-    uint32_t cand = 0, kept = 0;
+    uint32_t cand = 0, kept = 0, stored = 0;
     if (i < n && a.b.large[i] != 2) {  // no early return: the whole warp sums the counts below
         const uint32_t slot = a.b.slot[i];
         const int bits = a.b.bits;
@@ -559,7 +572,7 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                         box_of(a.b, n, j, lj, hj);
                         if (lj[0] <= hi[0] && lo[0] <= hj[0] && lj[1] <= hi[1] && lo[1] <= hj[1] &&
                             lj[2] <= hi[2] && lo[2] <= hj[2])
-                            emit<kMode>(a, i, j, cand, kept);
+                            emit<kMode>(a, i, j, cand, kept, stored);
                     }
                 }
             }
@@ -579,18 +592,18 @@ __global__ void __launch_bounds__(256) k_pairs(PairArgs a) {
                         int32_t lj[3], hj[3];
                         box_of(a.b, n, j, lj, hj);
                         if (x == max(lo[0], lj[0]) && y == max(lo[1], lj[1]) && z == max(lo[2], lj[2]))
-                            emit<kMode>(a, i, j, cand, kept);
+                            emit<kMode>(a, i, j, cand, kept, stored);
                     }
                 }
             }
         }
     }
-    if (kMode != kWritePass) {  // one pair of atomics per warp
-        cand = __reduce_add_sync(0xffffffffu, cand);
-        kept = __reduce_add_sync(0xffffffffu, kept);
-        if ((threadIdx.x & 31) == 0 && cand) {
-            atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), (unsigned long long)cand);
-            if (kept) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), (unsigned long long)kept);
+    if (kMode != kWritePass) {  // 64-bit warp sums, then one lane's atomics
+        const unsigned long long c64 = warp_sum_u64(cand), k64 = warp_sum_u64(kept), s64 = warp_sum_u64(stored);
+        if ((threadIdx.x & 31) == 0) {
+            if (c64) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_CAND_LO), c64);
+            if (k64) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_PAIRS_LO), k64);
+            if (s64) atomicAdd(reinterpret_cast<unsigned long long*>(a.scal + S_STORED), s64);
         }
     }
 }
@@ -1493,6 +1506,12 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         if (e != cudaSuccess) return cuda_fail(e, what);
         r = read_scalars(s, c, what);
         if (r != VX_OK) return r;
+        const uint64_t total = (uint64_t)c->h_scal[S_LVOL] | ((uint64_t)c->h_scal[S_LVOL + 1] << 32);
+        if (total > kMaxLargeEntries) {  // checked before the 32-bit offsets below are used
+            set_error("%s: fast REVs swept %llu bins together in one substep, more than %llu", what,
+                      (unsigned long long)total, (unsigned long long)kMaxLargeEntries);
+            return VX_BAD_INPUT;
+        }
         entries = c->h_scal[kHostCount];
         e = ensure_large(c, entries);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->keys2, 0xFF, (size_t)c->table2 * sizeof(unsigned long long), st);
@@ -1546,6 +1565,7 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         cudaError_t ge = cudaMemsetAsync(c->cnt, 0, ((size_t)n + 1) * sizeof(uint32_t), st);
         if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_CAND_LO, 0, 4 * sizeof(uint32_t), st);
         if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_STAGE, 0, sizeof(uint32_t), st);
+        if (ge == cudaSuccess) ge = cudaMemsetAsync(c->scal + S_STORED, 0, 2 * sizeof(uint32_t), st);
         if (ge != cudaSuccess) return cuda_fail(ge, what);
         if (n < kPairSmallScene) k_pairs<kAppendPass, 4><<<grid((size_t)n * 4), 256, 0, st>>>(pa);
         else k_pairs<kAppendPass, 1><<<grid(n), 256, 0, st>>>(pa);
@@ -1556,6 +1576,12 @@ int32_t contact_project(vx_scene* s, vx_contact_stats* out, uint32_t* slot_conta
         if (ge != cudaSuccess) return cuda_fail(ge, what);
         int32_t gr = read_scalars(s, c, what);
         if (gr != VX_OK) return gr;
+        const uint64_t stored64 = (uint64_t)c->h_scal[S_STORED] | ((uint64_t)c->h_scal[S_STORED + 1] << 32);
+        if (stored64 > kMaxStoredPairs) {  // checked before the 32-bit offsets are used
+            set_error("%s: %llu pairs can act in one sweep, more than %llu", what, (unsigned long long)stored64,
+                      (unsigned long long)kMaxStoredPairs);
+            return VX_OOM;
+        }
         const uint32_t stored = c->h_scal[kHostCount];
         if (first_generation) {  // the candidate and pair counts do not depend on the bound
             st_out.candidates = (uint64_t)c->h_scal[S_CAND_LO] | ((uint64_t)c->h_scal[S_CAND_HI] << 32);
