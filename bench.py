@@ -64,7 +64,13 @@ def parse():
     ap.add_argument("--inner-tolerance", type=float, default=0.0,
                     help="relative tolerance of each FP32 inner solve (0 = the library's default)")
     ap.add_argument("--max-iterations", type=int, default=50000)
-    ap.add_argument("--cpu-iterations", type=int, default=40, help="PCG iterations per CPU sample")
+    ap.add_argument("--cpu-iterations", type=int, default=400, help="PCG iterations per CPU sample")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="cpu_baseline: repeat CPU samples until this much time has passed")
+    ap.add_argument("--no-oracle-error", action="store_true",
+                    help="skip the C oracle's FP64 solve that the mixed pass is compared with")
+    ap.add_argument("--no-large-matvec", action="store_true",
+                    help="skip the streaming matvec timing on the 100^3 damaged lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -81,17 +87,8 @@ def build_workload(name, edge, seed):
 
 def predicted_positions(scene, h, gravity):
     """Explicit prediction of src/solver.rs:500-523 from rest (v0 = 0)."""
-    g = np.asarray(gravity, np.float64)
-    v = np.zeros_like(scene.position)
-    free = scene.kinematic == 0
-    v[free] = g * h
-    for a in range(3):
-        v[((scene.target_mask >> a) & 1).astype(bool), a] = 0.0
-    x = scene.position + v * h
-    for a in range(3):
-        m = ((scene.target_mask >> a) & 1).astype(bool)
-        x[m, a] = scene.target[m, a]
-    return x
+    from vxsim import scenes as S
+    return S.predict_from_rest(scene, h, gravity)
 
 
 def measured_peak():
@@ -158,18 +155,56 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_rate(scene, h, pred, iterations, threads):
-    """The reference's CPU block-Jacobi PCG loop (f32 port) on pass 0 of the scene."""
+def cpu_reference_rate(scene, h, pred, iterations, threads, min_seconds):
+    """The reference's CPU block-Jacobi PCG loop (f32 port) on pass 0 of the scene:
+    samples of `iterations` iterations repeated until `min_seconds` have passed."""
     import pyoracle as O
     o = O.OracleScene(scene)
     o.fit_rotations()
     o.assemble(h, pred)
     rows = o.pack_rows()
     dof = 3 * rows["n"]
+    O.pcg_rows_f32(rows, max(2, iterations // 8), 0.0, threads)  # warm the pages and threads
+    it, dt, samples = 0, 0.0, 0
+    while samples == 0 or dt < min_seconds:
+        t0 = time.perf_counter()
+        _, k, _ = O.pcg_rows_f32(rows, iterations, 0.0, threads)
+        dt += time.perf_counter() - t0
+        it += k
+        samples += 1
+    return rows, dof, it, dt, samples
+
+
+def large_matvec(ctx, flush, peak, edge=100):
+    """The streaming FP32 matvec on the damaged lattice of `edge`^3 REVs (inputs
+    well above L2), launched alone after an L2 flush, CUDA events on the scene's
+    stream: its fraction of measured HBM against the canonical 136 B per REV."""
+    from vxsim import native as N
+    from vxsim import scenes as S
+    s = S.damaged_lattice(edge, seed=2)
+    d = N.DeviceScene(ctx, s)
+    d.set_predicted(s.position)
+    d.fit_rotations()
+    d.corotational_pass(1e-3, 1e-8, 1, precision=N.PRECISION_MIXED, kernel=N.KERNEL_STREAMING)
+    t = d.kernel_times(N.PRECISION_MIXED, reps=20, flush_ptr=flush.data_ptr(), flush_bytes=flush.numel())
+    active = s.active_count()
+    d.close()
+    gbs = BYTES_PER_REV["matvec_f32"] * active / (t["matvec_us"] * 1e-6) / 1e9
+    return {"workload": f"damaged_lattice {edge}^3", "active_revs": active, "matvec_us_cold_l2": t["matvec_us"],
+            "update_us_cold_l2": t["update_us"], "matvec_gbs": gbs, "frac": gbs / peak,
+            "bytes_per_rev": BYTES_PER_REV["matvec_f32"]}
+
+
+def oracle_first_pass(scene, h, pred, tolerance):
+    """The C oracle's first pass of the step in FP64 (rotation fit, assembly on
+    the prediction, block-Jacobi PCG to `tolerance`): the checker that the
+    mixed pass's displacement is compared with."""
+    import pyoracle as O
+    o = O.OracleScene(scene)
+    o.fit_rotations()
     t0 = time.perf_counter()
-    _, it, _ = O.pcg_rows_f32(rows, iterations, 0.0, threads)
-    dt = time.perf_counter() - t0
-    return rows, dof, it, dt
+    it, res = o.solve_coupled(h, 200000, tolerance, predicted=pred)
+    return o.positions() - scene.position, it, res, time.perf_counter() - t0
 
 
 def reference_arm(args):
@@ -204,7 +239,8 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n, "dof_active": dof},
-        "cpu_baseline": {"value": value, "unit": "DOF-iter/s", "cores": threads, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "DOF-iter/s", "cores": threads, "kind": "port", "sample": sample,
+                         "omp_num_threads": threads, "host_cpus": os.cpu_count()},
         "e2e": {"value": value, "unit": "DOF-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -324,12 +360,14 @@ def our_arm(args):
                  "update_us_cold_l2": cold["update_us"], "update_us_warm_l2": warm["update_us"],
                  "matvec_gbs_cold_l2": mv_bytes / (cold["matvec_us"] * 1e-6) / 1e9,
                  "update_gbs_cold_l2": up_bytes / (cold["update_us"] * 1e-6) / 1e9}
+    if not args.no_large_matvec:
+        streaming["large_lattice"] = large_matvec(ctx, flush, peak)
     if cold["persistent_iter_us"] > 0:
         # the whole inner solve is one persistent launch: algorithmic bytes of a
         # streamed iteration (matvec + update + direction) per iteration time
         it_bytes = (BYTES_PER_REV["matvec_f32"] + BYTES_PER_REV["update_f32"] + BYTES_PER_REV["direction_f32"]) * active
         achieved = it_bytes / (cold["persistent_iter_us"] * 1e-6) / 1e9
-        kernel = "k_pcg_persistent<4>"
+        kernel = "k_pcg_brick<4>" if cold["persistent_form"] == "brick" else "k_pcg_persistent<4>"
         bytes_per_launch = it_bytes * cold["persistent_iterations"]
         launch_us = cold["persistent_iter_us"] * cold["persistent_iterations"]
         traffic = prof.get("persistent_dram_bytes_per_rev_iteration")
@@ -417,10 +455,22 @@ def our_arm(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rows, dof, it, dt = cpu_reference_rate(scene, h, pred, args.cpu_iterations, threads)
+        rows, dof, it, dt, samples = cpu_reference_rate(scene, h, pred, args.cpu_iterations, threads,
+                                                         args.cpu_seconds)
         cpu = {"value": dof * it / dt, "unit": "DOF-iter/s", "cores": threads, "kind": "port",
-               "sample": f"{it} iterations of the reference's CPU block-Jacobi PCG loop (f32 restatement, "
-                         f"OpenMP) on pass 0 of this workload, {rows['n']} active REVs"}
+               "omp_num_threads": threads, "host_cpus": os.cpu_count(),
+               "sample": f"{samples} samples of {args.cpu_iterations} iterations ({it} in {dt:.1f} s) of the "
+                         f"reference's CPU block-Jacobi PCG loop (f32 restatement, OpenMP, {threads} threads) "
+                         f"on pass 0 of this workload, {rows['n']} active REVs"}
+        if not args.no_oracle_error:
+            # checker: the same first pass solved by the C oracle in FP64
+            dx_o, it_o, res_o, t_o = oracle_first_pass(scene, h, pred, 1e-12)
+            error_vs_fp64["oracle"] = {
+                "value": float(np.linalg.norm(dx_mixed - dx_o) / max(np.linalg.norm(dx_o), 1e-300)),
+                "gpu_fp64_vs_oracle": float(np.linalg.norm(dx_fp64 - dx_o) / max(np.linalg.norm(dx_o), 1e-300)),
+                "reference": "displacement of the first pass solved by the C oracle (FP64 block-Jacobi PCG) "
+                             "to a relative residual of 1e-12",
+                "oracle_iterations": it_o, "oracle_residual": res_o, "oracle_seconds": round(t_o, 1)}
 
     if rank == 0:
         line = {

@@ -193,11 +193,15 @@ int32_t vx_solve_pcg_f32(const float* rhs, const uint32_t* neighbors, const floa
  * the process exits. Systems of more than VX_NOALLOC_MAX_ROWS rows are
  * rejected with VX_BAD_INPUT.
  *
- * The first call on each device looks up that array's device address, so make
- * the first call on a device before any stream capture. All calls share the
- * one array and each call starts by clearing the parts that must be zero;
- * calls that overlap on the GPU (other threads or streams on the same device)
- * race on it and must not run at the same time.
+ * Every call looks up that array's device address on the current device
+ * (cudaGetSymbolAddress), so a device reset in between is harmless. Every call
+ * also reads its convergence scalars back and synchronizes its stream, so it
+ * must never be called while that stream is being captured into a graph. All
+ * calls share the one array and each call starts by clearing the parts that
+ * must be zero; calls that overlap on the GPU (other threads or streams on the
+ * same device) race on it and must not run at the same time. The initial
+ * residual norm is summed in the same order as vx_solve_pcg_f32 sums it, so the
+ * two entry points stop at the same iteration on the same system.
  */
 #define VX_NOALLOC_MAX_ROWS 65536u
 #define VX_NOALLOC_SCRATCH_BYTES 4194304u
@@ -311,6 +315,14 @@ int32_t vx_fracture_commit(vx_scene* scene, double dt, const vx_fracture_config*
  * non-kinematic REV), VX_EMPTY for kinematic REVs; out_count the cluster count.
  */
 int32_t vx_scene_rebuild_clusters(vx_scene* scene, uint32_t* clusters, uint32_t* out_count);
+/*
+ * Bond workspace last_force (src/solver.rs:638-640): per bond, the force
+ * F (K (u - plastic CELL)) (1 - damage) that the last fracture commit evaluated
+ * before updating the bond, f32 N, force[9n] ((axis*n+i)*3+c). A bond the
+ * commit skipped keeps its previous value (zero until its first evaluation),
+ * as the reference's workspace does.
+ */
+int32_t vx_scene_get_last_forces(vx_scene* scene, float* force);
 /* Per-bond fracture state, axis-major: plastic_strain[9n] ((axis*n+i)*3+c), damage[3n],
    equivalent_plastic_strain[3n], fatigue_damage[3n]; any may be NULL. */
 int32_t vx_scene_get_bond_state(vx_scene* scene, float* plastic_strain, float* damage,
@@ -614,6 +626,15 @@ typedef struct vx_tune_result {
 } vx_tune_result;
 int32_t vx_scene_autotune(vx_scene* scene, int32_t precision, const char* cache_path, vx_tune_result* out);
 
+/*
+ * Device time of the inner-solve kernels on the scene's assembled system, CUDA
+ * events on the scene's stream, averaged over reps launches; with flush (a
+ * device buffer of flush_bytes) written before each launch so L2 starts cold.
+ * out_us[5]: streaming matvec us, streaming update us, and for the MIXED
+ * precision when the on-chip form fits: its us per iteration over a 64-iteration
+ * solve, that solve's iterations, and its form (1 = brick plan with one grid
+ * reduction per iteration, 2 = contiguous-range plan, 0 = none).
+ */
 int32_t vx_scene_kernel_times(vx_scene* scene, int32_t precision, uint32_t reps, void* flush,
                               uint64_t flush_bytes, double* out_us);
 

@@ -766,9 +766,14 @@ void vxo_assemble(const vxo_scene* s, const uint8_t* target_mask, const double* 
  * with no free axis are identity rows with zero right-hand side, so they stay
  * zero and leave every dot product unchanged.
  */
+/* Rows are independent, so the parallel loop (above the reference's 32,768-REV
+ * Rayon threshold, src/solver.rs:1700-1709) gives the same bits as the serial one. */
+#define VXO_PAR_REVS 32768u
 void vxo_matvec(const vxo_system* sys, const double* p, double* out) {
     uint32_t n = sys->n;
-    for (uint32_t i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(static) if (n >= VXO_PAR_REVS)
+    for (long li = 0; li < (long)n; ++li) {
+        uint32_t i = (uint32_t)li;
         double v[3];
         mat_vec(sys->diag + 9 * (size_t)i, p + 3 * (size_t)i, v);
         const double* fi = sys->free + 3 * (size_t)i;
@@ -820,10 +825,37 @@ static void bj_apply(const double* l, const double* r, double* z) {
     z[2] = zz;
 }
 
+/*
+ * Serial in REV order below the threshold (the reference's serial path). Above
+ * it the reference sums with Rayon, whose order is not fixed; here each chunk of
+ * 4,096 REVs is summed in order and the chunk sums are added in chunk order, so
+ * the result does not depend on the thread count.
+ */
+#define VXO_DOT_CHUNK 4096u
 static double vdot(uint32_t n, const double* a, const double* b) {
+    if (n < VXO_PAR_REVS) {
+        double s = 0.0;
+        for (uint32_t i = 0; i < n; ++i) s += dot3(a + 3 * (size_t)i, b + 3 * (size_t)i);
+        return s;
+    }
+    long chunks = (long)((n + VXO_DOT_CHUNK - 1) / VXO_DOT_CHUNK);
+    double* part = (double*)malloc((size_t)chunks * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < chunks; ++c) {
+        uint32_t lo = (uint32_t)c * VXO_DOT_CHUNK, hi = lo + VXO_DOT_CHUNK < n ? lo + VXO_DOT_CHUNK : n;
+        double s = 0.0;
+        for (uint32_t i = lo; i < hi; ++i) s += dot3(a + 3 * (size_t)i, b + 3 * (size_t)i);
+        part[c] = s;
+    }
     double s = 0.0;
-    for (uint32_t i = 0; i < n; ++i) s += dot3(a + 3 * (size_t)i, b + 3 * (size_t)i);
+    for (long c = 0; c < chunks; ++c) s += part[c];
+    free(part);
     return s;
+}
+
+static void bj_apply_all(uint32_t n, const double* factor, const double* r, double* z) {
+#pragma omp parallel for schedule(static) if (n >= VXO_PAR_REVS)
+    for (long i = 0; i < (long)n; ++i) bj_apply(factor + 9 * (size_t)i, r + 3 * (size_t)i, z + 3 * (size_t)i);
 }
 
 /*
@@ -842,7 +874,7 @@ int vxo_pcg(const vxo_system* sys, const double* factor, uint32_t max_iterations
     double* ap = (double*)malloc(m * sizeof(double));
     memcpy(r, sys->rhs, 3 * (size_t)n * sizeof(double));
     memset(dx, 0, 3 * (size_t)n * sizeof(double));
-    for (uint32_t i = 0; i < n; ++i) bj_apply(factor + 9 * (size_t)i, r + 3 * (size_t)i, z + 3 * (size_t)i);
+    bj_apply_all(n, factor, r, z);
     memcpy(p, z, 3 * (size_t)n * sizeof(double));
     double rz = vdot(n, r, z);
     double initial = sqrt(vdot(n, r, r));
@@ -855,16 +887,18 @@ int vxo_pcg(const vxo_system* sys, const double* factor, uint32_t max_iterations
         double denom = vdot(n, p, ap);
         if (denom <= 1e-30) break;
         double alpha = rz / denom;
-        for (size_t t = 0; t < 3 * (size_t)n; ++t) {
+#pragma omp parallel for schedule(static) if (n >= VXO_PAR_REVS)
+        for (long t = 0; t < 3 * (long)n; ++t) {
             dx[t] += alpha * p[t];
             r[t] -= alpha * ap[t];
         }
         res = sqrt(vdot(n, r, r)) / initial;
         if (!fixed_iterations && res < tolerance) break;
-        for (uint32_t i = 0; i < n; ++i) bj_apply(factor + 9 * (size_t)i, r + 3 * (size_t)i, z + 3 * (size_t)i);
+        bj_apply_all(n, factor, r, z);
         double next = vdot(n, r, z);
         double beta = next / rz;
-        for (size_t t = 0; t < 3 * (size_t)n; ++t) p[t] = z[t] + beta * p[t];
+#pragma omp parallel for schedule(static) if (n >= VXO_PAR_REVS)
+        for (long t = 0; t < 3 * (long)n; ++t) p[t] = z[t] + beta * p[t];
         rz = next;
     }
     free(r);

@@ -63,7 +63,7 @@ def compare(rows, max_iterations, tolerance):
 
 
 def test_noalloc_matches_allocating_entry_point_on_two_calls_in_a_row():
-    big = packed_rows(S.wood_cube())              # 800 active rows
+    big = packed_rows(S.impose_axis_targets(S.wood_cube()))  # 800 active rows, top layer loaded
     small = packed_rows(S.mixed_block(8, seed=2))  # a different, smaller system after it
     assert small["n"] < big["n"]
     compare(big, 160, 1e-5)

@@ -51,6 +51,7 @@ static void carve(vx_scene* s, Arena& A, uint32_t n, uint32_t mc) {
     s->bond_b = A.take<float4>(3 * m);
     s->bond_c = A.take<float4>(3 * m);
     s->bond_d = A.take<float>(3 * m);
+    s->last_force = A.take<float>(9 * m);
     s->frac_partials = A.take<double>(5 * 3 * (size_t)blocks);
     s->frac_totals = A.take<double>(8);
     s->frac_counter = A.take<uint32_t>(2);
@@ -255,6 +256,9 @@ void scene_release(vx_scene* s) {
     if (s->h_done) cudaFreeHost(s->h_done);
     if (s->h_stage) cudaFreeHost(s->h_stage);
     if (s->arena.base) cudaFree(s->arena.base);
+    if (s->brick_buf) cudaFree(s->brick_buf);
+    s->brick_buf = nullptr;
+    s->brick_ok = false;
     if (s->stream) cudaStreamDestroy(s->stream);
     s->chunk64 = s->chunk32 = nullptr;
     s->ev[0] = s->ev[1] = nullptr;
@@ -850,6 +854,16 @@ int32_t vx_scene_get_bond_state(vx_scene* s, float* plastic, float* damage, floa
         if (damage) damage[e] = a[e].w;
         if (eqp) eqp[e] = b[e].w;
         if (fatigue) fatigue[e] = c[e].y;
+    }
+    return VX_OK;
+}
+
+int32_t vx_scene_get_last_forces(vx_scene* s, float* force) {
+    VX_CHECK_SCENE(s, force);
+    const size_t m = 9 * (size_t)s->n;
+    if (m) {
+        VX_TRY(cudaMemcpyAsync(force, s->last_force, m * sizeof(float), cudaMemcpyDeviceToHost, s->stream), "forces");
+        VX_TRY(cudaStreamSynchronize(s->stream), "forces");
     }
     return VX_OK;
 }

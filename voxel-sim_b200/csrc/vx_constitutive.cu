@@ -138,8 +138,11 @@ __global__ void k_assemble_bonds(SceneView s, BondArrays b, uint32_t* __restrict
         }
     }
     b.state[e] = st;
-    unsigned ballot = __ballot_sync(__activemask(), st == 2);
-    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && ballot) atomicAdd(assembled, __popc(ballot));
+    // one mask for the ballot and the leader: two reads could differ under
+    // independent thread scheduling and drop or double a group's count
+    const unsigned act = __activemask();
+    const unsigned ballot = __ballot_sync(act, st == 2);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && ballot) atomicAdd(assembled, __popc(ballot));
     store_sym(b.k64 + (size_t)a * 6 * n, n, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
     const uint32_t kn = kstride32(n);
     store_sym(b.k32 + (size_t)a * 6 * kn, kn, i, W.s[0], W.s[1], W.s[2], W.s[3], W.s[4], W.s[5]);
@@ -369,7 +372,7 @@ __device__ __forceinline__ double bond_energy(v3 u, const sym6& K, double damage
 
 __global__ void k_fracture_commit(SceneView s, BondArrays b, float4* __restrict__ bond_a, float4* __restrict__ bond_b,
                                   float4* __restrict__ bond_c, float* __restrict__ bond_d, uint32_t* __restrict__ nbr,
-                                  double dt, FractureCfg c, double* __restrict__ partials, uint32_t* __restrict__ counter,
+                                  float* __restrict__ last_force, double dt, FractureCfg c, double* __restrict__ partials, uint32_t* __restrict__ counter,
                                   double* __restrict__ totals) {
     const uint32_t n = s.n;
     const size_t m3n = 3 * (size_t)n;
@@ -395,6 +398,11 @@ __global__ void k_fracture_commit(SceneView s, BondArrays b, float4* __restrict_
             const double old_damage = damage;
             v3 u = u_total - plastic * kCell;
             const double before = bond_energy(u, K, old_damage);
+            // workspace last_force = F (K (u - plastic CELL)) (1 - damage) before the update (src/solver.rs:638-640)
+            const v3 f = mul(F, mul(K, u)) * (1.0 - old_damage);
+            last_force[3 * e] = (float)f.x;
+            last_force[3 * e + 1] = (float)f.y;
+            last_force[3 * e + 2] = (float)f.z;
             if (l.ductility > 1e-5) {  // return map, :226-243
                 const v3 ku0 = mul(K, u);
                 const v3 trial = mk(ku0.x / kArea, ku0.y / kArea, ku0.z / kArea);
@@ -475,7 +483,8 @@ cudaError_t launch_fracture_commit(vx_scene* s, double dt, const vx_fracture_con
                   cfg->fatigue_threshold, cfg->plastic_heat_fraction};
     const unsigned grid = (unsigned)((m + kThreads - 1) / kThreads);
     k_fracture_commit<<<grid, kThreads, 0, s->stream>>>(view_of(s), s->bonds, s->bond_a, s->bond_b, s->bond_c,
-                                                        s->bond_d, s->nbr, dt, c, s->frac_partials, s->frac_counter,
+                                                        s->bond_d, s->nbr, s->last_force, dt, c, s->frac_partials,
+                                                        s->frac_counter,
                                                         s->frac_totals);
     return cudaGetLastError();
 }

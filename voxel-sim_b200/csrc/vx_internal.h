@@ -96,6 +96,7 @@ struct vx_scene {
     float4* bond_b;               // [3n] plastic xyz, equivalent plastic strain
     float4* bond_c;               // [3n] plastic work, fatigue damage, previous / reversal stress ratio
     float* bond_d;                // [3n] loading increment (fatigue)
+    float* last_force;            // [3n][3] Bond workspace last_force, N, of the last fracture commit
     double* frac_partials;        // [5 * 3 * blocks] block partials of the dissipation
     double* frac_totals;          // [8] dissipation totals of the last fracture stage
     uint32_t* frac_counter;       // [2] last-block ticket, bonds broken
@@ -178,6 +179,19 @@ struct vx_scene {
     unsigned persist_G = 0, persist_cap = 0, persist_R = 0;
     size_t persist_smem = 0;
     int nbcode_state = 0;         // 0 = not yet read back, 1 = all deltas encoded, 2 = some did not fit
+    // brick plan of the on-chip inner solve (vx_brick.cu): blocks own spatially
+    // compact sets of REVs; one device allocation holds the plan's tables
+    bool brick_ok = false;
+    unsigned brick_G = 0, brick_cap = 0, brick_hz = 0, brick_hk = 0, brick_R = 0;
+    size_t brick_smem = 0;
+    void* brick_buf = nullptr;
+    uint4* brick_info = nullptr;      // [G] own REVs, halo z slots, halo K slots, neighbour blocks
+    uint32_t* brick_own = nullptr;    // [G][cap] REV of each local REV
+    uint32_t* brick_ref = nullptr;    // [G][3][cap] six 16-bit neighbour refs per local REV
+    uint32_t* brick_hzg = nullptr;    // [G][hz] REV of each halo z slot
+    uint32_t* brick_hke = nullptr;    // [G][hk] bond of each halo K slot
+    uint32_t* brick_nbk = nullptr;    // [G][32] blocks whose REVs are in the halo
+    uint32_t* brick_pub = nullptr;    // [G] iteration whose z the block has published
     uint32_t active = 0;          // REVs with a free axis (cached per target set)
     bool active_cached = false;
     bool assembled = false;

@@ -558,7 +558,7 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
     }
     out_us[0] = 1000.0 * tm / reps;
     out_us[1] = 1000.0 * tu / reps;
-    out_us[2] = out_us[3] = 0.0;
+    out_us[2] = out_us[3] = out_us[4] = 0.0;
     if (precision == VX_PRECISION_MIXED && persistent_plan(s)) {
         // one persistent inner solve of a fixed iteration count on r = b
         const uint32_t iters = 64;
@@ -586,6 +586,7 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
         }
         out_us[2] = its > 0 ? 1000.0 * ms / its : 0.0;
         out_us[3] = its;
+        out_us[4] = s->brick_ok ? 1.0 : 2.0;
     }
     return VX_OK;
 }

@@ -28,6 +28,7 @@
 
 #include "vx_device.cuh"
 #include "vx_kernels.h"
+#include "vx_grid.cuh"
 #include "vx_layout.cuh"
 
 namespace vx {
@@ -61,80 +62,6 @@ struct PersistArgs {
     uint32_t max_iterations;
     unsigned long long spin_limit;
 };
-
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned long long v) {
-    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-// Block-wide sum of NV values, published as this block's partials, then the
-// grid-wide totals once all G blocks have arrived at reduction number `seq`
-// (the arrival counter only grows: reduction seq is complete at seq * G).
-// The __syncthreads before the release makes every thread's earlier global
-// stores part of what the release publishes; the acquire by lane 0, then
-// __syncwarp and the final __syncthreads, order every thread's later loads
-// after the other blocks' released stores. Returns false (in every thread)
-// when a wait ran out here or in another block.
-template <int NV>
-__device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[NV], const PersistArgs& a,
-                                           unsigned long long seq, double (*sh)[32], double* tot, int* s_ok,
-                                           double (&out)[NV]) {
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5, G = gridDim.x;
-#pragma unroll
-    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
-    }
-    __syncthreads();
-    if (warp == 0) {
-        double b[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) b[k] = warp_sum(lane < nw ? sh[k][lane] : 0.0);
-        int ok = 1;
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
-            red_release_add(a.count, 1ull);
-            const unsigned long long target = seq * G;
-            unsigned long long spins = 0;
-            while (ld_acquire(a.count) < target) {
-                if (++spins >= a.spin_limit || ((spins & 63) == 0 && *(volatile int32_t*)a.err)) {
-                    ok = 0;
-                    break;
-                }
-            }
-            if (!ok) atomicExch(a.err, 1);
-            else if (*(volatile int32_t*)a.err) ok = 0;
-        }
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        __syncwarp();
-        double t[NV];
-#pragma unroll
-        for (int k = 0; k < NV; ++k) t[k] = 0.0;
-        if (ok) {
-            for (unsigned blk = lane; blk < G; blk += 32) {
-#pragma unroll
-                for (int k = 0; k < NV; ++k) t[k] += __ldcg(a.part + (size_t)slot[k] * G + blk);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < NV; ++k) t[k] = warp_sum(t[k]);
-        if (lane == 0) {
-#pragma unroll
-            for (int k = 0; k < NV; ++k) tot[k] = t[k];
-            *s_ok = ok;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < NV; ++k) out[k] = tot[k];
-    return *s_ok != 0;
-}
 
 struct F3 {
     float x, y, z;
@@ -376,12 +303,18 @@ cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t
 
 }  // namespace
 
-// Whether the persistent inner solve fits this scene on this GPU; caches the shape.
+// Whether the persistent inner solve fits this scene on this GPU; caches the
+// shape. The brick plan (vx_brick.cu) is preferred; the contiguous-range plan
+// below is the form for scenes the brick plan does not take.
 bool persistent_plan(vx_scene* s) {
     if (s->persist_checked) return s->persist_ok;
     s->persist_checked = true;
     s->persist_ok = false;
     if (s->n == 0) return false;
+    if (brick_plan(s)) {
+        s->persist_ok = true;
+        return true;
+    }
     if (s->nbcode_state == 0) {  // once per topology: did every neighbour delta fit?
         uint32_t bad = 0;
         if (cudaMemcpyAsync(&bad, s->nbcode_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
@@ -412,6 +345,7 @@ bool persistent_plan(vx_scene* s) {
 
 // One FP32 inner solve A32 d = r64 / |r64| in a single cooperative launch.
 int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations) {
+    if (s->brick_ok) return solve_inner_brick(s, tolerance, max_iterations);
     PersistArgs a;
     a.n = s->n;
     a.cap = s->persist_cap;

@@ -159,6 +159,21 @@ Shim g_shim;
 
 constexpr int kShimChunk = 16;
 
+// Puts the caller's current device back when the shim returns: the shim works
+// on device 0 (as cuda_solver.rs does) and must not move the calling thread.
+struct DeviceRestore {
+    int device = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            device = -1;
+            (void)cudaGetLastError();
+        }
+    }
+    ~DeviceRestore() {
+        if (device >= 0) cudaSetDevice(device);
+    }
+};
+
 }  // namespace
 }  // namespace vx
 
@@ -189,6 +204,7 @@ extern "C" int32_t vx_solve_pcg_f32(const float* rhs, const uint32_t* neighbors,
         return VX_OK;
     }
     std::lock_guard<std::mutex> guard(g_shim.lock);
+    DeviceRestore restore;
     Shim& S = g_shim;
     cudaError_t e = cudaSuccess;
     if (!S.init) {
@@ -353,20 +369,19 @@ namespace vx {
 namespace {
 
 constexpr size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
-// r, z, p (two), Ap, then the reduction partials, the scalars and a status word
+// r, z, p (two), Ap, then the reduction partials, the scalars, a status word
+// and the right-hand side's squared norm
 constexpr size_t noalloc_bytes(size_t n) {
     return 5 * al256(3 * n * sizeof(float)) + al256(2 * ((n + kThreads - 1) / kThreads) * sizeof(double)) +
-           al256(sizeof(ShimScalars)) + al256(sizeof(uint32_t));
+           al256(sizeof(ShimScalars)) + al256(sizeof(uint32_t)) + al256(sizeof(double));
 }
 static_assert(noalloc_bytes(VX_NOALLOC_MAX_ROWS) <= VX_NOALLOC_SCRATCH_BYTES,
               "the scratch array must hold a system of VX_NOALLOC_MAX_ROWS rows");
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_lock;
-void* g_noalloc_base[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once
-// per device. Host code cannot use the array's name as a device pointer.
+// Device address of the scratch array on the current device. Host code cannot
+// use the array's name as a device pointer. The address is looked up on every
+// call rather than kept: a device reset reloads the module and would leave a
+// kept address pointing at memory that no longer exists.
 int32_t noalloc_base(char** out) {
     int device = -1;
     cudaError_t e = cudaGetDevice(&device);
@@ -374,23 +389,28 @@ int32_t noalloc_base(char** out) {
         set_error("vx_solve_pcg_f32_noalloc: no current CUDA device: %s", cudaGetErrorString(e));
         return VX_NO_DEVICE;
     }
-    if (device < 0 || device >= kMaxDevices) {
-        set_error("vx_solve_pcg_f32_noalloc: device %d is beyond the %d devices supported", device, kMaxDevices);
-        return VX_BAD_INPUT;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, vx_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        set_error("vx_solve_pcg_f32_noalloc: scratch address lookup failed on device %d: %s", device,
+                  cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
     }
-    std::lock_guard<std::mutex> guard(g_noalloc_lock);
-    if (!g_noalloc_base[device]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, vx_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            set_error("vx_solve_pcg_f32_noalloc: scratch address lookup failed on device %d: %s", device,
-                      cudaGetErrorString(e));
-            return VX_CUDA_ERROR;
-        }
-        g_noalloc_base[device] = p;
-    }
-    *out = static_cast<char*>(g_noalloc_base[device]);
+    *out = static_cast<char*>(p);
     return VX_OK;
+}
+
+// |rhs|^2 summed by one thread in index order with separate multiply and add
+// roundings: the same bits as vx_solve_pcg_f32's host loop, so both entry
+// points stop at the same iteration on the same system.
+__global__ void k_noalloc_rhs_norm(uint32_t count, const float* __restrict__ rhs, double* __restrict__ out) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double s = 0.0;
+    for (uint32_t t = 0; t < count; ++t) {
+        const double v = (double)rhs[t];
+        s = __dadd_rn(s, __dmul_rn(v, v));
+    }
+    *out = s;
 }
 
 // Neighbour slots must name a row of the system (or be empty).
@@ -464,7 +484,8 @@ extern "C" int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* 
     unsigned blocks_n = (unsigned)((m + kThreads - 1) / kThreads);
     size_t vec = al256(3 * m * sizeof(float));
     size_t off_r = 0, off_z = vec, off_p0 = 2 * vec, off_p1 = 3 * vec, off_ap = 4 * vec, off_part = 5 * vec,
-           off_sc = off_part + al256(2 * (size_t)blocks_n * sizeof(double)), off_status = off_sc + al256(sizeof(ShimScalars));
+           off_sc = off_part + al256(2 * (size_t)blocks_n * sizeof(double)), off_status = off_sc + al256(sizeof(ShimScalars)),
+           off_norm = off_status + al256(sizeof(uint32_t));
     ShimArgs A[2];
     for (int k = 0; k < 2; ++k) {
         A[k].n = n;
@@ -489,12 +510,15 @@ extern "C" int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* 
     if (e == cudaSuccess) {
         k_noalloc_validate<<<(unsigned)((6 * m + 255) / 256), 256, 0, s>>>(n, d_neighbors, d_status);
         k_noalloc_init<<<blocks_n, kThreads, 0, s>>>(A[0], d_rhs);
+        k_noalloc_rhs_norm<<<1, 1, 0, s>>>((uint32_t)(3 * m), d_rhs, (double*)(B + off_norm));
         e = cudaGetLastError();
     }
     ShimScalars h{};
     uint32_t status = 0;
+    double initial_sq = 0.0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, A[0].sc, sizeof(ShimScalars), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&initial_sq, B + off_norm, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         set_error("vx_solve_pcg_f32_noalloc: set-up failed: %s", cudaGetErrorString(e));
@@ -504,7 +528,7 @@ extern "C" int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* 
         set_error("vx_solve_pcg_f32_noalloc: a neighbour slot names a row outside the %u-row system", n);
         return VX_BAD_INPUT;
     }
-    double initial = std::sqrt(h.rr);
+    double initial = std::sqrt(initial_sq);
     if (!(initial > 1e-12)) {
         // (src/cuda_solver.rs:316-324) a zero right-hand side returns a zero correction
         e = cudaMemsetAsync(d_out_dx, 0, 3 * m * sizeof(float), s);
@@ -513,7 +537,7 @@ extern "C" int32_t vx_solve_pcg_f32_noalloc(const float* d_rhs, const uint32_t* 
             set_error("vx_solve_pcg_f32_noalloc: %s", cudaGetErrorString(e));
             return VX_CUDA_ERROR;
         }
-        if (!std::isfinite(h.rr)) {
+        if (!std::isfinite(initial_sq)) {
             set_error("CUDA PCG produced a non-finite residual norm");
             return VX_NONFINITE;
         }

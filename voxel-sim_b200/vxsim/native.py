@@ -222,6 +222,7 @@ def load(path: Path | None = None):
     L.vx_fracture_commit.argtypes = [C.c_void_p, C.c_double, C.POINTER(VxFractureConfig), C.POINTER(VxDissipation),
                                      C.POINTER(C.c_uint32)]
     L.vx_scene_get_bond_state.argtypes = [C.c_void_p, f32p, f32p, f32p, f32p]
+    L.vx_scene_get_last_forces.argtypes = [C.c_void_p, f32p]
     L.vx_scene_rebuild_clusters.argtypes = [C.c_void_p, u32p, C.POINTER(C.c_uint32)]
     L.vx_scene_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.POINTER(VxTuneResult)]
     L.vx_server_create.argtypes = [C.c_void_p, C.POINTER(VxServerConfig), C.POINTER(C.c_void_p)]
@@ -408,11 +409,12 @@ class DeviceScene:
         return int(load().vx_scene_stream(self.h) or 0)
 
     def kernel_times(self, precision, reps=20, flush_ptr=0, flush_bytes=0):
-        out = np.zeros(4, np.float64)
+        out = np.zeros(5, np.float64)
         check(load().vx_scene_kernel_times(self.h, precision, reps, C.c_void_p(flush_ptr), flush_bytes,
                                            _p(out, C.c_double)))
         return {"matvec_us": float(out[0]), "update_us": float(out[1]), "persistent_iter_us": float(out[2]),
-                "persistent_iterations": int(out[3])}
+                "persistent_iterations": int(out[3]),
+                "persistent_form": {0: None, 1: "brick", 2: "range"}[int(out[4])]}
 
     # -- the solve ------------------------------------------------------------
     def fit_rotations(self) -> float:
@@ -464,6 +466,12 @@ class DeviceScene:
                                              _p(fa, C.c_float)))
         return dict(plastic=pl.reshape(3, -1, 3), damage=dm.reshape(3, -1), eq_plastic=ep.reshape(3, -1),
                     fatigue=fa.reshape(3, -1))
+
+    def last_forces(self) -> np.ndarray:
+        """Bond workspace last_force of the last fracture commit, (3, n, 3) f32 N."""
+        out = np.zeros(9 * self.n, np.float32)
+        check(load().vx_scene_get_last_forces(self.h, _p(out, C.c_float)))
+        return out.reshape(3, -1, 3)
 
     def set_velocities(self, v):
         v = self._vec(v)

@@ -265,6 +265,34 @@ def wood_cube(edge=10, displacement=1e-4) -> Scene:
     return s
 
 
+def impose_axis_targets(scene: Scene) -> Scene:
+    """Move every targeted axis of every REV onto its target, as the substep's
+    prediction does before the solve (src/solver.rs:506-512). On the wood cube
+    this lifts the top layer by the displacement, so the pass that follows
+    loads the bonds below it (the axial fixture of src/experiments.rs:79-85)."""
+    for a in range(3):
+        sel = ((scene.target_mask >> a) & 1).astype(bool)
+        scene.position[sel, a] = scene.target[sel, a]
+    return scene
+
+
+def predict_from_rest(scene: Scene, h: float, gravity) -> np.ndarray:
+    """Predicted positions of the first substep from rest (v0 = 0): the explicit
+    prediction of src/solver.rs:500-523. Free REVs drift by g h^2 on their
+    untargeted axes; targeted axes sit on their targets; kinematic REVs stay."""
+    g = np.asarray(gravity, np.float64)
+    v = np.zeros_like(scene.position)
+    free = scene.kinematic == 0
+    v[free] = g * h
+    for a in range(3):
+        v[((scene.target_mask >> a) & 1).astype(bool), a] = 0.0
+    x = scene.position + v * h
+    for a in range(3):
+        m = ((scene.target_mask >> a) & 1).astype(bool)
+        x[m, a] = scene.target[m, a]
+    return x
+
+
 def random_unit_vectors(rng, n) -> np.ndarray:
     v = rng.normal(size=(n, 3))
     v /= np.linalg.norm(v, axis=1, keepdims=True)
