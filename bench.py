@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--request-steps", type=int, default=100, help="served: fixed steps per request")
     ap.add_argument("--slots", type=int, default=256, help="served: resident scenes at most")
     ap.add_argument("--lanes", type=int, default=3, help="served: pools by scene size, each with its own stream")
+    ap.add_argument("--no-fp64-compare", action="store_true",
+                    help="served: skip the plain FP64 single-scene solves of the template scenes")
     ap.add_argument("--scenes", type=int, default=512, help="batched: scenes per batch")
     ap.add_argument("--fp64-sample", type=int, default=None,
                     help="batched: scenes timed in the plain FP64 single-scene form (default all)")
@@ -493,9 +495,9 @@ def our_arm(args):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": total_launch,
-            "tuning": {"kernel": "persistent" if tuning["kernel"] == N.KERNEL_PERSISTENT else "streaming",
-                       "blocks_per_sm": tuning["blocks_per_sm"], "us_per_iteration": tuning["us_per_iteration"],
-                       "candidates_us": [round(c[2], 2) for c in tuning["candidates"]]},
+            "tuning": {"choice": N.tune_label(tuning["kernel"], tuning["blocks_per_sm"]),
+                       "us_per_iteration": tuning["us_per_iteration"],
+                       "candidates_us": {N.tune_label(k, b): round(us, 2) for k, b, us in tuning["candidates"]}},
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -603,6 +605,19 @@ def served_arm(args):
                        drain=args.drain, tolerance=args.tolerance, seed=77 + rank)
     clk = clocks.stop()
     st = out["stats"]
+    # the plain FP64 single-scene form on the same template scenes, weighted by
+    # how often the request stream picked each
+    fp64 = None
+    if not args.no_fp64_compare:
+        import numpy as np
+        ref = V.fp64_single_scene_rate(ctx, [s for s, _ in out["template_scenes"]], tolerance=args.tolerance)
+        picks = np.bincount(out["template_picks"], minlength=len(ref["seconds"]))
+        per_solve = float(np.dot(picks, ref["seconds"]) / max(picks.sum(), 1))
+        served_rate = st["solves"] / out["wall_s"]
+        fp64 = {"solves_per_s": 1.0 / per_solve, "worst_true_residual": ref["worst_true_residual"],
+                "form": "vx_corotational_pass, VX_PRECISION_FP64, each template scene alone, first substep's "
+                        "pass, weighted by the request mix",
+                "speedup_served_vs_fp64": served_rate * per_solve}
     if rank == 0:
         print(json.dumps({
             "metric": "served solves/s (Poisson scene-step requests, continuous batching, FP32 inner PCG in FP64 "
@@ -617,6 +632,7 @@ def served_arm(args):
                        "lanes": out["lanes"],
                        "parallelism": f"replicas{world}"},
             "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"], "max_step_ms": st["max_step_ms"],
+            "request_latency_s": out["request_latency_s"], "fp64_single_scene": fp64,
             "scene_steps_per_s": st["scene_steps"] / out["wall_s"],
             "requests": out["requests"], "completed": out["completed"], "not_converged": out["not_converged"],
             "queued_at_end": st["queued"], "resident_at_end": st["resident"], "rounds": st["rounds"],

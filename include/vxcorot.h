@@ -593,30 +593,29 @@ int32_t vx_scene_checkpoint(vx_scene* scene, int32_t op);
 /* The scene's CUDA stream (a cudaStream_t), for callers that order or time work around it. */
 void* vx_scene_stream(vx_scene* scene);
 /*
- * Average device time of one launch of the PCG matvec and update kernels on the
- * scene's assembled system (precision VX_PRECISION_FP64 or VX_PRECISION_MIXED
- * for the FP32 kernels), timed with CUDA events on the scene stream over reps
- * launches each. When flush_bytes > 0 the device buffer flush is overwritten
- * before every timed launch so the kernels read from HBM, not L2.
- * out_us[0] = matvec, out_us[1] = update, in microseconds. For
- * VX_PRECISION_MIXED on a scene that takes the persistent inner solve,
- * out_us[2] = its time per iteration (one launch of out_us[3] iterations),
- * else both are 0. out_us has four entries.
- */
-/*
  * Autotuner (no counterpart in the reference). After a pass has assembled the
  * scene, times a 64-iteration inner solve of the given precision for every
  * candidate launch configuration and keeps the fastest for the scene's later
- * passes (VX_KERNEL_AUTO follows it): the streaming kernels with a register
- * budget of 3, 4 or 5 blocks of 256 threads per SM, and for MIXED the
- * persistent kernel when the scene fits. With cache_path (or NULL), a choice
- * found there for this GPU, precision and scene size (log2 of the REV count)
- * is applied without timing, and a new choice is stored. Positions and bond
- * state are not changed; the solver's work vectors are.
+ * passes (VX_KERNEL_AUTO follows it):
+ *   - the streaming kernels with a register budget of 3, 4 or 5 blocks of 256
+ *     threads per SM (candidate_blocks = that budget);
+ *   - for MIXED, when the scene fits on chip, the persistent forms
+ *     (candidate_blocks = VX_PERSIST_*): the brick plan with one or two
+ *     threads per REV and tiles of at least 256 or 128 REVs per block, and
+ *     the contiguous-range plan.
+ * With cache_path (or NULL), a choice found there for this GPU, precision and
+ * scene size (log2 of the REV count) is applied without timing, and a new
+ * choice is stored. Positions and bond state are not changed; the solver's
+ * work vectors are.
  */
+#define VX_PERSIST_BRICK_T1_256 1   /* brick plan, 1 thread per REV, >= 256 REVs per block */
+#define VX_PERSIST_BRICK_T2_256 2   /* brick plan, 2 threads per REV, >= 256 REVs per block */
+#define VX_PERSIST_BRICK_T1_128 3   /* brick plan, 1 thread per REV, >= 128 REVs per block */
+#define VX_PERSIST_BRICK_T2_128 4   /* brick plan, 2 threads per REV, >= 128 REVs per block */
+#define VX_PERSIST_RANGE 5          /* contiguous-range plan (classic two-reduction recurrence) */
 typedef struct vx_tune_result {
     int32_t kernel;               /* VX_KERNEL_STREAMING or VX_KERNEL_PERSISTENT */
-    int32_t blocks_per_sm;        /* register budget of the streaming kernels */
+    int32_t blocks_per_sm;        /* streaming: register budget; persistent: VX_PERSIST_* form */
     double us_per_iteration;      /* of the chosen configuration */
     int32_t from_cache;           /* 1: read from cache_path, nothing timed */
     uint32_t candidates;          /* timed configurations (at most 8) */
@@ -634,6 +633,8 @@ int32_t vx_scene_autotune(vx_scene* scene, int32_t precision, const char* cache_
  * precision when the on-chip form fits: its us per iteration over a 64-iteration
  * solve, that solve's iterations, and its form (1 = brick plan with one grid
  * reduction per iteration, 2 = contiguous-range plan, 0 = none).
+ * The streaming kernels are timed alone, one launch of each per rep after the
+ * flush (when given), on the scene's assembled system.
  */
 int32_t vx_scene_kernel_times(vx_scene* scene, int32_t precision, uint32_t reps, void* flush,
                               uint64_t flush_bytes, double* out_us);

@@ -187,3 +187,21 @@ def test_pool_step_is_bit_identical_alone_and_in_a_mix(ctx):
     assert others
     alone.close()
     mixed.close()
+
+
+def test_sharded_front_end_gives_each_scene_its_pool_result(ctx):
+    """vxsim.sharding with this process as the only rank: the batch goes to one
+    pool through sharding.pool_pass, and every scene's displacement is the bits
+    of the same scene solved alone in a pool (slots do not interact)."""
+    from vxsim import sharding as Hs
+    sc = scenes()
+    out = Hs.solve_sharded(sc, Hs.pool_pass(ctx, h=H, tolerance=TOL, max_iterations=CAP))
+    assert len(out) == len(sc)
+    for s, res in zip(sc, out):
+        assert res["stats"]["converged"] == 1 and res["stats"]["true_residual"] <= TOL
+        alone = N.DevicePool(ctx, 1 << 16, 2)
+        k = alone.add(s)
+        alone.fit_rotations()
+        alone.corotational_pass(H, TOL, CAP)
+        assert np.array_equal(alone.positions(k) - s.position, res["displacement"])
+        alone.close()

@@ -94,14 +94,19 @@ __device__ __forceinline__ F3 smul(const Sym<float>& s, F3 v) {
 __device__ __forceinline__ Sym<float> sym_of(float4 a, float2 b) { return {a.x, a.y, a.z, a.w, b.x, b.y}; }
 __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-// R own REVs per thread (local index threadIdx.x + k * blockDim.x).
-template <int R>
+// R own REVs per thread group; TPR threads (1 or 2) per REV. A group's own
+// REV k is local index (threadIdx.x / TPR) + k * (blockDim.x / TPR). With two
+// threads per REV, the first takes the mass term and the REV's three own bonds,
+// the second its three incoming bonds, and a shuffle adds the halves; both keep
+// the REV's vectors, and only the first publishes and writes them.
+template <int R, int TPR>
 __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
     extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
     __shared__ double tot[3];
     __shared__ int s_ok;
     const uint32_t b = blockIdx.x, T = blockDim.x, n = a.n, cap = a.cap;
+    const uint32_t group = threadIdx.x / TPR, half = threadIdx.x % TPR, stride = T / TPR;
     const uint4 info = a.info[b];
     const uint32_t cnt = info.x, nz = info.y, nk = info.z, nnb = info.w;
     float4* sK4 = smem4;                                               // [3][cap] (xx, yy, zz, xy)
@@ -143,7 +148,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
     }
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        const uint32_t l = threadIdx.x + k * T;
+        const uint32_t l = group + k * stride;
         gid[k] = l < cnt ? own[l] : 0u;
 #pragma unroll
         for (int c = 0; c < 3; ++c) x[k][c] = r[k][c] = p[k][c] = s[k][c] = w[k][c] = 0.f;
@@ -166,8 +171,8 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
         // ---- z = D^-1 r, into the block's table and the global copy ----
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const uint32_t l = threadIdx.x + k * T;
-            if (l >= cnt) continue;
+            const uint32_t l = group + k * stride;
+            if (l >= cnt || half != 0) continue;
             const F3 z = smul(load_sym(a.Dinv, n, gid[k]), F3{r[k][0], r[k][1], r[k][2]});
             const float4 z4 = make_float4(z.x, z.y, z.z, 0.f);
             sZ[l] = z4;
@@ -207,36 +212,51 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const uint32_t l = threadIdx.x + k * T;
-            if (l >= cnt) continue;
-            const float4 zi4 = sZ[l];
-            const F3 zi = {zi4.x, zi4.y, zi4.z};
-            const uint32_t words[3] = {sRef[l], sRef[cap + l], sRef[2 * cap + l]};
-            const uint8_t fl = sFL[l];
-            const float mh = sM[l];
-            F3 sum = {mh * zi.x, mh * zi.y, mh * zi.z};
-#pragma unroll
-            for (int t = 0; t < 6; ++t) {
-                const uint32_t ref = (words[t >> 1] >> (16 * (t & 1))) & 0xFFFFu;
-                if (ref == kNoRef) continue;
-                const float4 zj = sZ[ref];
-                Sym<float> Kb;
-                if (t < 3) {
-                    Kb = sym_of(sK4[t * cap + l], sK2[t * cap + l]);
-                } else if (ref < cnt) {
-                    Kb = sym_of(sK4[(t - 3) * cap + ref], sK2[(t - 3) * cap + ref]);
-                } else {
-                    Kb = sym_of(sKh4[ref - cnt], sKh2[ref - cnt]);
+            const uint32_t l = group + k * stride;
+            const bool valid = l < cnt;
+            F3 zi = {0.f, 0.f, 0.f}, sum = {0.f, 0.f, 0.f};
+            if (valid) {
+                const float4 zi4 = sZ[l];
+                zi = {zi4.x, zi4.y, zi4.z};
+                if (half == 0) {
+                    const float mh = sM[l];
+                    sum = {mh * zi.x, mh * zi.y, mh * zi.z};
                 }
-                const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
-                sum.x += kv.x, sum.y += kv.y, sum.z += kv.z;
+                constexpr int kTerms = 6 / TPR;
+#pragma unroll
+                for (int u = 0; u < kTerms; ++u) {
+                    const int t = TPR == 1 ? u : (int)half * 3 + u;
+                    const uint32_t word = sRef[(t >> 1) * cap + l];
+                    const uint32_t ref = (word >> (16 * (t & 1))) & 0xFFFFu;
+                    if (ref == kNoRef) continue;
+                    const float4 zj = sZ[ref];
+                    Sym<float> Kb;
+                    if (t < 3) {
+                        Kb = sym_of(sK4[t * cap + l], sK2[t * cap + l]);
+                    } else if (ref < cnt) {
+                        Kb = sym_of(sK4[(t - 3) * cap + ref], sK2[(t - 3) * cap + ref]);
+                    } else {
+                        Kb = sym_of(sKh4[ref - cnt], sKh2[ref - cnt]);
+                    }
+                    const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
+                    sum.x += kv.x, sum.y += kv.y, sum.z += kv.z;
+                }
             }
+            if constexpr (TPR == 2) {  // every lane takes part: both halves of a REV share a warp
+                sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
+                sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
+                sum.z += __shfl_xor_sync(0xffffffffu, sum.z, 1);
+            }
+            if (!valid) continue;
+            const uint8_t fl = sFL[l];
             const F3 wv = {(fl & 1) ? sum.x : zi.x, (fl & 2) ? sum.y : zi.y, (fl & 4) ? sum.z : zi.z};
             w[k][0] = wv.x, w[k][1] = wv.y, w[k][2] = wv.z;
-            const F3 rv = {r[k][0], r[k][1], r[k][2]};
-            acc[0] += (double)dot3(rv, zi);
-            acc[1] += (double)dot3(wv, zi);
-            acc[2] += (double)dot3(rv, rv);
+            if (half == 0) {
+                const F3 rv = {r[k][0], r[k][1], r[k][2]};
+                acc[0] += (double)dot3(rv, zi);
+                acc[1] += (double)dot3(wv, zi);
+                acc[2] += (double)dot3(rv, rv);
+            }
         }
         double tt[3];
         if (!grid_reduce<3>(acc, slots, a, seq++, red, tot, &s_ok, tt)) {
@@ -274,7 +294,7 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
         const float af = (float)alpha, bf = (float)beta;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const uint32_t l = threadIdx.x + k * T;
+            const uint32_t l = group + k * stride;
             if (l >= cnt) continue;
             const float4 z4 = sZ[l];
             const float zc[3] = {z4.x, z4.y, z4.z};
@@ -294,8 +314,8 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
     if (*(volatile int32_t*)a.err) status = VX_TIMEOUT;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        const uint32_t l = threadIdx.x + k * T;
-        if (l >= cnt) continue;
+        const uint32_t l = group + k * stride;
+        if (l >= cnt || half != 0) continue;
         const size_t g = gid[k];
         a.x[g] = x[k][0], a.x[n + g] = x[k][1], a.x[2 * (size_t)n + g] = x[k][2];
     }
@@ -309,13 +329,14 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
     }
 }
 
-template <int R>
+template <int R, int TPR>
 cudaError_t launch_r(const BrickArgs& a, unsigned G, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_pcg_brick<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_pcg_brick<R, TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     BrickArgs args = a;
     void* params[] = {&args};
-    return cudaLaunchCooperativeKernel((void*)k_pcg_brick<R>, dim3(G), dim3(kBThreads), params, smem, st);
+    return cudaLaunchCooperativeKernel((void*)k_pcg_brick<R, TPR>, dim3(G), dim3(kBThreads), params, smem, st);
 }
 
 // Morton key of a cell (21 bits per axis, offsets from the scene's lowest cell).
@@ -343,18 +364,20 @@ struct BrickTables {
 };
 
 // Builds the tables from the creation positions' lattice cells (f32, [3][n])
-// and the bond tables nbr/rev ([3][n], VX_EMPTY for none). Returns false when
-// a block's tables would not fit `max_smem` bytes of shared memory, a block
-// borders more than 32 others, or a block would own more than 4 REVs per thread.
-bool brick_tables(uint32_t n, unsigned max_blocks, size_t max_smem, const float* rest, const uint32_t* nbr,
-                  const uint32_t* rev, BrickTables* out) {
-    if (n == 0) return false;
+// and the bond tables nbr/rev ([3][n], VX_EMPTY for none): at most max_blocks
+// blocks of at least min_per_block REVs each (the last one excepted). Returns
+// false when a block's tables would not fit `max_smem` bytes of shared memory,
+// a block borders more than 32 others, or a block would own more than four
+// REVs per group of `tpr` threads.
+bool brick_tables(uint32_t n, unsigned max_blocks, unsigned min_per_block, unsigned tpr, size_t max_smem,
+                  const float* rest, const uint32_t* nbr, const uint32_t* rev, BrickTables* out) {
+    if (n == 0 || min_per_block == 0 || (tpr != 1 && tpr != 2)) return false;
     unsigned G = max_blocks;
-    const unsigned min_blocks = (n + 255) / 256;  // at least 256 REVs per block
+    const unsigned min_blocks = (n + min_per_block - 1) / min_per_block;
     if (min_blocks < G) G = min_blocks;
     if (G == 0) G = 1;
     const uint32_t cap = (n + G - 1) / G;
-    if (cap > 4u * kBThreads) return false;
+    if (cap > 4u * kBThreads / tpr) return false;
     G = (n + cap - 1) / cap;  // no empty block
     const size_t m = 3 * (size_t)n;
 
@@ -482,11 +505,11 @@ bool brick_tables(uint32_t n, unsigned max_blocks, size_t max_smem, const float*
     return true;
 }
 
-// Builds and uploads the brick plan of a scene from its creation positions and
-// current bond tables. Returns false (no plan) when brick_tables declines or
-// the device does not take cooperative launches; the range plan of
-// vx_persistent.cu is then tried.
-bool brick_plan(vx_scene* s) {
+// Builds and uploads the brick plan of a scene in the given form
+// (VX_PERSIST_BRICK_*) from its creation positions and current bond tables.
+// Returns false (no plan) when brick_tables declines or the device does not
+// take cooperative launches.
+bool brick_plan(vx_scene* s, int form) {
     s->brick_ok = false;
     if (s->brick_buf) {
         cudaStreamSynchronize(s->stream);
@@ -495,8 +518,6 @@ bool brick_plan(vx_scene* s) {
     }
     const uint32_t n = s->n;
     if (n == 0) return false;
-    if (const char* v = std::getenv("VXCOROT_PERSISTENT"))
-        if (std::strcmp(v, "range") == 0) return false;
     int dev = s->device, max_smem = 0, coop = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -509,9 +530,12 @@ bool brick_plan(vx_scene* s) {
         cudaMemcpyAsync(rev.data(), s->rev, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
         cudaStreamSynchronize(s->stream) != cudaSuccess)
         return false;
+    const unsigned min_per_block = (form == VX_PERSIST_BRICK_T1_128 || form == VX_PERSIST_BRICK_T2_128) ? 128 : 256;
+    const unsigned tpr = (form == VX_PERSIST_BRICK_T2_256 || form == VX_PERSIST_BRICK_T2_128) ? 2 : 1;
     BrickTables T;
     // the kernel's static shared memory (reduction slots) takes the last 2 KB
-    if (!brick_tables(n, (unsigned)s->sm_count, (size_t)max_smem - 2048, rest.data(), nbr.data(), rev.data(), &T))
+    if (!brick_tables(n, (unsigned)s->sm_count, min_per_block, tpr, (size_t)max_smem - 2048, rest.data(), nbr.data(),
+                      rev.data(), &T))
         return false;
     void* buf = nullptr;
     if (cudaMalloc(&buf, T.image.size()) != cudaSuccess) {
@@ -535,7 +559,9 @@ bool brick_plan(vx_scene* s) {
     s->brick_cap = T.cap;
     s->brick_hz = (unsigned)T.hz_cap;
     s->brick_hk = (unsigned)T.hk_cap;
-    s->brick_R = T.cap <= (uint32_t)kBThreads ? 1 : (T.cap <= 2u * kBThreads ? 2 : 4);
+    const uint32_t groups = kBThreads / tpr;
+    s->brick_tpr = tpr;
+    s->brick_R = T.cap <= groups ? 1 : (T.cap <= 2u * groups ? 2 : 4);
     s->brick_smem = T.smem;
     s->brick_ok = true;
     return true;
@@ -579,10 +605,14 @@ int32_t solve_inner_brick(vx_scene* s, double tolerance, uint32_t max_iterations
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->brick_pub, 0, s->brick_G * sizeof(uint32_t), s->stream);
     if (e == cudaSuccess) {
-        switch (s->brick_R) {
-            case 1: e = launch_r<1>(a, s->brick_G, s->brick_smem, s->stream); break;
-            case 2: e = launch_r<2>(a, s->brick_G, s->brick_smem, s->stream); break;
-            default: e = launch_r<4>(a, s->brick_G, s->brick_smem, s->stream); break;
+        const unsigned key = s->brick_R * 4 + s->brick_tpr;
+        switch (key) {
+            case 1 * 4 + 1: e = launch_r<1, 1>(a, s->brick_G, s->brick_smem, s->stream); break;
+            case 2 * 4 + 1: e = launch_r<2, 1>(a, s->brick_G, s->brick_smem, s->stream); break;
+            case 4 * 4 + 1: e = launch_r<4, 1>(a, s->brick_G, s->brick_smem, s->stream); break;
+            case 1 * 4 + 2: e = launch_r<1, 2>(a, s->brick_G, s->brick_smem, s->stream); break;
+            case 2 * 4 + 2: e = launch_r<2, 2>(a, s->brick_G, s->brick_smem, s->stream); break;
+            default: e = launch_r<4, 2>(a, s->brick_G, s->brick_smem, s->stream); break;
         }
     }
     s->launches += 1;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -928,9 +929,19 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
                 if (l.compare(0, key.size() + 1, key + " ") == 0) {
                     int kernel = 0, blocks = 0;
                     double us = 0.0;
-                    if (std::sscanf(l.c_str() + key.size() + 1, "%d %d %lf", &kernel, &blocks, &us) == 3 &&
-                        (kernel == VX_KERNEL_STREAMING || (kernel == VX_KERNEL_PERSISTENT && persistent_plan(s))) &&
-                        blocks >= 3 && blocks <= 5) {
+                    bool usable = false;
+                    if (std::sscanf(l.c_str() + key.size() + 1, "%d %d %lf", &kernel, &blocks, &us) == 3) {
+                        if (kernel == VX_KERNEL_STREAMING) {
+                            usable = blocks >= 3 && blocks <= 5;
+                        } else if (kernel == VX_KERNEL_PERSISTENT && blocks >= VX_PERSIST_BRICK_T1_256 &&
+                                   blocks <= VX_PERSIST_RANGE) {
+                            const int old_form = s->persist_form;
+                            apply_tuning(s, kernel, blocks);
+                            usable = persistent_plan(s);
+                            if (!usable) apply_tuning(s, s->tuned_kernel, old_form);
+                        }
+                    }
+                    if (usable) {
                         std::fclose(f);
                         apply_tuning(s, kernel, blocks);
                         out->kernel = kernel;
@@ -951,13 +962,33 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
         int blocks;
     };
     std::vector<Cand> cands = {{VX_KERNEL_STREAMING, 3}, {VX_KERNEL_STREAMING, 4}, {VX_KERNEL_STREAMING, 5}};
-    if (precision == VX_PRECISION_MIXED && persistent_plan(s)) cands.push_back({VX_KERNEL_PERSISTENT, 4});
-    const int old_blocks = s->pcg_minb;
+    const int old_blocks = s->pcg_minb, old_form = s->persist_form;
+    if (precision == VX_PRECISION_MIXED) {
+        // the persistent forms that fit; brick forms with the same blocks and
+        // threads per REV (a large scene reaches the same tiles from either
+        // minimum) are timed once
+        std::vector<std::array<unsigned, 3>> seen;
+        for (int form = VX_PERSIST_BRICK_T1_256; form <= VX_PERSIST_RANGE; ++form) {
+            s->persist_form = form;
+            s->persist_checked = false;
+            if (!persistent_plan(s)) continue;
+            if (form != VX_PERSIST_RANGE) {
+                const std::array<unsigned, 3> shape = {s->brick_G, s->brick_cap, s->brick_tpr};
+                if (std::find(seen.begin(), seen.end(), shape) != seen.end()) continue;
+                seen.push_back(shape);
+            }
+            cands.push_back({VX_KERNEL_PERSISTENT, form});
+        }
+        s->persist_form = old_form;
+        s->persist_checked = false;
+    }
     int best = -1;
-    for (size_t k = 0; k < cands.size(); ++k) {
+    for (size_t k = 0; k < cands.size() && k < 8; ++k) {
         double us = 0.0;
         int32_t r = time_candidate(s, precision, cands[k].kernel, cands[k].blocks, &us);
         if (r != VX_OK) {
+            s->persist_form = old_form;
+            s->persist_checked = false;
             apply_tuning(s, -1, old_blocks);
             return r;
         }
@@ -966,6 +997,10 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
         out->candidate_us[k] = us;
         out->candidates = (uint32_t)(k + 1);
         if (best < 0 || us < out->candidate_us[best]) best = (int)k;
+    }
+    if (cands[best].kernel != VX_KERNEL_PERSISTENT) {
+        s->persist_form = old_form;
+        s->persist_checked = false;
     }
     apply_tuning(s, cands[best].kernel, cands[best].blocks);
     out->kernel = cands[best].kernel;

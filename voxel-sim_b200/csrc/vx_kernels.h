@@ -84,7 +84,7 @@ int32_t solve_mixed(vx_scene* s, double tolerance, uint32_t max_iterations, doub
 // persistent on-chip FP32 inner solve (vx_persistent.cu)
 bool persistent_plan(vx_scene* s);
 int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations);
-bool brick_plan(vx_scene* s);
+bool brick_plan(vx_scene* s, int form);
 int32_t solve_inner_brick(vx_scene* s, double tolerance, uint32_t max_iterations);
 // |b - A x64| / |b| with the FP64 operator (device scalars updated)
 int32_t true_residual(vx_scene* s, double* out);

@@ -610,7 +610,16 @@ static void set_minb(vx_scene* s, int mb) {
 // the first run of a candidate warms its graph and is not timed.
 int32_t time_candidate(vx_scene* s, int32_t precision, int32_t kernel, int mb, double* us) {
     const uint32_t iters = 64;
-    set_minb(s, mb);
+    if (kernel == VX_KERNEL_PERSISTENT) {
+        s->persist_form = mb;  // mb names the persistent form (VX_PERSIST_*)
+        s->persist_checked = false;
+        if (!persistent_plan(s)) {
+            *us = 1e30;
+            return VX_OK;
+        }
+    } else {
+        set_minb(s, mb);
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -653,8 +662,17 @@ int32_t time_candidate(vx_scene* s, int32_t precision, int32_t kernel, int mb, d
     return VX_OK;
 }
 
+// Streaming: mb is the register budget (blocks per SM). Persistent: mb is the
+// form (VX_PERSIST_*), and the plan is rebuilt for it at the next pass.
 void apply_tuning(vx_scene* s, int32_t kernel, int mb) {
-    set_minb(s, mb);
+    if (kernel == VX_KERNEL_PERSISTENT) {
+        if (s->persist_form != mb) {
+            s->persist_form = mb;
+            s->persist_checked = false;
+        }
+    } else {
+        set_minb(s, mb);
+    }
     s->tuned_kernel = kernel;
 }
 

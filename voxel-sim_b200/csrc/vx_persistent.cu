@@ -25,6 +25,7 @@
 // The waits are bounded; when a bound is hit the kernel records VX_TIMEOUT
 // and every block leaves its loop at its next reduction.
 #include <cstdlib>
+#include <cstring>
 
 #include "vx_device.cuh"
 #include "vx_kernels.h"
@@ -304,16 +305,24 @@ cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t
 }  // namespace
 
 // Whether the persistent inner solve fits this scene on this GPU; caches the
-// shape. The brick plan (vx_brick.cu) is preferred; the contiguous-range plan
-// below is the form for scenes the brick plan does not take.
+// shape. Without a chosen form the brick plan (vx_brick.cu) is preferred and
+// the contiguous-range plan below takes the scenes it does not; a chosen form
+// (the autotuner's, or VXCOROT_PERSISTENT=range) is that form or nothing.
 bool persistent_plan(vx_scene* s) {
     if (s->persist_checked) return s->persist_ok;
     s->persist_checked = true;
     s->persist_ok = false;
+    s->brick_ok = false;
     if (s->n == 0) return false;
-    if (brick_plan(s)) {
-        s->persist_ok = true;
-        return true;
+    int form = s->persist_form;
+    if (const char* v = std::getenv("VXCOROT_PERSISTENT"))
+        if (std::strcmp(v, "range") == 0) form = VX_PERSIST_RANGE;
+    if (form != VX_PERSIST_RANGE) {
+        if (brick_plan(s, form == 0 ? VX_PERSIST_BRICK_T1_256 : form)) {
+            s->persist_ok = true;
+            return true;
+        }
+        if (form != 0) return false;
     }
     if (s->nbcode_state == 0) {  // once per topology: did every neighbour delta fit?
         uint32_t bad = 0;

@@ -121,6 +121,18 @@ class VxContactHeat(C.Structure):
 FIELD_POSITION, FIELD_VELOCITY, FIELD_PREVIOUS = 0, 1, 2
 
 
+PERSIST_FORMS = {1: "brick, 1 thread/REV, >=256 REVs/block", 2: "brick, 2 threads/REV, >=256 REVs/block",
+                 3: "brick, 1 thread/REV, >=128 REVs/block", 4: "brick, 2 threads/REV, >=128 REVs/block",
+                 5: "range (classic recurrence)"}
+
+
+def tune_label(kernel: int, blocks: int) -> str:
+    """Readable name of an autotuner candidate (kernel, blocks field)."""
+    if kernel == KERNEL_PERSISTENT:
+        return "persistent " + PERSIST_FORMS.get(blocks, str(blocks))
+    return f"streaming, {blocks} blocks/SM"
+
+
 class VxTuneResult(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("blocks_per_sm", C.c_int32), ("us_per_iteration", C.c_double),
                 ("from_cache", C.c_int32), ("candidates", C.c_uint32), ("candidate_kernel", C.c_int32 * 8),

@@ -27,11 +27,12 @@ from . import native as N
 from . import scenes as S
 
 
-def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6, blade: str = "contact") -> tuple:
+def served_scene(rng, dof_lo: float = 1e3, dof_hi: float = 2e6, blade: str = "contact", dof=None) -> tuple:
     """(scene, moving mask) for one request. The boxes are drawn as fractions of
     the cube edge, then the edge is chosen so the union holds about the drawn
-    REV count (DOF / 3) of wood."""
-    revs = math.exp(rng.uniform(math.log(dof_lo / 3.0), math.log(dof_hi / 3.0)))
+    REV count (DOF / 3) of wood: `dof` when given, else log-uniform over
+    [dof_lo, dof_hi]."""
+    revs = (dof if dof is not None else math.exp(rng.uniform(math.log(dof_lo), math.log(dof_hi)))) / 3.0
     boxes = []
     for _ in range(int(rng.integers(1, 5))):
         a, b = rng.random(3), rng.random(3)
@@ -93,7 +94,10 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
                blade_speed: float = 1.0, hbm_fraction: float = 0.8, tolerance: float = 1e-8,
                blade: str = "contact", lanes: int = 3) -> dict:
     rng = np.random.default_rng(seed)
-    pool = [served_scene(rng, blade=blade) for _ in range(templates)]
+    # the templates' sizes are a log-spaced grid over 1k-2M DOF (the stratified
+    # form of log-uniform: the extremes of the range are always present)
+    grid = np.exp(np.linspace(math.log(1e3), math.log(2e6), templates))
+    pool = [served_scene(rng, blade=blade, dof=float(d)) for d in grid]
     real = blade == "contact"
     params = N.step_params(1e-3, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5,
                            gravity=(0.0, 0.0, -9.81), tolerance=tolerance, max_iterations=20000,
@@ -123,7 +127,12 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
     st = srv.stats()
     srv.close()
     done = [r for r in results if r["status"] in (N.VX_OK, N.VX_NOT_CONVERGED)]
+    latency = [r["queued_s"] + r["run_s"] for r in done]
     return {
+        "request_latency_s": {"p50": float(np.percentile(latency, 50)) if latency else None,
+                              "p99": float(np.percentile(latency, 99)) if latency else None,
+                              "max": float(max(latency)) if latency else None},
+        "request_solves": int(sum(r["passes"] for r in done)),
         "requests": len(tickets), "completed": len(done), "arrival_rate": rate, "arrival_window_s": duration,
         "blade": blade, "lanes": lanes,
         "submit_s": submit_s, "wall_s": wall, "steps_per_request": steps,
@@ -132,4 +141,34 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
         "not_converged": sum(1 for r in done if r["status"] == N.VX_NOT_CONVERGED),
         "worst_residual": max((r["worst_residual"] for r in done), default=None),
         "mean_queued_s": float(np.mean([r["queued_s"] for r in done])) if done else None,
+        "template_scenes": [(s, m) for s, m in pool], "template_picks": picks.tolist(),
     }
+
+
+def fp64_single_scene_rate(ctx: N.Context, scenes, h: float = 1e-3, tolerance: float = 1e-8,
+                           gravity=(0.0, 0.0, -9.81)) -> dict:
+    """The plain FP64 single-scene form on the given scenes: each one resident
+    alone, its first substep's pass (prediction under gravity from rest,
+    rotation fit, assembly, FP64 block-Jacobi PCG to `tolerance`) solved once
+    to warm it, then timed once with CUDA events on its stream."""
+    import torch
+    times, worst = [], 0.0
+    for s in scenes:
+        pred = S.predict_from_rest(s, h, gravity)
+        d = N.DeviceScene(ctx, s)
+        d.set_predicted(pred)
+        d.save_state()
+        for timed in (False, True):
+            d.restore_state()
+            ext = torch.cuda.ExternalStream(d.stream_ptr)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            d.fit_rotations()
+            st = d.corotational_pass(h, tolerance, 200000, precision=N.PRECISION_FP64)
+            e1.record(ext)
+            e1.synchronize()
+            if timed:
+                times.append(e0.elapsed_time(e1) / 1000.0)
+                worst = max(worst, st["true_residual"])
+        d.close()
+    return {"seconds": times, "worst_true_residual": worst}
