@@ -71,6 +71,10 @@ def parse():
                     help="cpu_baseline: repeat CPU samples until this much time has passed")
     ap.add_argument("--no-oracle-error", action="store_true",
                     help="skip the C oracle's FP64 solve that the mixed pass is compared with")
+    ap.add_argument("--no-batched-ratio", action="store_true",
+                    help="skip the batched-vs-FP64 single-scene comparison in the default line")
+    ap.add_argument("--batched-ratio-scenes", type=int, default=64,
+                    help="scenes in the default line's batched comparison")
     ap.add_argument("--no-large-matvec", action="store_true",
                     help="skip the streaming matvec timing on the 100^3 damaged lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -364,6 +368,15 @@ def our_arm(args):
                  "update_gbs_cold_l2": up_bytes / (cold["update_us"] * 1e-6) / 1e9}
     if not args.no_large_matvec:
         streaming["large_lattice"] = large_matvec(ctx, flush, peak)
+    batched = None
+    if not args.no_batched_ratio:
+        # a smaller batch of the batched workload, so its ratio to the plain FP64
+        # single-scene form is in the default line
+        from vxsim import batched as B
+        small = B.batched_scenes(args.batched_ratio_scenes, seed=2024 + rank)
+        batched = batched_vs_fp64(ctx, local, small, 3, 2, args.tolerance, args.max_iterations)
+        batched["workload"] = (f"batched {len(small)} box-union scenes (edge log-uniform 8-48), one pass each, "
+                               f"3 timed batched solves")
     if cold["persistent_iter_us"] > 0:
         # the whole inner solve is one persistent launch: algorithmic bytes of a
         # streamed iteration (matvec + update + direction) per iteration time
@@ -492,6 +505,7 @@ def our_arm(args):
                          "bytes_per_launch": bytes_per_launch, "launch_us": launch_us,
                          "peak_source": f"{peak_kind} hbm_gbs", "note": note},
             "streaming_kernels": streaming,
+            "batched": batched,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": total_launch,
@@ -509,29 +523,23 @@ def our_arm(args):
     return 0
 
 
-def batched_arm(args):
-    """The batched workload (512 box-union scenes, one corotational pass each, FP32 inner PCG in FP64
-    refinement to 1e-8, solved together in one pool) against the same scenes solved one at a time in the
-    plain FP64 single-scene form. Prints one JSON line; value = batched solves/s."""
+def batched_vs_fp64(ctx, local, scenes, steps, warmup, tolerance, max_iterations, fp64_sample=None):
+    """The batched form (every scene resident in one pool, one corotational pass
+    each, FP32 inner PCG in FP64 refinement) timed over `steps` batched solves
+    with CUDA events on the pool's stream and an L2 flush before each, against
+    the same scenes solved one at a time in the plain FP64 single-scene form
+    (each scene warmed once, then timed once)."""
     import torch
     from vxsim import batched as B
     from vxsim import native as N
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    scenes = B.batched_scenes(args.scenes, seed=2024 + rank)
-    ctx = N.Context(local)
-    bs = B.BatchedSolve(ctx, scenes, tolerance=args.tolerance, max_iterations=args.max_iterations)
+    bs = B.BatchedSolve(ctx, scenes, tolerance=tolerance, max_iterations=max_iterations)
     ext = torch.cuda.ExternalStream(bs.stream_ptr, device=torch.device("cuda", local))
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    for _ in range(warmup):
         bs.solve()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     total_ms, dof_iters, worst, launches = 0.0, 0.0, 0.0, 0
-    for k in range(args.steps):
+    for k in range(steps):
         with torch.cuda.stream(ext):
             flush.fill_(k & 0xFF)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -545,14 +553,9 @@ def batched_arm(args):
             dof_iters += 3.0 * st["active"] * st["iterations"]
             worst = max(worst, st["true_residual"])
         launches += 1 + max(st["kernel_launches"] for st in stats)
-    clk = clocks.stop()
-    solves_per_s = len(scenes) * args.steps / (total_ms / 1000.0)
-    revs = sum(s.n for s in scenes)
     bs.close()
-
-    # the plain FP64 single-scene form on the same scenes, one at a time
-    sample = scenes if args.fp64_sample is None else scenes[:args.fp64_sample]
-    ss = B.SingleSceneSolves(ctx, sample, tolerance=args.tolerance, max_iterations=args.max_iterations)
+    sample = scenes if fp64_sample is None else scenes[:fp64_sample]
+    ss = B.SingleSceneSolves(ctx, sample, tolerance=tolerance, max_iterations=max_iterations)
     for k in range(len(sample)):  # warm every scene: its graph capture stays out of the timed solves
         ss.solve(k)
     fp64_ms, fp64_worst = 0.0, 0.0
@@ -566,24 +569,50 @@ def batched_arm(args):
         fp64_ms += e0.elapsed_time(e1)
         fp64_worst = max(fp64_worst, st["true_residual"])
     ss.close()
+    solves_per_s = len(scenes) * steps / (total_ms / 1000.0)
     fp64_solves_per_s = len(sample) / (fp64_ms / 1000.0)
+    return {"solves_per_s": solves_per_s, "ms_per_step": total_ms / steps,
+            "dof_iters_per_s": dof_iters / (total_ms / 1000.0), "worst_true_residual": worst,
+            "revs_total": sum(s.n for s in scenes), "scenes": len(scenes), "gpu_launches": launches,
+            "fp64_single_scene": {"solves_per_s": fp64_solves_per_s, "scenes_timed": len(sample),
+                                  "worst_true_residual": fp64_worst,
+                                  "form": "vx_corotational_pass, VX_PRECISION_FP64, one scene at a time"},
+            "speedup_vs_fp64_single_scene": solves_per_s / fp64_solves_per_s}
+
+
+def batched_arm(args):
+    """The batched workload (512 box-union scenes, one corotational pass each, FP32 inner PCG in FP64
+    refinement to 1e-8, solved together in one pool) against the same scenes solved one at a time in the
+    plain FP64 single-scene form. Prints one JSON line; value = batched solves/s."""
+    import torch
+    from vxsim import batched as B
+    from vxsim import native as N
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    scenes = B.batched_scenes(args.scenes, seed=2024 + rank)
+    ctx = N.Context(local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    out = batched_vs_fp64(ctx, local, scenes, args.steps, args.warmup, args.tolerance, args.max_iterations,
+                          args.fp64_sample)
+    clk = clocks.stop()
     if rank == 0:
         print(json.dumps({
             "metric": "batched solves/s (one corotational pass per scene, FP32 inner PCG in FP64 refinement "
                       "to 1e-8)",
-            "value": solves_per_s * world, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "value": out["solves_per_s"] * world, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": f"batched {len(scenes)} box-union scenes, edge log-uniform 8-48",
-                       "scenes": len(scenes), "revs_total": revs, "tolerance": args.tolerance,
+                       "scenes": len(scenes), "revs_total": out["revs_total"], "tolerance": args.tolerance,
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
-            "dof_iters_per_s": dof_iters / (total_ms / 1000.0),
-            "worst_true_residual": worst,
-            "fp64_single_scene": {"solves_per_s": fp64_solves_per_s, "scenes_timed": len(sample),
-                                  "worst_true_residual": fp64_worst,
-                                  "form": "vx_corotational_pass, VX_PRECISION_FP64, one scene at a time"},
-            "speedup_vs_fp64_single_scene": solves_per_s / fp64_solves_per_s,
-            "gpu_launches": launches, "clocks": clk,
+            "dof_iters_per_s": out["dof_iters_per_s"],
+            "worst_true_residual": out["worst_true_residual"],
+            "fp64_single_scene": out["fp64_single_scene"],
+            "speedup_vs_fp64_single_scene": out["speedup_vs_fp64_single_scene"],
+            "gpu_launches": out["gpu_launches"], "clocks": clk,
         }), flush=True)
     ctx.close()
     return 0

@@ -141,8 +141,12 @@ def step_params():
 
 
 def test_pool_step_matches_single_scene_steps(ctx):
-    """vx_pool_step against vx_scene_step on each scene (both reach 1e-8 in
-    every pass, so they agree to the solve error), over three steps."""
+    """vx_pool_step against vx_scene_step on each scene over three steps. Both
+    reach 1e-8 in every pass, so they agree to the solve error: the pool runs
+    the classic recurrence, the single scene the on-chip Chronopoulos-Gear one,
+    so the two stop at different points inside the 1e-8 ball, and six passes
+    give a relative difference up to about kappa * 1e-8 (measured 1.6e-5 on the
+    8^3 block); the bar is 5e-5."""
     sc = scenes()
     pool = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)
     slots = [pool.add(s) for s in sc]
@@ -157,10 +161,10 @@ def test_pool_step_matches_single_scene_steps(ctx):
         for _ in range(3):
             assert d.step(p)["status"] == N.VX_OK
         x0 = s.position
-        assert rel(pool.positions(k) - x0, d.positions() - x0) < 1e-5
+        assert rel(pool.positions(k) - x0, d.positions() - x0) < 5e-5
         # velocities are (x - predicted) / h: a position difference within the
         # bar above, divided by the substep h = 0.5 ms
-        v_bar = 1e-5 * np.linalg.norm(d.positions() - x0) / 5e-4
+        v_bar = 5e-5 * np.linalg.norm(d.positions() - x0) / 5e-4
         assert np.linalg.norm(pool.velocities(k) - d.velocities()) <= v_bar
         d.close()
     pool.close()

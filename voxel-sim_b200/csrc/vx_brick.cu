@@ -22,14 +22,15 @@
 // update); vectors are FP32, dot products are summed in FP64, and alpha and
 // beta are rounded to FP32 where they scale vectors.
 //
-// One iteration: z = D^-1 r, published to the block's z table and to the
-// global copy; a release of the block's iteration flag; an acquire of the
-// flags of the blocks that own its halo REVs (not a grid barrier); the halo z
-// gathered from the global copy; w = A z from shared memory; one grid
-// reduction of (gamma, delta, rho), which is also what keeps a block from
-// overwriting its global z while a neighbour may still be reading it. Every
-// wait is bounded: a wait that runs out records VX_TIMEOUT and every block
-// leaves at its next wait.
+// One iteration: a release of the block's iteration flag once its z is in
+// place; w's terms between the block's own REVs (no wait needed); an acquire
+// of the flags of the blocks that own its halo REVs (not a grid barrier),
+// overlapped by those terms; the halo z gathered from the global copy and the
+// halo terms; one grid reduction of (gamma, delta, rho), which is also what
+// keeps a block from overwriting its global z while a neighbour may still be
+// reading it; the update, which forms the next z = D^-1 r into the block's
+// table and the global copy. Every wait is bounded: a wait that runs out
+// records VX_TIMEOUT and every block leaves at its next wait.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -48,6 +49,7 @@ namespace {
 constexpr int kBThreads = 512;
 constexpr uint32_t kNoRef = 0xFFFFu;
 constexpr int kMaxNeighbourBlocks = 32;
+constexpr uint8_t kHaloBit = 0x80;  // in the shared copy of a REV's flags: it has a halo neighbour
 // shared memory per own REV: K float4[3] + float2[3], z float4, refs 3 words,
 // m/h^2, flags; per halo z slot a float4; per halo K slot float4 + float2
 constexpr size_t kOwnBytes = 3 * 16 + 3 * 8 + 16 + 12 + 4 + 1;
@@ -129,7 +131,14 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
             sRef[ax * cap + l] = __ldg(a.ref + ((size_t)b * 3 + ax) * cap + l);
         }
         sM[l] = __ldg(a.mh2 + g);
-        sFL[l] = __ldg(a.flags + g);
+        // the free-axis flags, plus whether any of the REV's neighbours is a halo REV
+        uint8_t fl = __ldg(a.flags + g);
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+            const uint32_t ref = (sRef[(t >> 1) * cap + l] >> (16 * (t & 1))) & 0xFFFFu;
+            if (ref != kNoRef && ref >= cnt) fl |= kHaloBit;
+        }
+        sFL[l] = fl;
     }
     for (uint32_t h = threadIdx.x; h < nk; h += T) {
         const uint32_t e = __ldg(a.hke + (size_t)b * a.hk_cap + h);
@@ -167,20 +176,59 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
     int32_t status = VX_OK;
     bool first = true;
     const unsigned lane = threadIdx.x & 31;
-    while (true) {
-        // ---- z = D^-1 r, into the block's table and the global copy ----
+    // z0 = D^-1 r0; later z's are formed at the end of each update
 #pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const uint32_t l = group + k * stride;
-            if (l >= cnt || half != 0) continue;
-            const F3 z = smul(load_sym(a.Dinv, n, gid[k]), F3{r[k][0], r[k][1], r[k][2]});
-            const float4 z4 = make_float4(z.x, z.y, z.z, 0.f);
-            sZ[l] = z4;
-            a.zg[gid[k]] = z4;
+    for (int k = 0; k < R; ++k) {
+        const uint32_t l = group + k * stride;
+        if (l >= cnt || half != 0) continue;
+        const F3 z = smul(load_sym(a.Dinv, n, gid[k]), F3{r[k][0], r[k][1], r[k][2]});
+        const float4 z4 = make_float4(z.x, z.y, z.z, 0.f);
+        sZ[l] = z4;
+        a.zg[gid[k]] = z4;
+    }
+    // one pass over a REV's bond terms: the ones whose neighbour is the block's
+    // own (halo == false) or a halo REV (halo == true), added to acc
+    auto terms = [&](uint32_t l, F3 zi, bool halo, float (&acc)[3]) {
+        constexpr int kTerms = 6 / TPR;
+#pragma unroll
+        for (int u = 0; u < kTerms; ++u) {
+            const int t = TPR == 1 ? u : (int)half * 3 + u;
+            const uint32_t word = sRef[(t >> 1) * cap + l];
+            const uint32_t ref = (word >> (16 * (t & 1))) & 0xFFFFu;
+            if (ref == kNoRef || (ref >= cnt) != halo) continue;
+            const float4 zj = sZ[ref];
+            Sym<float> Kb;
+            if (t < 3) {
+                Kb = sym_of(sK4[t * cap + l], sK2[t * cap + l]);
+            } else if (ref < cnt) {
+                Kb = sym_of(sK4[(t - 3) * cap + ref], sK2[(t - 3) * cap + ref]);
+            } else {
+                Kb = sym_of(sKh4[ref - cnt], sKh2[ref - cnt]);
+            }
+            const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
+            acc[0] += kv.x, acc[1] += kv.y, acc[2] += kv.z;
         }
+    };
+    while (true) {
+        // ---- the block's z (from the last update) is in place: publish it ----
         __syncthreads();
         ++pub;
         if (threadIdx.x == 0) st_release_u32(a.pub + b, pub);
+        // ---- w = A z, the block's own neighbours first (no wait needed) ----
+        // w = P (m/h^2 z + sum K (z - z_nbr)) + (I - P) z; w[k] holds the sum so far
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t l = group + k * stride;
+            w[k][0] = w[k][1] = w[k][2] = 0.f;
+            if (l >= cnt) continue;
+            const float4 zi4 = sZ[l];
+            const F3 zi = {zi4.x, zi4.y, zi4.z};
+            if (half == 0) {
+                const float mh = sM[l];
+                w[k][0] = mh * zi.x, w[k][1] = mh * zi.y, w[k][2] = mh * zi.z;
+            }
+            terms(l, zi, false, w[k]);
+        }
         // ---- wait for the blocks that own this block's halo REVs ----
         if (threadIdx.x < 32) {
             int ok = 1;
@@ -205,54 +253,35 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
             status = VX_TIMEOUT;
             break;
         }
-        // ---- halo z ----
+        // ---- halo z, then the halo terms and the partials ----
         for (uint32_t h = threadIdx.x; h < nz; h += T) sZ[cnt + h] = __ldcg(a.zg + __ldg(a.hzg + (size_t)b * a.hz_cap + h));
         __syncthreads();
-        // ---- w = A z: P (m/h^2 z + sum K (z - z_nbr)) + (I - P) z; partials ----
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t l = group + k * stride;
             const bool valid = l < cnt;
-            F3 zi = {0.f, 0.f, 0.f}, sum = {0.f, 0.f, 0.f};
-            if (valid) {
+            F3 zi = {0.f, 0.f, 0.f};
+            if (valid && (sFL[l] & kHaloBit)) {
                 const float4 zi4 = sZ[l];
                 zi = {zi4.x, zi4.y, zi4.z};
-                if (half == 0) {
-                    const float mh = sM[l];
-                    sum = {mh * zi.x, mh * zi.y, mh * zi.z};
-                }
-                constexpr int kTerms = 6 / TPR;
-#pragma unroll
-                for (int u = 0; u < kTerms; ++u) {
-                    const int t = TPR == 1 ? u : (int)half * 3 + u;
-                    const uint32_t word = sRef[(t >> 1) * cap + l];
-                    const uint32_t ref = (word >> (16 * (t & 1))) & 0xFFFFu;
-                    if (ref == kNoRef) continue;
-                    const float4 zj = sZ[ref];
-                    Sym<float> Kb;
-                    if (t < 3) {
-                        Kb = sym_of(sK4[t * cap + l], sK2[t * cap + l]);
-                    } else if (ref < cnt) {
-                        Kb = sym_of(sK4[(t - 3) * cap + ref], sK2[(t - 3) * cap + ref]);
-                    } else {
-                        Kb = sym_of(sKh4[ref - cnt], sKh2[ref - cnt]);
-                    }
-                    const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
-                    sum.x += kv.x, sum.y += kv.y, sum.z += kv.z;
-                }
+                terms(l, zi, true, w[k]);
             }
             if constexpr (TPR == 2) {  // every lane takes part: both halves of a REV share a warp
-                sum.x += __shfl_xor_sync(0xffffffffu, sum.x, 1);
-                sum.y += __shfl_xor_sync(0xffffffffu, sum.y, 1);
-                sum.z += __shfl_xor_sync(0xffffffffu, sum.z, 1);
+                w[k][0] += __shfl_xor_sync(0xffffffffu, w[k][0], 1);
+                w[k][1] += __shfl_xor_sync(0xffffffffu, w[k][1], 1);
+                w[k][2] += __shfl_xor_sync(0xffffffffu, w[k][2], 1);
             }
             if (!valid) continue;
+            const float4 zi4 = sZ[l];
+            zi = {zi4.x, zi4.y, zi4.z};
             const uint8_t fl = sFL[l];
-            const F3 wv = {(fl & 1) ? sum.x : zi.x, (fl & 2) ? sum.y : zi.y, (fl & 4) ? sum.z : zi.z};
-            w[k][0] = wv.x, w[k][1] = wv.y, w[k][2] = wv.z;
+            if (!(fl & 1)) w[k][0] = zi.x;
+            if (!(fl & 2)) w[k][1] = zi.y;
+            if (!(fl & 4)) w[k][2] = zi.z;
             if (half == 0) {
                 const F3 rv = {r[k][0], r[k][1], r[k][2]};
+                const F3 wv = {w[k][0], w[k][1], w[k][2]};
                 acc[0] += (double)dot3(rv, zi);
                 acc[1] += (double)dot3(wv, zi);
                 acc[2] += (double)dot3(rv, rv);
@@ -292,10 +321,12 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
         }
         const double alpha = gamma / pap;
         const float af = (float)alpha, bf = (float)beta;
+        // ---- update, and the next z = D^-1 r into the block's table and the global copy ----
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t l = group + k * stride;
             if (l >= cnt) continue;
+            const Sym<float> Di = load_sym(a.Dinv, n, gid[k]);
             const float4 z4 = sZ[l];
             const float zc[3] = {z4.x, z4.y, z4.z};
 #pragma unroll
@@ -304,6 +335,12 @@ __global__ void __launch_bounds__(kBThreads, 1) k_pcg_brick(BrickArgs a) {
                 s[k][c] = fmaf(bf, s[k][c], w[k][c]);
                 x[k][c] = fmaf(af, p[k][c], x[k][c]);
                 r[k][c] = fmaf(-af, s[k][c], r[k][c]);
+            }
+            if (half == 0) {
+                const F3 z = smul(Di, F3{r[k][0], r[k][1], r[k][2]});
+                const float4 zn = make_float4(z.x, z.y, z.z, 0.f);
+                sZ[l] = zn;
+                a.zg[gid[k]] = zn;
             }
         }
         its += 1;
@@ -537,8 +574,11 @@ bool brick_plan(vx_scene* s, int form) {
     if (!brick_tables(n, (unsigned)s->sm_count, min_per_block, tpr, (size_t)max_smem - 2048, rest.data(), nbr.data(),
                       rev.data(), &T))
         return false;
+    // after the tables, the grid reductions' partials: 3 per block (the scene's
+    // own partials array is sized for blocks of at least 256 REVs)
+    const size_t part_bytes = ((size_t)3 * T.G * sizeof(double) + 255) & ~size_t(255);
     void* buf = nullptr;
-    if (cudaMalloc(&buf, T.image.size()) != cudaSuccess) {
+    if (cudaMalloc(&buf, T.image.size() + part_bytes) != cudaSuccess) {
         (void)cudaGetLastError();
         return false;
     }
@@ -555,6 +595,7 @@ bool brick_plan(vx_scene* s, int form) {
     s->brick_hke = reinterpret_cast<uint32_t*>(B + T.o_hk);
     s->brick_nbk = reinterpret_cast<uint32_t*>(B + T.o_nb);
     s->brick_pub = reinterpret_cast<uint32_t*>(B + T.o_pub);
+    s->brick_part = reinterpret_cast<double*>(B + T.image.size());
     s->brick_G = T.G;
     s->brick_cap = T.cap;
     s->brick_hz = (unsigned)T.hz_cap;
@@ -590,7 +631,7 @@ int32_t solve_inner_brick(vx_scene* s, double tolerance, uint32_t max_iterations
     a.scale_from = &s->sc->r64_norm;
     a.x = s->x32;
     a.zg = reinterpret_cast<float4*>(s->zp32);
-    a.part = s->partials;
+    a.part = s->brick_part;
     a.count = reinterpret_cast<unsigned long long*>(s->barrier);
     a.err = reinterpret_cast<int32_t*>(s->barrier + 2);
     a.sc = s->sc32;

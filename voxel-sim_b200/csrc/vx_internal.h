@@ -194,6 +194,7 @@ struct vx_scene {
     uint32_t* brick_hke = nullptr;    // [G][hk] bond of each halo K slot
     uint32_t* brick_nbk = nullptr;    // [G][32] blocks whose REVs are in the halo
     uint32_t* brick_pub = nullptr;    // [G] iteration whose z the block has published
+    double* brick_part = nullptr;     // [3][G] grid-reduction partials
     uint32_t active = 0;          // REVs with a free axis (cached per target set)
     bool active_cached = false;
     bool assembled = false;
