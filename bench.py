@@ -76,7 +76,7 @@ def parse():
     ap.add_argument("--batched-ratio-scenes", type=int, default=64,
                     help="scenes in the default line's batched comparison")
     ap.add_argument("--no-large-matvec", action="store_true",
-                    help="skip the streaming matvec timing on the 100^3 damaged lattice")
+                    help="skip the streaming matvec timing on the 160^3 damaged lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -181,7 +181,7 @@ def cpu_reference_rate(scene, h, pred, iterations, threads, min_seconds):
     return rows, dof, it, dt, samples
 
 
-def large_matvec(ctx, flush, peak, edge=100):
+def large_matvec(ctx, flush, peak, edge=160):
     """The streaming FP32 matvec on the damaged lattice of `edge`^3 REVs (inputs
     well above L2), launched alone after an L2 flush, CUDA events on the scene's
     stream: its fraction of measured HBM against the canonical 136 B per REV."""
