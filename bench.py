@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="served: skip the plain FP64 single-scene solves of the template scenes")
     ap.add_argument("--scenes", type=int, default=512, help="batched: scenes per batch")
+    ap.add_argument("--pool-kernel", default="auto", choices=["auto", "persistent", "streaming"],
+                    help="batched: inner solves in persistent waves (auto, persistent) or tile kernels")
     ap.add_argument("--fp64-sample", type=int, default=None,
                     help="batched: scenes timed in the plain FP64 single-scene form (default all)")
     ap.add_argument("--edge", type=int, default=None)
@@ -523,7 +525,8 @@ def our_arm(args):
     return 0
 
 
-def batched_vs_fp64(ctx, local, scenes, steps, warmup, tolerance, max_iterations, fp64_sample=None):
+def batched_vs_fp64(ctx, local, scenes, steps, warmup, tolerance, max_iterations, fp64_sample=None,
+                    kernel=None):
     """The batched form (every scene resident in one pool, one corotational pass
     each, FP32 inner PCG in FP64 refinement) timed over `steps` batched solves
     with CUDA events on the pool's stream and an L2 flush before each, against
@@ -532,7 +535,8 @@ def batched_vs_fp64(ctx, local, scenes, steps, warmup, tolerance, max_iterations
     import torch
     from vxsim import batched as B
     from vxsim import native as N
-    bs = B.BatchedSolve(ctx, scenes, tolerance=tolerance, max_iterations=max_iterations)
+    bs = B.BatchedSolve(ctx, scenes, tolerance=tolerance, max_iterations=max_iterations,
+                        kernel=N.KERNEL_AUTO if kernel is None else kernel)
     ext = torch.cuda.ExternalStream(bs.stream_ptr, device=torch.device("cuda", local))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     for _ in range(warmup):
@@ -595,8 +599,10 @@ def batched_arm(args):
     ctx = N.Context(local)
     clocks = ClockSampler(local)
     clocks.start()
+    kernel = {"auto": N.KERNEL_AUTO, "persistent": N.KERNEL_PERSISTENT,
+              "streaming": N.KERNEL_STREAMING}[args.pool_kernel]
     out = batched_vs_fp64(ctx, local, scenes, args.steps, args.warmup, args.tolerance, args.max_iterations,
-                          args.fp64_sample)
+                          args.fp64_sample, kernel)
     clk = clocks.stop()
     if rank == 0:
         print(json.dumps({
@@ -607,6 +613,7 @@ def batched_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": f"batched {len(scenes)} box-union scenes, edge log-uniform 8-48",
                        "scenes": len(scenes), "revs_total": out["revs_total"], "tolerance": args.tolerance,
+                       "inner_solve": args.pool_kernel,
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
             "dof_iters_per_s": out["dof_iters_per_s"],
             "worst_true_residual": out["worst_true_residual"],

@@ -209,3 +209,45 @@ def test_sharded_front_end_gives_each_scene_its_pool_result(ctx):
         alone.corotational_pass(H, TOL, CAP)
         assert np.array_equal(alone.positions(k) - s.position, res["displacement"])
         alone.close()
+
+
+def test_persistent_waves_match_the_tile_kernels(ctx):
+    """The pool's inner solves in waves of the persistent kernel (one cooperative
+    launch per wave, per-slot reductions and convergence masks) against the
+    chunk graph of tile kernels: both reach 1e-8 per slot and take the same
+    inner iterations, and the displacements agree to the solve error."""
+    sc = scenes()
+    out = {}
+    for kernel in (N.KERNEL_STREAMING, N.KERNEL_PERSISTENT):
+        pool = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)
+        slots = [pool.add(s) for s in sc]
+        pool.fit_rotations()
+        status, stats = pool.corotational_pass(H, TOL, CAP, kernel=kernel)
+        assert status == N.VX_OK
+        out[kernel] = [(pool.positions(k) - s.position, stats[k]) for s, k in zip(sc, slots)]
+        pool.close()
+    for (d_s, st_s), (d_p, st_p) in zip(out[N.KERNEL_STREAMING], out[N.KERNEL_PERSISTENT]):
+        assert st_s["converged"] == 1 and st_p["converged"] == 1
+        assert st_p["true_residual"] <= TOL and st_s["true_residual"] <= TOL
+        assert abs(st_p["iterations"] - st_s["iterations"]) <= 0.02 * st_s["iterations"] + 4
+        assert rel(d_p, d_s) < 2e-5
+
+
+def test_persistent_waves_of_many_slots(ctx):
+    """More slots than fit one wave (each 16^3 slot takes 3 blocks of at most
+    1,536 REVs, so 60 slots need two waves of at most 148 blocks): every slot
+    converges and equals the same scene solved alone in a pool, bit for bit."""
+    s = S.mixed_block(16, seed=9)
+    pool = N.DevicePool(ctx, 60 * s.n + 4096, 64)
+    slots = [pool.add(s) for _ in range(60)]
+    pool.fit_rotations()
+    status, stats = pool.corotational_pass(H, TOL, CAP, kernel=N.KERNEL_PERSISTENT)
+    assert status == N.VX_OK and all(stats[k]["converged"] == 1 for k in slots)
+    alone = N.DevicePool(ctx, s.n + 4096, 2)
+    a = alone.add(s)
+    alone.fit_rotations()
+    alone.corotational_pass(H, TOL, CAP, kernel=N.KERNEL_PERSISTENT)
+    ref = alone.positions(a)
+    assert all(np.array_equal(pool.positions(k), ref) for k in slots)
+    alone.close()
+    pool.close()

@@ -92,4 +92,73 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
     return *s_ok != 0;
 }
 
+// grid_reduce for blocks that work for different problems (the slots of a
+// pool): the NV values are summed over the blocks [fb, fb + nb) of this block's
+// own problem, in block order, and `act` over all G blocks (a count of blocks
+// still at work, which tells every block when to stop). With fb = 0 and nb = G
+// the NV sums are grid_reduce's bits. Partial rows: slot[k] for the NV values,
+// act_row for act; A as for grid_reduce.
+template <int NV, class A>
+__device__ __forceinline__ bool grid_reduce_ranged(double (&v)[NV], double act, const int (&slot)[NV], int act_row,
+                                                   const A& a, unsigned long long seq, uint32_t fb, uint32_t nb,
+                                                   double (*sh)[32], double* tot, int* s_ok, double (&out)[NV],
+                                                   double* act_total) {
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5, G = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double b[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) b[k] = warp_sum(lane < nw ? sh[k][lane] : 0.0);
+        int ok = 1;
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
+            a.part[(size_t)act_row * G + blockIdx.x] = act;
+            red_release_add_u64(a.count, 1ull);
+            const unsigned long long target = seq * G;
+            unsigned long long spins = 0;
+            while (ld_acquire_u64(a.count) < target) {
+                if (++spins >= a.spin_limit || ((spins & 63) == 0 && *(volatile int32_t*)a.err)) {
+                    ok = 0;
+                    break;
+                }
+            }
+            if (!ok) atomicExch(a.err, 1);
+            else if (*(volatile int32_t*)a.err) ok = 0;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        double t[NV], ta = 0.0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = 0.0;
+        if (ok) {
+            for (unsigned blk = lane; blk < nb; blk += 32) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) t[k] += __ldcg(a.part + (size_t)slot[k] * G + fb + blk);
+            }
+            for (unsigned blk = lane; blk < G; blk += 32) ta += __ldcg(a.part + (size_t)act_row * G + blk);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = warp_sum(t[k]);
+        ta = warp_sum(ta);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) tot[k] = t[k];
+            tot[NV] = ta;
+            *s_ok = ok;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = tot[k];
+    *act_total = tot[NV];
+    return *s_ok != 0;
+}
+
 }  // namespace vx

@@ -18,6 +18,20 @@ struct ContactState;  // grow-only buffers of the contact stage (vx_contact.cu)
 void set_error(const char* fmt, ...);
 void clear_error();
 
+// Per-slot device state of a pool pass (vx_pool.cu; the persistent inner solve
+// of vx_persistent.cu reads a slot's inner target and writes its outcome).
+struct SlotState {
+    // FP32 inner solve
+    double rz, initial, beta, alpha, residual_in, tol_in;
+    uint32_t its, max_its;
+    int32_t done, status_in;
+    // FP64 refinement
+    double r64_norm, b_norm, residual;
+    uint32_t used, outer;
+    int32_t status, outer_done;
+    int32_t inner_on, enabled;
+};
+
 // Device-side recurrence scalars of one PCG solve (FP64 or FP32 inner).
 struct PcgScalars {
     double rz[2];       // r . z of iteration k in slot k & 1

@@ -40,6 +40,9 @@ constexpr int kPThreads = 512;
 // shared memory per REV: K float4[3] + float2[3], (z, p_old) float4 + float2,
 // three delta words, the mass term and one flag byte
 constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 4 + 1;
+// REVs per block at most when a pool's slots are packed into waves
+// (1,536 x 113 B = 174 KB of shared memory, three REVs per thread)
+constexpr uint32_t kPoolBlockRevs = 1536;
 
 struct PersistArgs {
     uint32_t n;
@@ -62,6 +65,10 @@ struct PersistArgs {
     double tolerance;
     uint32_t max_iterations;
     unsigned long long spin_limit;
+    // pools: one row per block (first REV, REV count, slot, first block of the
+    // slot << 16 | blocks of the slot) and the slots' states; null for one scene
+    const uint4* blocks;
+    SlotState* st;
 };
 
 struct F3 {
@@ -83,7 +90,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     constexpr bool kPrefetch = R <= 2;
     extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
-    __shared__ double tot[3];
+    __shared__ double tot[4];
     __shared__ int s_ok;
     const uint32_t n = a.n, cap = a.cap, T = blockDim.x;
     float4* sK4 = smem4;                                       // [3][cap] owned bonds (xx, yy, zz, xy)
@@ -93,8 +100,24 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     uint32_t* sNB = reinterpret_cast<uint32_t*>(sZP2 + cap);   // [3][cap] neighbour deltas
     float* sM = reinterpret_cast<float*>(sNB + 3 * cap);       // [cap] m/h^2
     uint8_t* sFL = reinterpret_cast<uint8_t*>(sM + cap);       // [cap] free-axis flags
-    const uint32_t lo = blockIdx.x * cap;
-    const uint32_t cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
+    // this block's range and problem: the whole grid for one scene, or one
+    // slot's blocks in a pool (its own target, iteration cap and outcome)
+    uint32_t lo, cnt, slot = 0, fb = 0, nb = gridDim.x;
+    double scale_norm, tolerance;
+    uint32_t max_iterations;
+    bool mine = true;  // this block's problem still iterates
+    if (a.blocks) {
+        const uint4 bi = a.blocks[blockIdx.x];
+        lo = bi.x, cnt = bi.y, slot = bi.z, fb = bi.w >> 16, nb = bi.w & 0xFFFFu;
+        const SlotState& S = a.st[slot];
+        mine = S.enabled && S.inner_on;
+        scale_norm = S.r64_norm, tolerance = S.tol_in, max_iterations = S.max_its;
+        if (!mine) cnt = 0;
+    } else {
+        lo = blockIdx.x * cap;
+        cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
+        scale_norm = *a.scale_from, tolerance = a.tolerance, max_iterations = a.max_iterations;
+    }
 
     for (uint32_t li = threadIdx.x; li < cnt; li += T) {
         const size_t i = lo + li;
@@ -111,11 +134,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
 
     float x[R][3], r[R][3], p[R][3], ap[R][3];
     Sym<float> ireg[kPrefetch ? R : 1];
-    double scale = 1.0;
-    {
-        double rn = *a.scale_from;
-        scale = rn > 0.0 ? 1.0 / rn : 1.0;
-    }
+    const double scale = scale_norm > 0.0 ? 1.0 / scale_norm : 1.0;
     double acc[2] = {0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -139,34 +158,39 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     unsigned long long seq = 1;
     const int su[2] = {1, 2};
     const int sm[1] = {0};
-    double t2[2];
-    bool alive = grid_reduce<2>(acc, su, a, seq++, red, tot, &s_ok, t2);
+    constexpr int kActRow = 3;
+    double t2[2], act = 0.0;
+    bool alive = grid_reduce_ranged<2>(acc, mine ? 1.0 : 0.0, su, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t2,
+                                       &act);
     const double initial = sqrt(t2[1]);
     double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
     uint32_t its = 0;
     int32_t status = alive ? VX_OK : VX_TIMEOUT;
-    bool done = !alive;
-    if (alive) {
+    if (alive && mine) {
         if (!isfinite(t2[0]) || !isfinite(t2[1])) {
-            done = true;
+            mine = false;
             status = VX_NONFINITE;
         } else if (!(initial > 1e-12)) {
-            done = true;
-        } else if (a.max_iterations == 0) {
-            done = true;
+            mine = false;
+        } else if (max_iterations == 0) {
+            mine = false;
             status = VX_NOT_CONVERGED;
         }
     }
 
-    while (!done) {
+    // A problem that has stopped leaves its blocks idle; they keep taking part
+    // in the reductions until no block of the grid has work left, so every
+    // block leaves the loop at the same reduction.
+    while (alive) {
         const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
         // ---- matvec phase: p = z + beta p_old,
         //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
         double pap[1] = {0.0};
+        const uint32_t cnt_now = mine ? cnt : 0;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_now) continue;
             const uint32_t i = lo + li;
             int32_t dl[6];
 #pragma unroll
@@ -217,27 +241,29 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
 #pragma unroll
             for (int k = 0; k < R; ++k) {  // in flight during the wait below
                 const uint32_t li = threadIdx.x + k * T;
-                if (li < cnt) ireg[k] = load_sym(a.Dinv, n, lo + li);
+                if (li < cnt_now) ireg[k] = load_sym(a.Dinv, n, lo + li);
             }
         }
         double t1[1];
-        if (!grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1)) {
+        if (!grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t1, &act)) {
             status = VX_TIMEOUT;
             break;
         }
+        if (act == 0.0) break;  // no block of the grid has work left
         const double pap_all = t1[0];
-        if (!isfinite(pap_all) || pap_all <= 1e-30) {
+        if (mine && (!isfinite(pap_all) || pap_all <= 1e-30)) {
             its += 1;  // the matvec happened (src/solver.rs:1861-1866)
             if (!isfinite(pap_all)) status = VX_NONFINITE;
-            break;
+            mine = false;
         }
-        const float alpha = (float)(rz / pap_all);
+        const float alpha = mine ? (float)(rz / pap_all) : 0.f;
         // ---- update phase; every block has read the old (z, p_old): publish the new ----
         double au[2] = {0.0, 0.0};
+        const uint32_t cnt_up = mine ? cnt : 0;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_up) continue;
             const size_t i = lo + li;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -256,21 +282,23 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             au[0] += (double)dot3(rr, z);
             au[1] += (double)dot3(rr, rr);
         }
-        double tu[2];
-        if (!grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu)) {
+        double tu[2], act_u = 0.0;
+        if (!grid_reduce_ranged<2>(au, 0.0, su, kActRow, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u)) {
             status = VX_TIMEOUT;
             break;
         }
-        its += 1;
-        residual = sqrt(tu[1]) / initial;
-        if (!isfinite(tu[0]) || !isfinite(tu[1])) {
-            status = VX_NONFINITE;
-            done = true;
-        } else if (residual < a.tolerance) {
-            done = true;
-        } else if (its >= a.max_iterations) {
-            status = VX_NOT_CONVERGED;
-            done = true;
+        if (mine) {
+            its += 1;
+            residual = sqrt(tu[1]) / initial;
+            if (!isfinite(tu[0]) || !isfinite(tu[1])) {
+                status = VX_NONFINITE;
+                mine = false;
+            } else if (residual < tolerance) {
+                mine = false;
+            } else if (its >= max_iterations) {
+                status = VX_NOT_CONVERGED;
+                mine = false;
+            }
         }
         rz_prev = rz;
         rz = tu[0];
@@ -283,13 +311,24 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
         const size_t i = lo + li;
         a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        PcgScalars* sc = a.sc;
-        sc->iterations = its;
-        sc->residual = residual;
-        sc->initial = initial;
-        sc->status = status;
-        sc->done = 1;
+    if (threadIdx.x == 0 && blockIdx.x == fb) {
+        if (a.blocks) {
+            SlotState& S = a.st[slot];
+            if (S.enabled && S.inner_on) {
+                S.its = its;
+                S.residual_in = residual;
+                S.initial = initial;
+                S.status_in = status;
+                S.done = 1;
+            }
+        } else {
+            PcgScalars* sc = a.sc;
+            sc->iterations = its;
+            sc->residual = residual;
+            sc->initial = initial;
+            sc->status = status;
+            sc->done = 1;
+        }
     }
 }
 
@@ -352,6 +391,65 @@ bool persistent_plan(vx_scene* s) {
     return true;
 }
 
+uint32_t persistent_block_cap() { return kPoolBlockRevs; }
+
+// One cooperative launch of the persistent inner solve over the pool slots of
+// a wave: d_blocks holds one row per block (first REV, REV count, slot, first
+// block of the slot << 16 | the slot's blocks); each slot solves
+// A32 d = r64 / |r64| on its own REVs to its own inner target (SlotState) and
+// writes its outcome there. Blocks of slots that are not iterating are idle.
+int32_t solve_inner_slots(vx_scene* s, const uint4* d_blocks, SlotState* st, unsigned G, uint32_t cap) {
+    int dev = s->device, max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t smem = ((size_t)kBytesPerRev * cap + 15) & ~size_t(15);
+    if (cap == 0 || cap > 4u * kPThreads || G > (unsigned)s->sm_count || smem + 4096 > (size_t)max_smem) {
+        set_error("persistent pool PCG: a wave of %u blocks of %u REVs does not fit", G, cap);
+        return VX_BAD_INPUT;
+    }
+    PersistArgs a;
+    a.n = s->n;
+    a.cap = cap;
+    a.kn = kstride32(s->n);
+    a.flags = s->flags;
+    a.mh2 = s->mh2_32;
+    a.K = s->bonds.k32;
+    a.Dinv = s->dinv32;
+    a.code = s->nbcode;
+    a.src = s->r64;
+    a.scale_from = nullptr;
+    a.x = s->x32;
+    a.zp4 = reinterpret_cast<float4*>(s->zp32);
+    a.zp2 = reinterpret_cast<float2*>(s->zp32 + 4 * (size_t)s->n);
+    a.part = s->partials;
+    a.count = reinterpret_cast<unsigned long long*>(s->barrier);
+    a.err = reinterpret_cast<int32_t*>(s->barrier + 2);
+    a.sc = nullptr;
+    a.tolerance = 0.0;
+    a.max_iterations = 0;
+    a.blocks = d_blocks;
+    a.st = st;
+    a.spin_limit = 4000000ull;
+    if (const char* v = std::getenv("VXCOROT_BARRIER_SPINS")) {
+        unsigned long long lim = std::strtoull(v, nullptr, 10);
+        if (lim > 0 && lim < a.spin_limit) a.spin_limit = lim;
+    }
+    const unsigned R = (cap + kPThreads - 1) / kPThreads;
+    cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
+    if (e == cudaSuccess) {
+        switch (R <= 1 ? 1 : (R <= 2 ? 2 : 4)) {
+            case 1: e = launch_r<1>(a, G, smem, s->stream); break;
+            case 2: e = launch_r<2>(a, G, smem, s->stream); break;
+            default: e = launch_r<4>(a, G, smem, s->stream); break;
+        }
+    }
+    s->launches += 1;
+    if (e != cudaSuccess) {
+        set_error("persistent pool PCG launch failed: %s", cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    return VX_OK;
+}
+
 // One FP32 inner solve A32 d = r64 / |r64| in a single cooperative launch.
 int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations) {
     if (s->brick_ok) return solve_inner_brick(s, tolerance, max_iterations);
@@ -375,6 +473,8 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     a.sc = s->sc32;
     a.tolerance = tolerance;
     a.max_iterations = max_iterations;
+    a.blocks = nullptr;
+    a.st = nullptr;
     a.spin_limit = 4000000ull;  // ~1-2 s of polling at one reduction
     // VXCOROT_BARRIER_SPINS lowers the bound so a test can make the wait run out
     if (const char* v = std::getenv("VXCOROT_BARRIER_SPINS")) {

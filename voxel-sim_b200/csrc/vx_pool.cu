@@ -28,19 +28,6 @@
 
 namespace vx {
 
-// Per-slot device state of a pool pass.
-struct SlotState {
-    // FP32 inner solve
-    double rz, initial, beta, alpha, residual_in, tol_in;
-    uint32_t its, max_its;
-    int32_t done, status_in;
-    // FP64 refinement
-    double r64_norm, b_norm, residual;
-    uint32_t used, outer;
-    int32_t status, outer_done;
-    int32_t inner_on, enabled;
-};
-
 struct PoolArgs {
     uint32_t tiles;
     uint32_t slots;
@@ -79,6 +66,14 @@ struct vx_pool {
     vx::SlotState* h_st = nullptr;          // pinned [slots]
     int32_t* h_flag = nullptr;              // pinned [4]
     cudaGraphExec_t chunk = nullptr;
+    // the slots packed into waves of the persistent inner solve: block rows
+    // (first REV, REV count, slot, first block of the slot << 16 | its blocks)
+    // and per wave its first row, block count and largest block
+    bool waves_dirty = true;
+    bool waves_ok = false;
+    std::vector<uint4> wave_rows;
+    std::vector<uint4> waves;               // (first row, blocks, largest block, 0)
+    uint4* d_wave_rows = nullptr;
 };
 
 namespace vx {
@@ -451,6 +446,84 @@ int32_t pool_select(vx_pool* p, const uint8_t* enabled, std::vector<uint8_t>& on
     return VX_OK;
 }
 
+// Packs the occupied slots into waves of the persistent inner solve: a slot of
+// n REVs takes ceil(n / 1,536) blocks of equal size, slots go largest first to
+// the first wave with room (at most one block per SM), and each wave is one
+// cooperative launch. A slot's blocks and sums depend on its own size only, so
+// its iterates do not depend on which slots share its wave. The waves are
+// unavailable when the device has no cooperative launch or a neighbour delta
+// of the pool does not fit the kernel's 16-bit table.
+bool pool_waves(vx_pool* p) {
+    vx_scene* s = &p->s;
+    if (s->nbcode_state == 0) {  // once per topology (launch_reverse_neighbors resets it)
+        uint32_t bad = 0;
+        if (cudaMemcpyAsync(&bad, s->nbcode_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            return false;
+        s->nbcode_state = bad == 0 ? 1 : 2;
+    }
+    if (s->nbcode_state != 1) return false;
+    if (!p->waves_dirty) return p->waves_ok;
+    p->waves_dirty = false;
+    p->waves_ok = false;
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, s->device);
+    if (!coop) return false;
+    const uint32_t cap_max = persistent_block_cap();
+    const unsigned G_max = (unsigned)s->sm_count;
+    std::vector<uint32_t> order;
+    for (uint32_t k = 0; k < p->slots; ++k)
+        if (p->used[k] && p->rev_n[k]) order.push_back(k);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return p->rev_n[a] > p->rev_n[b]; });
+    struct Wave {
+        unsigned blocks = 0;
+        std::vector<uint32_t> slots;
+    };
+    std::vector<Wave> ws;
+    for (uint32_t k : order) {
+        const unsigned nb = (p->rev_n[k] + cap_max - 1) / cap_max;
+        if (nb > G_max || nb > 0xFFFFu) return false;
+        size_t w = 0;
+        while (w < ws.size() && ws[w].blocks + nb > G_max) ++w;
+        if (w == ws.size()) ws.emplace_back();
+        ws[w].blocks += nb;
+        ws[w].slots.push_back(k);
+    }
+    p->wave_rows.clear();
+    p->waves.clear();
+    for (const Wave& w : ws) {
+        const uint32_t first_row = (uint32_t)p->wave_rows.size();
+        uint32_t largest = 0, fb = 0;
+        for (uint32_t k : w.slots) {
+            const uint32_t n = p->rev_n[k], nb = (n + cap_max - 1) / cap_max, cap = (n + nb - 1) / nb;
+            const uint32_t base = p->first[k] * 256u;
+            for (uint32_t b = 0; b < nb; ++b) {
+                const uint32_t lo = b * cap, cnt = std::min(cap, n - lo);
+                p->wave_rows.push_back(make_uint4(base + lo, cnt, k, (fb << 16) | nb));
+                largest = std::max(largest, cnt);
+            }
+            fb += nb;
+        }
+        p->waves.push_back(make_uint4(first_row, w.blocks, largest, 0));
+    }
+    if (p->d_wave_rows) {
+        cudaStreamSynchronize(s->stream);
+        cudaFree(p->d_wave_rows);
+        p->d_wave_rows = nullptr;
+    }
+    if (p->wave_rows.empty()) return false;
+    if (cudaMalloc(&p->d_wave_rows, p->wave_rows.size() * sizeof(uint4)) != cudaSuccess) {
+        (void)cudaGetLastError();
+        p->d_wave_rows = nullptr;
+        return false;
+    }
+    if (cudaMemcpy(p->d_wave_rows, p->wave_rows.data(), p->wave_rows.size() * sizeof(uint4), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+        return false;
+    p->waves_ok = true;
+    return true;
+}
+
 int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint8_t>& on_slot, vx_pass_stats* out) {
     vx_scene* s = &p->s;
     cudaStream_t st = s->stream;
@@ -463,7 +536,14 @@ int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint
     }
     VX_POOL_TRY(cudaMemcpyAsync(p->st, p->h_st, p->slots * sizeof(SlotState), cudaMemcpyHostToDevice, st), "pool state");
     k_pool_zero<<<G, kThreads, 0, st>>>(P, s->x64, s->n);
-    VX_POOL_TRY(pool_chunk_graph(p, P), "pool graph capture");
+    // the inner solves: persistent waves (VX_KERNEL_AUTO / PERSISTENT) or the
+    // chunk graph of tile kernels (VX_KERNEL_STREAMING, or no waves)
+    const bool waves = prm->kernel != VX_KERNEL_STREAMING && pool_waves(p);
+    if (prm->kernel == VX_KERNEL_PERSISTENT && !waves) {
+        set_error("vx_pool_pass: the persistent inner solve is not available for this pool");
+        return VX_BAD_INPUT;
+    }
+    if (!waves) VX_POOL_TRY(pool_chunk_graph(p, P), "pool graph capture");
     IterArgs<double> a64 = pool_args64(s);
     const uint32_t outer_cap = P.max_outer + 2;
     for (uint32_t outer = 0; outer < outer_cap; ++outer) {
@@ -474,6 +554,22 @@ int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint
         VX_POOL_TRY(cudaMemcpyAsync(&p->h_flag[0], p->pending, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "pool");
         VX_POOL_TRY(cudaStreamSynchronize(st), "pool outer step");
         if (p->h_flag[0] == 0) break;
+        if (waves) {
+            for (const uint4& w : p->waves) {
+                int32_t r = solve_inner_slots(s, p->d_wave_rows + w.x, p->st, w.y, w.z);
+                if (r != VX_OK) return r;
+            }
+            VX_POOL_TRY(cudaMemcpyAsync(&p->h_flag[3], s->barrier + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+                        "pool");
+            VX_POOL_TRY(cudaStreamSynchronize(st), "pool inner solve");
+            if (p->h_flag[3]) {
+                set_error("persistent pool PCG: a grid barrier wait ran out");
+                return VX_TIMEOUT;
+            }
+            k_pool_accumulate<<<G, kThreads, 0, st>>>(P, s->x64, s->x32, s->n);
+            s->launches += 1;
+            continue;
+        }
         VX_POOL_TRY(cudaMemsetAsync(p->active, 0, sizeof(int32_t), st), "pool");
         k_pool_init<<<G, kThreads, 0, st>>>(pool_args32(s, 0), P, s->r64);
         k_pool_scal_init<<<GS, 256, 0, st>>>(P);
@@ -629,6 +725,7 @@ int32_t vx_pool_destroy(vx_pool* p) {
     cudaSetDevice(p->s.device);
     if (p->s.stream) cudaStreamSynchronize(p->s.stream);
     if (p->chunk) cudaGraphExecDestroy(p->chunk);
+    if (p->d_wave_rows) cudaFree(p->d_wave_rows);
     if (p->extra) cudaFree(p->extra);
     if (p->h_st) cudaFreeHost(p->h_st);
     if (p->h_flag) cudaFreeHost(p->h_flag);
@@ -795,6 +892,7 @@ int32_t vx_pool_add(vx_pool* p, const vx_scene_desc* d, uint32_t* out_slot) {
     p->count[slot] = need;
     p->rev_n[slot] = n;
     p->used[slot] = 1;
+    p->waves_dirty = true;
     *out_slot = slot;
     return VX_OK;
 }
@@ -817,6 +915,7 @@ int32_t vx_pool_remove(vx_pool* p, uint32_t slot) {
     for (uint32_t t = p->first[slot]; t < p->first[slot] + p->count[slot]; ++t) p->owner[t] = VX_EMPTY_U32;
     p->used[slot] = 0;
     p->rev_n[slot] = 0;
+    p->waves_dirty = true;
     return VX_OK;
 }
 

@@ -33,8 +33,9 @@ class BatchedSolve:
     from the state saved at construction."""
 
     def __init__(self, ctx: N.Context, scenes, h: float = 1e-3, tolerance: float = 1e-8,
-                 max_iterations: int = 20000):
+                 max_iterations: int = 20000, kernel: int = N.KERNEL_AUTO):
         self.scenes = scenes
+        self.kernel = kernel
         self.pool = N.DevicePool(ctx, pool_capacity(scenes), len(scenes))
         self.slots = [self.pool.add(s) for s in scenes]
         self.h, self.tolerance, self.max_iterations = h, tolerance, max_iterations
@@ -47,7 +48,7 @@ class BatchedSolve:
     def solve(self):
         self.pool.restore_state()
         self.pool.fit_rotations()
-        status, stats = self.pool.corotational_pass(self.h, self.tolerance, self.max_iterations)
+        status, stats = self.pool.corotational_pass(self.h, self.tolerance, self.max_iterations, kernel=self.kernel)
         return status, [stats[k] for k in self.slots]
 
     def close(self):

@@ -753,10 +753,13 @@ class DevicePool:
         return out
 
     def corotational_pass(self, h, tolerance, max_iterations, enabled=None, reuse=False, inner_tolerance=0.0,
-                          max_outer=0, allow=(VX_NOT_CONVERGED,)):
+                          max_outer=0, kernel=KERNEL_AUTO, allow=(VX_NOT_CONVERGED,)):
+        """One pass of every selected slot. kernel: KERNEL_AUTO / KERNEL_PERSISTENT
+        solve the slots in waves of the persistent kernel, KERNEL_STREAMING with
+        the tile kernels."""
         m = self._mask(enabled)
         p = VxPassParams(h, tolerance, max_iterations, PRECISION_MIXED, int(reuse), inner_tolerance, max_outer,
-                         KERNEL_AUTO)
+                         kernel)
         stats = (VxPassStats * self.slots)()
         status = check(load().vx_pool_pass(self.h, _p(m, C.c_uint8), C.byref(p), stats), allow=allow)
         return status, [stats[k].as_dict() for k in range(self.slots)]
