@@ -59,7 +59,7 @@ def parse():
                     help="served: skip the plain FP64 single-scene solves of the template scenes")
     ap.add_argument("--scenes", type=int, default=512, help="batched: scenes per batch")
     ap.add_argument("--pool-kernel", default="auto", choices=["auto", "persistent", "streaming"],
-                    help="batched: inner solves in persistent waves (auto, persistent) or tile kernels")
+                    help="batched: inner solves in tile kernels (auto, streaming) or persistent waves")
     ap.add_argument("--fp64-sample", type=int, default=None,
                     help="batched: scenes timed in the plain FP64 single-scene form (default all)")
     ap.add_argument("--edge", type=int, default=None)

@@ -536,9 +536,12 @@ int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint
     }
     VX_POOL_TRY(cudaMemcpyAsync(p->st, p->h_st, p->slots * sizeof(SlotState), cudaMemcpyHostToDevice, st), "pool state");
     k_pool_zero<<<G, kThreads, 0, st>>>(P, s->x64, s->n);
-    // the inner solves: persistent waves (VX_KERNEL_AUTO / PERSISTENT) or the
-    // chunk graph of tile kernels (VX_KERNEL_STREAMING, or no waves)
-    const bool waves = prm->kernel != VX_KERNEL_STREAMING && pool_waves(p);
+    // the inner solves: persistent waves (VX_KERNEL_PERSISTENT) or the chunk
+    // graph of tile kernels (VX_KERNEL_AUTO / STREAMING). The waves run one after
+    // another, each as long as its slowest slot, where the tile kernels advance
+    // every slot at once; on the batched workload the tile kernels measured
+    // faster, so they are the default.
+    const bool waves = prm->kernel == VX_KERNEL_PERSISTENT && pool_waves(p);
     if (prm->kernel == VX_KERNEL_PERSISTENT && !waves) {
         set_error("vx_pool_pass: the persistent inner solve is not available for this pool");
         return VX_BAD_INPUT;

@@ -620,6 +620,7 @@ def _bind_pool(L):
                  "vx_pool_set_previous", "vx_pool_get_previous"):
         getattr(L, name).argtypes = [C.c_void_p, C.c_uint32, f64p]
     L.vx_pool_set_targets.argtypes = [C.c_void_p, C.c_uint32, u8p, f64p]
+    L.vx_pool_advance_targets.argtypes = [C.c_void_p, u8p, f64p]
     L.vx_pool_fit_rotations.argtypes = [C.c_void_p, u8p, f64p]
     L.vx_pool_pass.argtypes = [C.c_void_p, u8p, C.POINTER(VxPassParams), C.POINTER(VxPassStats)]
     L.vx_pool_bond_stress.argtypes = [C.c_void_p, C.c_uint32, f32p, f32p, u32p, C.c_uint32, u32p]
@@ -693,6 +694,13 @@ class DevicePool:
         check(load().vx_pool_get_rotations(self.h, slot, _p(out, C.c_double)))
         return out.reshape(-1, 4)
 
+    def advance_targets(self, delta, enabled=None):
+        """Moves the targets marked VX_TARGET_MOVING of every selected slot by
+        delta[slot] (slots x 3 metres)."""
+        m = self._mask(enabled)
+        d = np.ascontiguousarray(delta, np.float64).reshape(-1)
+        check(load().vx_pool_advance_targets(self.h, _p(m, C.c_uint8), _p(d, C.c_double)))
+
     def set_targets(self, slot, mask, target=None):
         m = np.ascontiguousarray(mask, np.uint8)
         t = None if target is None else self._v(target)
@@ -754,9 +762,9 @@ class DevicePool:
 
     def corotational_pass(self, h, tolerance, max_iterations, enabled=None, reuse=False, inner_tolerance=0.0,
                           max_outer=0, kernel=KERNEL_AUTO, allow=(VX_NOT_CONVERGED,)):
-        """One pass of every selected slot. kernel: KERNEL_AUTO / KERNEL_PERSISTENT
-        solve the slots in waves of the persistent kernel, KERNEL_STREAMING with
-        the tile kernels."""
+        """One pass of every selected slot. kernel: KERNEL_PERSISTENT solves the
+        slots in waves of the persistent kernel, KERNEL_AUTO / KERNEL_STREAMING
+        with the tile kernels."""
         m = self._mask(enabled)
         p = VxPassParams(h, tolerance, max_iterations, PRECISION_MIXED, int(reuse), inner_tolerance, max_outer,
                          kernel)
