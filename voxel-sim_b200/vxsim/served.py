@@ -145,30 +145,36 @@ def run_served(ctx: N.Context, rate: float = 200.0, duration: float = 5.0, steps
     }
 
 
-def fp64_single_scene_rate(ctx: N.Context, scenes, h: float = 1e-3, tolerance: float = 1e-8,
-                           gravity=(0.0, 0.0, -9.81)) -> dict:
-    """The plain FP64 single-scene form on the given scenes: each one resident
-    alone, its first substep's pass (prediction under gravity from rest,
-    rotation fit, assembly, FP64 block-Jacobi PCG to `tolerance`) solved once
-    to warm it, then timed once with CUDA events on its stream."""
+def single_scene_step_rate(ctx: N.Context, templates, precision: int, steps: int = 4, tolerance: float = 1e-8,
+                           blade_speed: float = 1.0, blade: str = "contact") -> dict:
+    """The single-scene form on the served requests' own steps: each template
+    (scene, moving mask) resident alone, stepped `steps` times as a request
+    is (prediction under gravity, two corotational passes, contact and
+    fracture with the blade advancing 1 mm per step), timed with CUDA events on
+    the scene's stream around each step. Per template: seconds and solves."""
     import torch
-    times, worst = [], 0.0
-    for s in scenes:
-        pred = S.predict_from_rest(s, h, gravity)
+    real = blade == "contact"
+    params = N.step_params(1e-3, substeps=1, corotation_iterations=2, corotation_tolerance=1e-5,
+                           gravity=(0.0, 0.0, -9.81), tolerance=tolerance, max_iterations=200000,
+                           precision=precision, fracture=real, contact=real)
+    out = []
+    for s, moving in templates:
         d = N.DeviceScene(ctx, s)
-        d.set_predicted(pred)
-        d.save_state()
-        for timed in (False, True):
-            d.restore_state()
-            ext = torch.cuda.ExternalStream(d.stream_ptr)
+        mask = np.ascontiguousarray(s.target_mask, np.uint8)
+        target = np.array(s.target, np.float64)
+        ext = torch.cuda.ExternalStream(d.stream_ptr)
+        secs, solves, worst = 0.0, 0, 0.0
+        for _ in range(steps):
+            target[np.asarray(moving, bool), 2] -= blade_speed * 1e-3
+            d.set_targets(mask, target)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(ext)
-            d.fit_rotations()
-            st = d.corotational_pass(h, tolerance, 200000, precision=N.PRECISION_FP64)
+            st = d.step(params)
             e1.record(ext)
             e1.synchronize()
-            if timed:
-                times.append(e0.elapsed_time(e1) / 1000.0)
-                worst = max(worst, st["true_residual"])
+            secs += e0.elapsed_time(e1) / 1000.0
+            solves += st["passes"]
+            worst = max(worst, st["residual"])
         d.close()
-    return {"seconds": times, "worst_true_residual": worst}
+        out.append({"n": s.n, "seconds": secs, "solves": solves, "worst_residual": worst})
+    return out
