@@ -64,7 +64,10 @@ def parse():
                     help="batched: scenes timed in the plain FP64 single-scene form (default all)")
     ap.add_argument("--edge", type=int, default=None)
     ap.add_argument("--passes", type=int, default=None)
-    ap.add_argument("--tolerance", type=float, default=1e-8)
+    ap.add_argument("--tolerance", type=float, default=None,
+                    help="pass target (default: the workload's, 1e-8; 1e-10 for the wood cube)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="the FP32-inner / FP64-refinement form, or the plain FP64 form")
     ap.add_argument("--inner-tolerance", type=float, default=0.0,
                     help="relative tolerance of each FP32 inner solve (0 = the library's default)")
     ap.add_argument("--max-iterations", type=int, default=50000)
@@ -81,7 +84,10 @@ def parse():
                     help="skip the streaming matvec timing on the 160^3 damaged lattice")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.tolerance is None:
+        a.tolerance = 1e-10 if a.workload == "wood_cube" else 1e-8
+    return a
 
 
 def build_workload(name, edge, seed):
@@ -292,7 +298,7 @@ def our_arm(args):
     pred = predicted_positions(scene, h, meta["gravity"])
     free_dof = int(scene.free_mask().sum())
     active = scene.active_count()
-    precision = N.PRECISION_MIXED
+    precision = N.PRECISION_FP64 if args.precision == "fp64" else N.PRECISION_MIXED
 
     ctx = N.Context(local)
     ds = N.DeviceScene(ctx, scene)
@@ -362,8 +368,9 @@ def our_arm(args):
     warm = ds.kernel_times(precision, reps=20)
     peak, peak_kind = measured_peak()
     prof = profiled_traffic() or {}
-    mv_bytes = BYTES_PER_REV["matvec_f32"] * active
-    up_bytes = BYTES_PER_REV["update_f32"] * active
+    fp64 = precision == N.PRECISION_FP64
+    mv_bytes = BYTES_PER_REV["matvec_f64" if fp64 else "matvec_f32"] * active
+    up_bytes = BYTES_PER_REV["update_f64" if fp64 else "update_f32"] * active
     streaming = {"matvec_us_cold_l2": cold["matvec_us"], "matvec_us_warm_l2": warm["matvec_us"],
                  "update_us_cold_l2": cold["update_us"], "update_us_warm_l2": warm["update_us"],
                  "matvec_gbs_cold_l2": mv_bytes / (cold["matvec_us"] * 1e-6) / 1e9,
@@ -393,7 +400,7 @@ def our_arm(args):
                 "so HBM traffic per iteration is far below the streamed algorithmic bytes")
     else:
         achieved = streaming["matvec_gbs_cold_l2"]
-        kernel = "k_matvec<float>"
+        kernel = "k_matvec<double>" if fp64 else "k_matvec<float>"
         bytes_per_launch = mv_bytes
         launch_us = cold["matvec_us"]
         # the capture nearest in size: whether the inputs fit L2 changes the bytes per REV
@@ -401,6 +408,8 @@ def our_arm(args):
         near = min(caps, key=lambda c: abs(math.log(c["revs"] / max(scene.n, 1))), default=None)
         traffic = near["bytes_per_rev"] * scene.n if near else None
         note = "streaming matvec launched alone after an L2 flush"
+        if fp64:
+            traffic = None  # the profiled captures are of the FP32 matvec
 
     # the step's first pass against the plain FP64 form solved to 1e-12 on the same
     # system (that form matches the C oracle to 1e-10 on the 10^3 wood cube)
@@ -491,12 +500,14 @@ def our_arm(args):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "DOF-iter/s", "n_gpus": world, "steps": args.steps,
+            "metric": "PCG DOF-iters/s (plain FP64 PCG)" if fp64 else METRIC, "value": value,
+            "unit": "DOF-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
             "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n,
                        "dof_nominal": 3 * scene.n, "dof_active": free_dof, "passes": passes,
-                       "tolerance": args.tolerance, "precision": "FP32 inner PCG, FP64 refinement",
+                       "tolerance": args.tolerance,
+                       "precision": "plain FP64 PCG" if fp64 else "FP32 inner PCG, FP64 refinement",
                        "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
             "solves_per_s": job_solves / (job_ms / 1000.0),
             "iterations_per_solve": total_it / (passes * args.steps),
