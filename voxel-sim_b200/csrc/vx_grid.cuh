@@ -97,7 +97,10 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
 // own problem, in block order, and `act` over all G blocks (a count of blocks
 // still at work, which tells every block when to stop). With fb = 0 and nb = G
 // the NV sums are grid_reduce's bits. Partial rows: slot[k] for the NV values,
-// act_row for act; A as for grid_reduce.
+// act_row for act (act_row < 0: no act value). A row may only be written again
+// by a reduction that has a grid barrier between it and this one's reads: a
+// block past this barrier could otherwise overwrite a row another block has
+// not read yet. A as for grid_reduce.
 template <int NV, class A>
 __device__ __forceinline__ bool grid_reduce_ranged(double (&v)[NV], double act, const int (&slot)[NV], int act_row,
                                                    const A& a, unsigned long long seq, uint32_t fb, uint32_t nb,
@@ -119,7 +122,7 @@ __device__ __forceinline__ bool grid_reduce_ranged(double (&v)[NV], double act, 
         if (lane == 0) {
 #pragma unroll
             for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
-            a.part[(size_t)act_row * G + blockIdx.x] = act;
+            if (act_row >= 0) a.part[(size_t)act_row * G + blockIdx.x] = act;
             red_release_add_u64(a.count, 1ull);
             const unsigned long long target = seq * G;
             unsigned long long spins = 0;
@@ -142,7 +145,8 @@ __device__ __forceinline__ bool grid_reduce_ranged(double (&v)[NV], double act, 
 #pragma unroll
                 for (int k = 0; k < NV; ++k) t[k] += __ldcg(a.part + (size_t)slot[k] * G + fb + blk);
             }
-            for (unsigned blk = lane; blk < G; blk += 32) ta += __ldcg(a.part + (size_t)act_row * G + blk);
+            if (act_row >= 0)
+                for (unsigned blk = lane; blk < G; blk += 32) ta += __ldcg(a.part + (size_t)act_row * G + blk);
         }
 #pragma unroll
         for (int k = 0; k < NV; ++k) t[k] = warp_sum(t[k]);

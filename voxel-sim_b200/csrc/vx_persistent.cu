@@ -160,8 +160,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     const int sm[1] = {0};
     constexpr int kActRow = 3;
     double t2[2], act = 0.0;
-    bool alive = grid_reduce_ranged<2>(acc, mine ? 1.0 : 0.0, su, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t2,
-                                       &act);
+    // only the matvec-phase reductions carry the count of working blocks (row
+    // kActRow): two of them always have a reduction, so a grid barrier, between
+    bool alive = grid_reduce_ranged<2>(acc, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, t2, &act);
     const double initial = sqrt(t2[1]);
     double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
     uint32_t its = 0;
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             au[1] += (double)dot3(rr, rr);
         }
         double tu[2], act_u = 0.0;
-        if (!grid_reduce_ranged<2>(au, 0.0, su, kActRow, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u)) {
+        if (!grid_reduce_ranged<2>(au, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u)) {
             status = VX_TIMEOUT;
             break;
         }
