@@ -710,9 +710,13 @@ int32_t vx_pool_create(vx_ctx* ctx, uint64_t max_revs, uint32_t max_slots, vx_po
     p->angle = (unsigned long long*)(p->extra + o_ang);
     p->s.max_angle_bits = p->angle;
     p->s.pool_slots = max_slots;
-    // the free arena is inert: no tile is on and every tile maps to no slot
+    // the free arena is inert: no tile is on, every tile maps to no slot, and no
+    // REV has a neighbour (a zeroed table would bond every free REV to REV 0
+    // and give REV 0 a reverse neighbour picked by whichever write lands last)
     std::vector<uint32_t> ts(p->tiles, VX_EMPTY_U32);
     e = cudaMemcpyAsync(p->s.tile_scene, ts.data(), p->tiles * 4, cudaMemcpyHostToDevice, p->s.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->s.nbr, 0xFF, 3 * (size_t)p->s.n * sizeof(uint32_t), p->s.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->s.rev, 0xFF, 3 * (size_t)p->s.n * sizeof(uint32_t), p->s.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->s.stream);
     if (e != cudaSuccess) {
         set_error("vx_pool_create: %s", cudaGetErrorString(e));
@@ -910,6 +914,11 @@ int32_t vx_pool_remove(vx_pool* p, uint32_t slot) {
     std::vector<uint32_t> ts(p->count[slot], VX_EMPTY_U32);
     cudaError_t e = cudaMemcpyAsync(p->s.tile_scene + p->first[slot], ts.data(), ts.size() * 4, cudaMemcpyHostToDevice,
                                     p->s.stream);
+    // the freed tiles lose their bonds again, and the reverse table forgets them
+    const size_t base = (size_t)p->first[slot] * 256, m = (size_t)p->count[slot] * 256, C = p->s.n;
+    for (int a = 0; a < 3 && e == cudaSuccess; ++a)
+        e = cudaMemsetAsync(p->s.nbr + a * C + base, 0xFF, m * sizeof(uint32_t), p->s.stream);
+    if (e == cudaSuccess) e = launch_reverse_neighbors(&p->s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(p->s.stream);
     if (e != cudaSuccess) {
         set_error("vx_pool_remove: %s", cudaGetErrorString(e));
