@@ -179,10 +179,13 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
         }
     }
 
-    // A problem that has stopped leaves its blocks idle; they keep taking part
-    // in the reductions until no block of the grid has work left, so every
-    // block leaves the loop at the same reduction.
+    // A problem that has stopped leaves its blocks idle; in a pool they keep
+    // taking part in the reductions until no block of the grid has work left,
+    // so every block leaves the loop at the same reduction. One scene is one
+    // problem: its blocks leave together as soon as it stops.
+    const bool multi = a.blocks != nullptr;
     while (alive) {
+        if (!multi && !mine) break;
         const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
         // ---- matvec phase: p = z + beta p_old,
         //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
@@ -246,16 +249,18 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             }
         }
         double t1[1];
-        if (!grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t1, &act)) {
+        if (!grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, multi ? kActRow : -1, a, seq++, fb, nb, red, tot,
+                                   &s_ok, t1, &act)) {
             status = VX_TIMEOUT;
             break;
         }
-        if (act == 0.0) break;  // no block of the grid has work left
+        if (multi && act == 0.0) break;  // no block of the grid has work left
         const double pap_all = t1[0];
         if (mine && (!isfinite(pap_all) || pap_all <= 1e-30)) {
             its += 1;  // the matvec happened (src/solver.rs:1861-1866)
             if (!isfinite(pap_all)) status = VX_NONFINITE;
             mine = false;
+            if (!multi) break;
         }
         const float alpha = mine ? (float)(rz / pap_all) : 0.f;
         // ---- update phase; every block has read the old (z, p_old): publish the new ----
