@@ -85,7 +85,9 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y
 // registers before the grid wait of the matvec phase, so its L2 latency
 // overlaps the wait; at R = 4 the registers are not there and it is loaded
 // where used.
-template <int R>
+// MULTI: the blocks work for several pool slots (a.blocks, a.st); otherwise
+// for one scene, whose reductions are grid_reduce's.
+template <int R, bool MULTI>
 __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) {
     constexpr bool kPrefetch = R <= 2;
     extern __shared__ float4 smem4[];
@@ -106,7 +108,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     double scale_norm, tolerance;
     uint32_t max_iterations;
     bool mine = true;  // this block's problem still iterates
-    if (a.blocks) {
+    if constexpr (MULTI) {
         const uint4 bi = a.blocks[blockIdx.x];
         lo = bi.x, cnt = bi.y, slot = bi.z, fb = bi.w >> 16, nb = bi.w & 0xFFFFu;
         const SlotState& S = a.st[slot];
@@ -162,7 +164,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     double t2[2], act = 0.0;
     // only the matvec-phase reductions carry the count of working blocks (row
     // kActRow): two of them always have a reduction, so a grid barrier, between
-    bool alive = grid_reduce_ranged<2>(acc, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, t2, &act);
+    bool alive;
+    if constexpr (MULTI) alive = grid_reduce_ranged<2>(acc, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, t2, &act);
+    else alive = grid_reduce<2>(acc, su, a, seq++, red, tot, &s_ok, t2);
     const double initial = sqrt(t2[1]);
     double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
     uint32_t its = 0;
@@ -183,9 +187,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     // taking part in the reductions until no block of the grid has work left,
     // so every block leaves the loop at the same reduction. One scene is one
     // problem: its blocks leave together as soon as it stops.
-    const bool multi = a.blocks != nullptr;
     while (alive) {
-        if (!multi && !mine) break;
+        if (!MULTI && !mine) break;
         const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
         // ---- matvec phase: p = z + beta p_old,
         //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
@@ -249,18 +252,22 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             }
         }
         double t1[1];
-        if (!grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, multi ? kActRow : -1, a, seq++, fb, nb, red, tot,
-                                   &s_ok, t1, &act)) {
+        bool ok_a;
+        if constexpr (MULTI)
+            ok_a = grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t1, &act);
+        else
+            ok_a = grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1);
+        if (!ok_a) {
             status = VX_TIMEOUT;
             break;
         }
-        if (multi && act == 0.0) break;  // no block of the grid has work left
+        if (MULTI && act == 0.0) break;  // no block of the grid has work left
         const double pap_all = t1[0];
         if (mine && (!isfinite(pap_all) || pap_all <= 1e-30)) {
             its += 1;  // the matvec happened (src/solver.rs:1861-1866)
             if (!isfinite(pap_all)) status = VX_NONFINITE;
             mine = false;
-            if (!multi) break;
+            if (!MULTI) break;
         }
         const float alpha = mine ? (float)(rz / pap_all) : 0.f;
         // ---- update phase; every block has read the old (z, p_old): publish the new ----
@@ -289,7 +296,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             au[1] += (double)dot3(rr, rr);
         }
         double tu[2], act_u = 0.0;
-        if (!grid_reduce_ranged<2>(au, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u)) {
+        bool ok_b;
+        if constexpr (MULTI) ok_b = grid_reduce_ranged<2>(au, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u);
+        else ok_b = grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu);
+        if (!ok_b) {
             status = VX_TIMEOUT;
             break;
         }
@@ -318,7 +328,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
         a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
     }
     if (threadIdx.x == 0 && blockIdx.x == fb) {
-        if (a.blocks) {
+        if constexpr (MULTI) {
             SlotState& S = a.st[slot];
             if (S.enabled && S.inner_on) {
                 S.its = its;
@@ -338,13 +348,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     }
 }
 
-template <int R>
+template <int R, bool MULTI>
 cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_pcg_persistent<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_pcg_persistent<R, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     PersistArgs args = a;
     void* params[] = {&args};
-    return cudaLaunchCooperativeKernel((void*)k_pcg_persistent<R>, dim3(G), dim3(kPThreads), params, smem, st);
+    return cudaLaunchCooperativeKernel((void*)k_pcg_persistent<R, MULTI>, dim3(G), dim3(kPThreads), params, smem, st);
 }
 
 }  // namespace
@@ -443,9 +454,9 @@ int32_t solve_inner_slots(vx_scene* s, const uint4* d_blocks, SlotState* st, uns
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
     if (e == cudaSuccess) {
         switch (R <= 1 ? 1 : (R <= 2 ? 2 : 4)) {
-            case 1: e = launch_r<1>(a, G, smem, s->stream); break;
-            case 2: e = launch_r<2>(a, G, smem, s->stream); break;
-            default: e = launch_r<4>(a, G, smem, s->stream); break;
+            case 1: e = launch_r<1, true>(a, G, smem, s->stream); break;
+            case 2: e = launch_r<2, true>(a, G, smem, s->stream); break;
+            default: e = launch_r<4, true>(a, G, smem, s->stream); break;
         }
     }
     s->launches += 1;
@@ -490,9 +501,9 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
     if (e == cudaSuccess) {
         switch (s->persist_R) {
-            case 1: e = launch_r<1>(a, s->persist_G, s->persist_smem, s->stream); break;
-            case 2: e = launch_r<2>(a, s->persist_G, s->persist_smem, s->stream); break;
-            default: e = launch_r<4>(a, s->persist_G, s->persist_smem, s->stream); break;
+            case 1: e = launch_r<1, false>(a, s->persist_G, s->persist_smem, s->stream); break;
+            case 2: e = launch_r<2, false>(a, s->persist_G, s->persist_smem, s->stream); break;
+            default: e = launch_r<4, false>(a, s->persist_G, s->persist_smem, s->stream); break;
         }
     }
     s->launches += 1;
