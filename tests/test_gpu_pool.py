@@ -134,10 +134,10 @@ def test_pool_bond_stress_matches_single_scene(ctx):
     pool.close()
 
 
-def step_params():
+def step_params(kernel=N.KERNEL_AUTO):
     return N.step_params(1e-3, substeps=2, corotation_iterations=3, corotation_tolerance=1e-6,
                          gravity=(0.0, 0.0, -9.81), tolerance=TOL, max_iterations=CAP,
-                         precision=N.PRECISION_MIXED)
+                         precision=N.PRECISION_MIXED, kernel=kernel)
 
 
 def test_pool_step_matches_single_scene_steps(ctx):
@@ -170,13 +170,16 @@ def test_pool_step_matches_single_scene_steps(ctx):
     pool.close()
 
 
-def test_pool_step_is_bit_identical_alone_and_in_a_mix(ctx):
+@pytest.mark.parametrize("kernel", [N.KERNEL_AUTO, N.KERNEL_PERSISTENT])
+def test_pool_step_is_bit_identical_alone_and_in_a_mix(ctx, kernel):
     """A scene stepped alone in a pool and the same scene stepped together
     with others (admitted at a different slot and tile range) end with the
-    same bits after three steps, velocities included."""
+    same bits after three steps, velocities included: with the tile kernels,
+    and with persistent waves, where the others also change the wave's
+    largest block (one kernel instantiation serves every wave for this)."""
     sc = scenes()
     target = sc[2]
-    p = step_params()
+    p = step_params(kernel)
     alone = N.DevicePool(ctx, target.n + 4096, 4)
     ka = alone.add(target)
     mixed = N.DevicePool(ctx, sum(s.n for s in sc) + 4096, 8)

@@ -450,15 +450,11 @@ int32_t solve_inner_slots(vx_scene* s, const uint4* d_blocks, SlotState* st, uns
         unsigned long long lim = std::strtoull(v, nullptr, 10);
         if (lim > 0 && lim < a.spin_limit) a.spin_limit = lim;
     }
-    const unsigned R = (cap + kPThreads - 1) / kPThreads;
+    // one instantiation for every wave: the compiler schedules and contracts the
+    // arithmetic of k_pcg_persistent<1>, <2> and <4> differently, and a slot's
+    // bits must not depend on the largest block of the wave it lands in
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
-    if (e == cudaSuccess) {
-        switch (R <= 1 ? 1 : (R <= 2 ? 2 : 4)) {
-            case 1: e = launch_r<1, true>(a, G, smem, s->stream); break;
-            case 2: e = launch_r<2, true>(a, G, smem, s->stream); break;
-            default: e = launch_r<4, true>(a, G, smem, s->stream); break;
-        }
-    }
+    if (e == cudaSuccess) e = launch_r<4, true>(a, G, smem, s->stream);
     s->launches += 1;
     if (e != cudaSuccess) {
         set_error("persistent pool PCG launch failed: %s", cudaGetErrorString(e));
