@@ -105,6 +105,16 @@ def predicted_positions(scene, h, gravity):
     return S.predict_from_rest(scene, h, gravity)
 
 
+def workload_config(args, scene, world):
+    """The `config` of a workload's line, the same in both arms."""
+    meta = scene.meta
+    return {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n,
+            "dof_nominal": 3 * scene.n, "dof_active": int(scene.free_mask().sum()),
+            "passes": args.passes or meta["passes"], "tolerance": args.tolerance,
+            "precision": "plain FP64 PCG" if args.precision == "fp64" else "FP32 inner PCG, FP64 refinement",
+            "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"}
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -249,10 +259,11 @@ def reference_arm(args):
               f"(src/solver.rs:1833-1911, restated in C, f32 vectors, f64 dots) on pass 0 of {meta['workload']} "
               f"{meta.get('edge')}^3 ({rows['n']} active REVs)")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "DOF-iter/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": "PCG DOF-iters/s (plain FP64 PCG)" if args.precision == "fp64" else METRIC,
+        "value": value, "unit": "DOF-iter/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n, "dof_active": dof},
+        "config": workload_config(args, scene, args.gpus),
         "cpu_baseline": {"value": value, "unit": "DOF-iter/s", "cores": threads, "kind": "port", "sample": sample,
                          "omp_num_threads": threads, "host_cpus": os.cpu_count()},
         "e2e": {"value": value, "unit": "DOF-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -504,11 +515,7 @@ def our_arm(args):
             "unit": "DOF-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if fp64 else "f32+f64", "data": "synthetic",
-            "config": {"workload": f"{meta['workload']} {meta.get('edge')}^3", "revs": scene.n,
-                       "dof_nominal": 3 * scene.n, "dof_active": free_dof, "passes": passes,
-                       "tolerance": args.tolerance,
-                       "precision": "plain FP64 PCG" if fp64 else "FP32 inner PCG, FP64 refinement",
-                       "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"},
+            "config": workload_config(args, scene, world),
             "solves_per_s": job_solves / (job_ms / 1000.0),
             "iterations_per_solve": total_it / (passes * args.steps),
             "worst_true_residual": worst,
