@@ -321,9 +321,9 @@ def test_persistent_kernels_agree_at_full_grid(ctx, edge):
 @pytest.mark.parametrize("edge", [24, 64])
 def test_brick_and_range_forms_agree(ctx, edge, monkeypatch):
     """The brick plan (Chronopoulos-Gear recurrence, one grid reduction per
-    iteration) is the form the scene takes; the contiguous-range plan (classic
-    recurrence, two reductions) is forced with VXCOROT_PERSISTENT=range. Both
-    reach the FP64 target over three passes and agree to the solve error."""
+    iteration, VXCOROT_PERSISTENT=brick) and the contiguous-range plan (classic
+    recurrence, two reductions, VXCOROT_PERSISTENT=range) both reach the FP64
+    target over three passes and agree to the solve error."""
     s = S.mixed_block(edge, seed=3)
     out, iters = {}, {}
     for form in ("brick", "range"):
@@ -342,6 +342,29 @@ def test_brick_and_range_forms_agree(ctx, edge, monkeypatch):
     print(f"{edge}^3 inner iterations over 3 passes: brick {iters['brick']}, range {iters['range']}")
     assert rel(out["brick"], out["range"]) < 2e-5
     assert abs(iters["brick"] - iters["range"]) <= 0.05 * iters["range"] + 16
+
+
+def test_wide_plate_takes_the_brick_form(ctx, monkeypatch):
+    """A 184 x 184 x 3 plate: its z-neighbour delta (33,856) does not fit the
+    range plan's int16 deltas, so the untuned persistent solve takes the brick
+    plan, and its result matches the streaming kernels'."""
+    monkeypatch.delenv("VXCOROT_PERSISTENT", raising=False)
+    cells = S.grid_cells(184, 184, 3)
+    s = S.from_cells(cells, 1, S.wood_config_materials(), anisotropy=1.0)
+    s.fix_voxels(np.nonzero(cells[:, 2] == 0)[0])
+    free = s.kinematic == 0
+    s.loads[free] = np.random.default_rng(4).normal(0.0, 0.05, size=(int(free.sum()), 3))
+    out = {}
+    for kernel in (N.KERNEL_PERSISTENT, N.KERNEL_STREAMING):
+        d = N.DeviceScene(ctx, s)
+        d.fit_rotations()
+        st = d.corotational_pass(1e-3, 1e-8, 20000, precision=N.PRECISION_MIXED, kernel=kernel)
+        assert st["converged"] == 1 and st["true_residual"] <= 1e-8, (kernel, st)
+        if kernel == N.KERNEL_PERSISTENT:
+            assert d.kernel_times(N.PRECISION_MIXED, reps=1)["persistent_form"] == "brick"
+        out[kernel] = d.positions() - s.position
+        d.close()
+    assert rel(out[N.KERNEL_PERSISTENT], out[N.KERNEL_STREAMING]) < 2e-5
 
 
 def test_persistent_solve_on_wood_cube_meets_fp64_target(ctx):

@@ -197,8 +197,8 @@ struct vx_scene {
     // compact sets of REVs; one device allocation holds the plan's tables
     bool brick_ok = false;
     unsigned brick_G = 0, brick_cap = 0, brick_hz = 0, brick_hk = 0, brick_R = 0, brick_tpr = 1;
-    int persist_form = 0;             // 0: brick (1 thread per REV, >= 256 REVs per block), else the
-                                      // range plan; VX_PERSIST_*: that form only (the autotuner's choice)
+    int persist_form = 0;             // 0: the range plan, else the brick plan (1 thread per REV, >= 256
+                                      // REVs per block); VX_PERSIST_*: that form only (the autotuner's choice)
     size_t brick_smem = 0;
     void* brick_buf = nullptr;
     uint4* brick_info = nullptr;      // [G] own REVs, halo z slots, halo K slots, neighbour blocks

@@ -214,7 +214,6 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
             F3 s = {mh * pi.x, mh * pi.y, mh * pi.z};
 #pragma unroll
             for (int t = 0; t < 6; ++t) {
-                const bool ok = dl[t] != 0;
                 const uint32_t j = (uint32_t)((int32_t)i + dl[t]);
                 const int ax = t < 3 ? t : t - 3;
                 const uint32_t lj = j - lo;
@@ -235,7 +234,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
                     Kb = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
                 }
                 const F3 pn = {fmaf(beta, q4.w, q4.x), fmaf(beta, q2.x, q4.y), fmaf(beta, q2.y, q4.z)};
-                const F3 d = ok ? F3{pi.x - pn.x, pi.y - pn.y, pi.z - pn.z} : F3{0.f, 0.f, 0.f};
+                // a missing neighbour has delta 0: j = i, pn = pi and d = 0 exactly
+                const F3 d = {pi.x - pn.x, pi.y - pn.y, pi.z - pn.z};
                 const F3 kv = smul(Kb, d);
                 s.x += kv.x, s.y += kv.y, s.z += kv.z;
             }
@@ -360,10 +360,14 @@ cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t
 
 }  // namespace
 
+static bool range_plan(vx_scene* s);
+
 // Whether the persistent inner solve fits this scene on this GPU; caches the
-// shape. Without a chosen form the brick plan (vx_brick.cu) is preferred and
-// the contiguous-range plan below takes the scenes it does not; a chosen form
-// (the autotuner's, or VXCOROT_PERSISTENT=range) is that form or nothing.
+// shape. Without a chosen form the contiguous-range plan below is preferred
+// (it measured faster at every size both fit) and the brick plan (vx_brick.cu)
+// takes the scenes it does not: neighbour deltas beyond int16, or a range too
+// large for shared memory. A chosen form (the autotuner's, or
+// VXCOROT_PERSISTENT=range|brick) is that form or nothing.
 bool persistent_plan(vx_scene* s) {
     if (s->persist_checked) return s->persist_ok;
     s->persist_checked = true;
@@ -371,15 +375,24 @@ bool persistent_plan(vx_scene* s) {
     s->brick_ok = false;
     if (s->n == 0) return false;
     int form = s->persist_form;
-    if (const char* v = std::getenv("VXCOROT_PERSISTENT"))
+    if (const char* v = std::getenv("VXCOROT_PERSISTENT")) {
         if (std::strcmp(v, "range") == 0) form = VX_PERSIST_RANGE;
-    if (form != VX_PERSIST_RANGE) {
-        if (brick_plan(s, form == 0 ? VX_PERSIST_BRICK_T1_256 : form)) {
-            s->persist_ok = true;
-            return true;
-        }
-        if (form != 0) return false;
+        else if (std::strcmp(v, "brick") == 0) form = VX_PERSIST_BRICK_T1_256;
     }
+    if (form != 0 && form != VX_PERSIST_RANGE) {
+        if (!brick_plan(s, form)) return false;
+        s->persist_ok = true;
+        return true;
+    }
+    if (!range_plan(s)) {
+        if (form != 0 || !brick_plan(s, VX_PERSIST_BRICK_T1_256)) return false;
+    }
+    s->persist_ok = true;
+    return true;
+}
+
+// The contiguous-range plan: block b owns REVs [b cap, (b + 1) cap).
+static bool range_plan(vx_scene* s) {
     if (s->nbcode_state == 0) {  // once per topology: did every neighbour delta fit?
         uint32_t bad = 0;
         if (cudaMemcpyAsync(&bad, s->nbcode_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
@@ -404,11 +417,11 @@ bool persistent_plan(vx_scene* s) {
     s->persist_cap = cap;
     s->persist_R = R <= 1 ? 1 : (R <= 2 ? 2 : 4);
     s->persist_smem = smem;
-    s->persist_ok = true;
     return true;
 }
 
 uint32_t persistent_block_cap() { return kPoolBlockRevs; }
+
 
 // One cooperative launch of the persistent inner solve over the pool slots of
 // a wave: d_blocks holds one row per block (first REV, REV count, slot, first
