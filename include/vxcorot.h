@@ -602,7 +602,8 @@ void* vx_scene_stream(vx_scene* scene);
  *   - for MIXED, when the scene fits on chip, the persistent forms
  *     (candidate_blocks = VX_PERSIST_*): the brick plan with one or two
  *     threads per REV and tiles of at least 256 or 128 REVs per block, and
- *     the contiguous-range plan.
+ *     the contiguous-range plan with the classic two reductions per
+ *     iteration or with one.
  * With cache_path (or NULL), a choice found there for this GPU, precision and
  * scene size (log2 of the REV count) is applied without timing, and a new
  * choice is stored. Positions and bond state are not changed; the solver's
@@ -613,15 +614,16 @@ void* vx_scene_stream(vx_scene* scene);
 #define VX_PERSIST_BRICK_T1_128 3   /* brick plan, 1 thread per REV, >= 128 REVs per block */
 #define VX_PERSIST_BRICK_T2_128 4   /* brick plan, 2 threads per REV, >= 128 REVs per block */
 #define VX_PERSIST_RANGE 5          /* contiguous-range plan (classic two-reduction recurrence) */
+#define VX_PERSIST_EXPANDED 6       /* contiguous-range plan, one reduction per iteration */
 typedef struct vx_tune_result {
     int32_t kernel;               /* VX_KERNEL_STREAMING or VX_KERNEL_PERSISTENT */
     int32_t blocks_per_sm;        /* streaming: register budget; persistent: VX_PERSIST_* form */
     double us_per_iteration;      /* of the chosen configuration */
     int32_t from_cache;           /* 1: read from cache_path, nothing timed */
-    uint32_t candidates;          /* timed configurations (at most 8) */
-    int32_t candidate_kernel[8];
-    int32_t candidate_blocks[8];
-    double candidate_us[8];
+    uint32_t candidates;          /* timed configurations (at most 12) */
+    int32_t candidate_kernel[12];
+    int32_t candidate_blocks[12];
+    double candidate_us[12];
 } vx_tune_result;
 int32_t vx_scene_autotune(vx_scene* scene, int32_t precision, const char* cache_path, vx_tune_result* out);
 
@@ -632,7 +634,8 @@ int32_t vx_scene_autotune(vx_scene* scene, int32_t precision, const char* cache_
  * out_us[5]: streaming matvec us, streaming update us, and for the MIXED
  * precision when the on-chip form fits: its us per iteration over a 64-iteration
  * solve, that solve's iterations, and its form (1 = brick plan with one grid
- * reduction per iteration, 2 = contiguous-range plan, 0 = none).
+ * reduction per iteration, 2 = contiguous-range plan, 3 = contiguous-range plan
+ * with one reduction per iteration, 0 = none).
  * The streaming kernels are timed alone, one launch of each per rep after the
  * flush (when given), on the scene's assembled system.
  */

@@ -319,14 +319,16 @@ def test_persistent_kernels_agree_at_full_grid(ctx, edge):
 
 
 @pytest.mark.parametrize("edge", [24, 64])
-def test_brick_and_range_forms_agree(ctx, edge, monkeypatch):
+def test_persistent_forms_agree(ctx, edge, monkeypatch):
     """The brick plan (Chronopoulos-Gear recurrence, one grid reduction per
-    iteration, VXCOROT_PERSISTENT=brick) and the contiguous-range plan (classic
-    recurrence, two reductions, VXCOROT_PERSISTENT=range) both reach the FP64
-    target over three passes and agree to the solve error."""
+    iteration, VXCOROT_PERSISTENT=brick), the contiguous-range plan with the
+    classic recurrence (two reductions, VXCOROT_PERSISTENT=range) and with the
+    expanded one (one reduction, VXCOROT_PERSISTENT=expanded) all reach the
+    FP64 target over three passes, agree to the solve error and take about the
+    same number of inner iterations."""
     s = S.mixed_block(edge, seed=3)
     out, iters = {}, {}
-    for form in ("brick", "range"):
+    for form in ("brick", "range", "expanded"):
         monkeypatch.setenv("VXCOROT_PERSISTENT", form)
         d = N.DeviceScene(ctx, s)
         it = 0
@@ -339,9 +341,10 @@ def test_brick_and_range_forms_agree(ctx, edge, monkeypatch):
         out[form] = d.positions() - s.position
         iters[form] = it
         d.close()
-    print(f"{edge}^3 inner iterations over 3 passes: brick {iters['brick']}, range {iters['range']}")
-    assert rel(out["brick"], out["range"]) < 2e-5
-    assert abs(iters["brick"] - iters["range"]) <= 0.05 * iters["range"] + 16
+    print(f"{edge}^3 inner iterations over 3 passes: {iters}")
+    for form in ("brick", "expanded"):
+        assert rel(out[form], out["range"]) < 2e-5, form
+        assert abs(iters[form] - iters["range"]) <= 0.05 * iters["range"] + 16, form
 
 
 def test_wide_plate_takes_the_brick_form(ctx, monkeypatch):
@@ -375,11 +378,11 @@ def test_persistent_solve_on_wood_cube_meets_fp64_target(ctx):
     assert st["converged"] == 1 and st["true_residual"] <= 1e-10, st
 
 
-@pytest.mark.parametrize("form", ["brick", "range"])
+@pytest.mark.parametrize("form", ["brick", "range", "expanded"])
 def test_persistent_barrier_wait_runs_out_and_reports_timeout(form):
     """A wait bounded at one poll runs out (no block is missing, the bound is
     simply too small): in the brick form the neighbour-flag wait or the grid
-    reduction, in the range form a grid reduction. The kernel records
+    reduction, in the range forms a grid reduction. The kernel records
     VX_TIMEOUT and returns, and the context stays usable."""
     import subprocess
     import sys

@@ -259,6 +259,8 @@ void scene_release(vx_scene* s) {
     if (s->arena.base) cudaFree(s->arena.base);
     if (s->brick_buf) cudaFree(s->brick_buf);
     s->brick_buf = nullptr;
+    if (s->exp_buf) cudaFree(s->exp_buf);
+    s->exp_buf = nullptr;
     s->brick_ok = false;
     if (s->stream) cudaStreamDestroy(s->stream);
     s->chunk64 = s->chunk32 = nullptr;
@@ -934,7 +936,7 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
                         if (kernel == VX_KERNEL_STREAMING) {
                             usable = blocks >= 3 && blocks <= 5;
                         } else if (kernel == VX_KERNEL_PERSISTENT && blocks >= VX_PERSIST_BRICK_T1_256 &&
-                                   blocks <= VX_PERSIST_RANGE) {
+                                   blocks <= VX_PERSIST_EXPANDED) {
                             const int old_form = s->persist_form;
                             apply_tuning(s, kernel, blocks);
                             usable = persistent_plan(s);
@@ -968,11 +970,11 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
         // threads per REV (a large scene reaches the same tiles from either
         // minimum) are timed once
         std::vector<std::array<unsigned, 3>> seen;
-        for (int form = VX_PERSIST_BRICK_T1_256; form <= VX_PERSIST_RANGE; ++form) {
+        for (int form = VX_PERSIST_BRICK_T1_256; form <= VX_PERSIST_EXPANDED; ++form) {
             s->persist_form = form;
             s->persist_checked = false;
             if (!persistent_plan(s)) continue;
-            if (form != VX_PERSIST_RANGE) {
+            if (form < VX_PERSIST_RANGE) {
                 const std::array<unsigned, 3> shape = {s->brick_G, s->brick_cap, s->brick_tpr};
                 if (std::find(seen.begin(), seen.end(), shape) != seen.end()) continue;
                 seen.push_back(shape);
@@ -983,7 +985,7 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
         s->persist_checked = false;
     }
     int best = -1;
-    for (size_t k = 0; k < cands.size() && k < 8; ++k) {
+    for (size_t k = 0; k < cands.size() && k < 12; ++k) {
         double us = 0.0;
         int32_t r = time_candidate(s, precision, cands[k].kernel, cands[k].blocks, &us);
         if (r != VX_OK) {

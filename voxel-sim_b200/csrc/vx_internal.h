@@ -209,6 +209,16 @@ struct vx_scene {
     uint32_t* brick_nbk = nullptr;    // [G][32] blocks whose REVs are in the halo
     uint32_t* brick_pub = nullptr;    // [G] iteration whose z the block has published
     double* brick_part = nullptr;     // [3][G] grid-reduction partials
+    // range plan with one reduction per iteration (vx_expanded.cu): published
+    // triples (u, v, p) in two parities and the partials, one allocation
+    bool exp_ok = false;
+    unsigned exp_G = 0, exp_cap = 0, exp_R = 0;
+    size_t exp_smem = 0;
+    void* exp_buf = nullptr;
+    float4* exp_pa = nullptr;         // [2][n] (u, v.x)
+    float4* exp_pb = nullptr;         // [2][n] (v.y, v.z, p.x, p.y)
+    float* exp_pc = nullptr;          // [2][n] p.z
+    double* exp_part = nullptr;       // [14][G]
     uint32_t active = 0;          // REVs with a free axis (cached per target set)
     bool active_cached = false;
     bool assembled = false;

@@ -586,7 +586,7 @@ int32_t kernel_times(vx_scene* s, int32_t precision, uint32_t reps, void* flush,
         }
         out_us[2] = its > 0 ? 1000.0 * ms / its : 0.0;
         out_us[3] = its;
-        out_us[4] = s->brick_ok ? 1.0 : 2.0;
+        out_us[4] = s->exp_ok ? 3.0 : (s->brick_ok ? 1.0 : 2.0);
     }
     return VX_OK;
 }

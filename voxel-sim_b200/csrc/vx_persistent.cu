@@ -363,44 +363,49 @@ cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t
 static bool range_plan(vx_scene* s);
 
 // Whether the persistent inner solve fits this scene on this GPU; caches the
-// shape. Without a chosen form the contiguous-range plan below is preferred
-// (it measured faster at every size both fit) and the brick plan (vx_brick.cu)
-// takes the scenes it does not: neighbour deltas beyond int16, or a range too
-// large for shared memory. A chosen form (the autotuner's, or
-// VXCOROT_PERSISTENT=range|brick) is that form or nothing.
+// shape. Without a chosen form the range plan with one reduction per
+// iteration (vx_expanded.cu) is preferred, then the range plan below with the
+// classic two, then the brick plan (vx_brick.cu), which takes the scenes whose
+// neighbour deltas do not fit an int16. A chosen form (the autotuner's, or
+// VXCOROT_PERSISTENT=expanded|range|brick) is that form or nothing.
 bool persistent_plan(vx_scene* s) {
     if (s->persist_checked) return s->persist_ok;
     s->persist_checked = true;
     s->persist_ok = false;
     s->brick_ok = false;
+    s->exp_ok = false;
     if (s->n == 0) return false;
     int form = s->persist_form;
     if (const char* v = std::getenv("VXCOROT_PERSISTENT")) {
-        if (std::strcmp(v, "range") == 0) form = VX_PERSIST_RANGE;
+        if (std::strcmp(v, "expanded") == 0) form = VX_PERSIST_EXPANDED;
+        else if (std::strcmp(v, "range") == 0) form = VX_PERSIST_RANGE;
         else if (std::strcmp(v, "brick") == 0) form = VX_PERSIST_BRICK_T1_256;
     }
-    if (form != 0 && form != VX_PERSIST_RANGE) {
-        if (!brick_plan(s, form)) return false;
-        s->persist_ok = true;
-        return true;
-    }
-    if (!range_plan(s)) {
-        if (form != 0 || !brick_plan(s, VX_PERSIST_BRICK_T1_256)) return false;
-    }
-    s->persist_ok = true;
-    return true;
+    bool ok;
+    if (form == VX_PERSIST_EXPANDED) ok = expanded_plan(s);
+    else if (form == VX_PERSIST_RANGE) ok = range_plan(s);
+    else if (form != 0) ok = brick_plan(s, form);
+    else ok = expanded_plan(s) || range_plan(s) || brick_plan(s, VX_PERSIST_BRICK_T1_256);
+    s->persist_ok = ok;
+    return ok;
 }
 
-// The contiguous-range plan: block b owns REVs [b cap, (b + 1) cap).
-static bool range_plan(vx_scene* s) {
-    if (s->nbcode_state == 0) {  // once per topology: did every neighbour delta fit?
+// Whether every neighbour delta j - i of the scene fits an int16 (read back
+// once per topology from k_neighbor_codes' flag).
+bool neighbor_deltas_fit(vx_scene* s) {
+    if (s->nbcode_state == 0) {
         uint32_t bad = 0;
         if (cudaMemcpyAsync(&bad, s->nbcode_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
             cudaStreamSynchronize(s->stream) != cudaSuccess)
             return false;
         s->nbcode_state = bad == 0 ? 1 : 2;
     }
-    if (s->nbcode_state != 1) return false;
+    return s->nbcode_state == 1;
+}
+
+// The contiguous-range plan: block b owns REVs [b cap, (b + 1) cap).
+static bool range_plan(vx_scene* s) {
+    if (!neighbor_deltas_fit(s)) return false;
     int dev = s->device, max_smem = 0, coop = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -478,6 +483,7 @@ int32_t solve_inner_slots(vx_scene* s, const uint4* d_blocks, SlotState* st, uns
 
 // One FP32 inner solve A32 d = r64 / |r64| in a single cooperative launch.
 int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_iterations) {
+    if (s->exp_ok) return solve_inner_expanded(s, tolerance, max_iterations);
     if (s->brick_ok) return solve_inner_brick(s, tolerance, max_iterations);
     PersistArgs a;
     a.n = s->n;

@@ -123,7 +123,7 @@ FIELD_POSITION, FIELD_VELOCITY, FIELD_PREVIOUS = 0, 1, 2
 
 PERSIST_FORMS = {1: "brick, 1 thread/REV, >=256 REVs/block", 2: "brick, 2 threads/REV, >=256 REVs/block",
                  3: "brick, 1 thread/REV, >=128 REVs/block", 4: "brick, 2 threads/REV, >=128 REVs/block",
-                 5: "range (classic recurrence)"}
+                 5: "range (classic recurrence)", 6: "range (one reduction per iteration)"}
 
 
 def tune_label(kernel: int, blocks: int) -> str:
@@ -135,8 +135,8 @@ def tune_label(kernel: int, blocks: int) -> str:
 
 class VxTuneResult(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("blocks_per_sm", C.c_int32), ("us_per_iteration", C.c_double),
-                ("from_cache", C.c_int32), ("candidates", C.c_uint32), ("candidate_kernel", C.c_int32 * 8),
-                ("candidate_blocks", C.c_int32 * 8), ("candidate_us", C.c_double * 8)]
+                ("from_cache", C.c_int32), ("candidates", C.c_uint32), ("candidate_kernel", C.c_int32 * 12),
+                ("candidate_blocks", C.c_int32 * 12), ("candidate_us", C.c_double * 12)]
 
     def as_dict(self):
         k = self.candidates
@@ -426,7 +426,7 @@ class DeviceScene:
                                            _p(out, C.c_double)))
         return {"matvec_us": float(out[0]), "update_us": float(out[1]), "persistent_iter_us": float(out[2]),
                 "persistent_iterations": int(out[3]),
-                "persistent_form": {0: None, 1: "brick", 2: "range"}[int(out[4])]}
+                "persistent_form": {0: None, 1: "brick", 2: "range", 3: "expanded"}[int(out[4])]}
 
     # -- the solve ------------------------------------------------------------
     def fit_rotations(self) -> float:
