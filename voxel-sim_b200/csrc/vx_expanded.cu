@@ -14,7 +14,8 @@
 // value every iteration, so the expansion's rounding does not accumulate
 // across iterations. An FP32 CPU emulation of both recurrences takes the same
 // iteration counts on mixed blocks of 8^3 to 48^3, a damaged lattice and a
-// box union, and the iterates agree to 1e-6.
+// box union, and the iterates agree to 1e-6
+// (tests/test_oracle_expanded_recurrence.py keeps three of those cases).
 //
 // The next direction p' = z' + beta' p of a neighbour must be formed without a
 // second grid barrier, so each block publishes, BEFORE the reduction, the
