@@ -49,6 +49,7 @@ namespace {
 constexpr int kEThreads = 512;
 constexpr int kEBytesPerRev = 3 * 16 + 3 * 8 + 16 + 16 + 4 + 12 + 4 + 1;
 constexpr int kENV = 7;  // values summed per iteration
+constexpr int kEW = 8;   // partials rows per parity: the seven sums and, in pools, the working-block count
 
 struct ExpArgs {
     uint32_t n;
@@ -65,13 +66,17 @@ struct ExpArgs {
     float4* pa;                 // [2][n] published (u.x, u.y, u.z, v.x)
     float4* pb;                 // [2][n] published (v.y, v.z, p.x, p.y)
     float* pc;                  // [2][n] published p.z
-    double* part;               // [2 * kENV][G] partials, two parities
+    double* part;               // [2 * kEW][G] partials, two parities
     unsigned long long* count;  // arrivals at the grid reductions so far
     int32_t* err;               // a wait ran out
     PcgScalars* sc;
     double tolerance;
     uint32_t max_iterations;
     unsigned long long spin_limit;
+    // pools: one row per block (first REV, REV count, slot, first block of the
+    // slot << 16 | blocks of the slot) and the slots' states; null for one scene
+    const uint4* blocks;
+    SlotState* st;
 };
 
 struct E3 {
@@ -92,12 +97,16 @@ __device__ __forceinline__ E3 next_dir(float4 A, float4 B, float C, float alpha,
 // R REVs per thread. With R <= 2 the inverse diagonal block is loaded into
 // registers before the matvec, so its L2 latency overlaps the neighbour loads;
 // at R = 4 the four loads are issued together after the matvec.
-template <int R>
+// MULTI: the blocks work for several pool slots (a.blocks, a.st), each slot's
+// sums taken over its own blocks in block order, so a slot's bits do not
+// depend on the slots beside it; a slot that has stopped leaves its blocks
+// idle, and every block leaves at the reduction where no block has work left.
+template <int R, bool MULTI>
 __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
     constexpr bool kPrefetch = R <= 2;
     extern __shared__ float4 smem4[];
     __shared__ double red[kENV][32];
-    __shared__ double tot[kENV];
+    __shared__ double tot[kENV + 1];
     __shared__ int s_ok;
     const uint32_t n = a.n, cap = a.cap, T = blockDim.x;
     float4* sK4 = smem4;                                      // [3][cap] owned bonds (xx, yy, zz, xy)
@@ -110,8 +119,25 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
     uint8_t* sFL = reinterpret_cast<uint8_t*>(sM + cap);      // [cap] free-axis flags
     // the (p.x, p.y) halves of the sPB records: record li at [2 li]
     const float2* sPBzw = reinterpret_cast<const float2*>(sPB) + 1;
-    const uint32_t lo = blockIdx.x * cap;
-    const uint32_t cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
+    // this block's range and problem: the whole grid for one scene, or one
+    // slot's blocks in a pool (its own target, iteration cap and outcome)
+    uint32_t lo, cnt, slot = 0, fb = 0, nb = gridDim.x;
+    double scale_norm, tolerance;
+    uint32_t max_iterations;
+    bool mine = true;  // this block's problem still iterates
+    if constexpr (MULTI) {
+        const uint4 bi = a.blocks[blockIdx.x];
+        lo = bi.x, cnt = bi.y, slot = bi.z, fb = bi.w >> 16, nb = bi.w & 0xFFFFu;
+        const SlotState& S = a.st[slot];
+        mine = S.enabled && S.inner_on;
+        scale_norm = S.r64_norm, tolerance = S.tol_in, max_iterations = S.max_its;
+        if (!mine) cnt = 0;
+    } else {
+        lo = blockIdx.x * cap;
+        cnt = lo < n ? (n - lo < cap ? n - lo : cap) : 0;
+        scale_norm = *a.scale_from, tolerance = a.tolerance, max_iterations = a.max_iterations;
+    }
+    constexpr int W = MULTI ? kEW : kENV;  // partials rows per parity
 
     for (uint32_t li = threadIdx.x; li < cnt; li += T) {
         const size_t i = lo + li;
@@ -132,7 +158,6 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
     float x[R][3], r[R][3], q[R][3];
     E3 pown[R];
     Sym<float> ireg[kPrefetch ? R : 1];
-    const double scale_norm = *a.scale_from;
     const double scale = scale_norm > 0.0 ? 1.0 / scale_norm : 1.0;
     double acc[2] = {0.0, 0.0};
 #pragma unroll
@@ -158,32 +183,36 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
     unsigned long long seq = 1;
     double t[kENV];
     bool alive;
+    double act = 0.0;
     {
-        const int sl[2] = {kENV, kENV + 1};  // parity-1 rows: iteration 0 sums into parity 0
+        const int sl[2] = {W, W + 1};  // parity-1 rows: iteration 0 sums into parity 0
         double t0[2];
-        alive = grid_reduce<2>(acc, sl, a, seq++, red, tot, &s_ok, t0);
+        if constexpr (MULTI) alive = grid_reduce_ranged<2>(acc, 0.0, sl, -1, a, seq++, fb, nb, red, tot, &s_ok, t0, &act);
+        else alive = grid_reduce<2>(acc, sl, a, seq++, red, tot, &s_ok, t0);
         t[0] = t0[0], t[1] = t0[1];
     }
     const double initial = sqrt(t[0]);
     double residual = 0.0;
     uint32_t its = 0;
     int32_t status = alive ? VX_OK : VX_TIMEOUT;
-    bool go = alive;
-    if (go) {
+    if (alive && mine) {
         if (!isfinite(t[0]) || !isfinite(t[1])) {
-            go = false;
+            mine = false;
             status = VX_NONFINITE;
         } else if (!(initial > 1e-12)) {
-            go = false;
-        } else if (a.max_iterations == 0) {
-            go = false;
+            mine = false;
+        } else if (max_iterations == 0) {
+            mine = false;
             status = VX_NOT_CONVERGED;
         }
     }
 
     float alpha_prev = 0.f, beta = 0.f;
-    while (go) {
-        const uint32_t par = its & 1u;  // this iteration writes parity par, reads par ^ 1
+    uint32_t loop = 0;  // iterations of the loop, the same in every block
+    while (alive) {
+        if (!MULTI && !mine) break;
+        const uint32_t cnt_now = mine ? cnt : 0;
+        const uint32_t par = loop & 1u;  // this iteration writes parity par, reads par ^ 1
         const float4* gA = a.pa + (size_t)(par ^ 1u) * n;
         const float4* gB = a.pb + (size_t)(par ^ 1u) * n;
         const float* gC = a.pc + (size_t)(par ^ 1u) * n;
@@ -191,7 +220,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 const uint32_t li = threadIdx.x + k * T;
-                if (li < cnt) ireg[k] = load_sym(a.Dinv, n, lo + li);
+                if (li < cnt_now) ireg[k] = load_sym(a.Dinv, n, lo + li);
             }
         }
         // ---- the block's own directions p = z + beta p_old, formed once from
@@ -199,7 +228,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_now) continue;
             const float4 B = sPB[li];
             const E3 pi = next_dir(sPA[li], B, sPC[li], alpha_prev, beta);
             sPB[li] = make_float4(B.x, B.y, pi.x, pi.y);
@@ -211,7 +240,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_now) continue;
             const uint32_t i = lo + li;
             int32_t dl[6];
 #pragma unroll
@@ -262,7 +291,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
             for (int k = 0; k < R; ++k) {
                 const uint32_t li = threadIdx.x + k * T;
-                if (li < cnt) Dk[k] = load_sym(a.Dinv, n, lo + li);
+                if (li < cnt_now) Dk[k] = load_sym(a.Dinv, n, lo + li);
             }
         }
         float4* wA = a.pa + (size_t)par * n;
@@ -271,7 +300,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_now) continue;
             const size_t i = lo + li;
             Sym<float> Di;
             if constexpr (kPrefetch) Di = ireg[k];
@@ -295,16 +324,26 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
         }
         int sl[kENV];
 #pragma unroll
-        for (int c = 0; c < kENV; ++c) sl[c] = c + kENV * (int)par;
-        if (!grid_reduce<kENV>(d, sl, a, seq++, red, tot, &s_ok, t)) {
+        for (int c = 0; c < kENV; ++c) sl[c] = c + W * (int)par;
+        bool ok;
+        if constexpr (MULTI)
+            ok = grid_reduce_ranged<kENV>(d, mine ? 1.0 : 0.0, sl, W * (int)par + kENV, a, seq++, fb, nb, red, tot,
+                                          &s_ok, t, &act);
+        else
+            ok = grid_reduce<kENV>(d, sl, a, seq++, red, tot, &s_ok, t);
+        if (!ok) {
             status = VX_TIMEOUT;
             break;
         }
+        if (MULTI && act == 0.0) break;  // no block of the grid has work left
+        ++loop;
+        if (!mine) continue;
         const double g = t[0], pq = t[1];
         if (!isfinite(g) || !isfinite(pq) || pq <= 1e-30) {
             its += 1;  // the matvec happened (src/solver.rs:1861-1866)
             if (!isfinite(g) || !isfinite(pq)) status = VX_NONFINITE;
-            break;
+            mine = false;
+            continue;
         }
         const float alpha = (float)(g / pq);
         const double al = (double)alpha;  // the vectors move by the FP32 alpha
@@ -314,7 +353,7 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt) continue;
+            if (li >= cnt_now) continue;
             x[k][0] = fmaf(alpha, pown[k].x, x[k][0]);
             x[k][1] = fmaf(alpha, pown[k].y, x[k][1]);
             x[k][2] = fmaf(alpha, pown[k].z, x[k][2]);
@@ -325,12 +364,12 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
         residual = sqrt(fmax(rr_next, 0.0)) / initial;
         if (!isfinite(g_next) || !isfinite(rr_next)) {
             status = VX_NONFINITE;
-            break;
-        }
-        if (residual < a.tolerance) break;
-        if (its >= a.max_iterations) {
+            mine = false;
+        } else if (residual < tolerance) {
+            mine = false;
+        } else if (its >= max_iterations) {
             status = VX_NOT_CONVERGED;
-            break;
+            mine = false;
         }
         beta = (float)(g_next / g);
         alpha_prev = alpha;
@@ -343,26 +382,62 @@ __global__ void __launch_bounds__(kEThreads, 1) k_pcg_expanded(ExpArgs a) {
         const size_t i = lo + li;
         a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
     }
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        PcgScalars* sc = a.sc;
-        sc->iterations = its;
-        sc->residual = residual;
-        sc->initial = initial;
-        sc->status = status;
-        sc->done = 1;
+    if (threadIdx.x == 0 && blockIdx.x == fb) {
+        if constexpr (MULTI) {
+            SlotState& S = a.st[slot];
+            if (S.enabled && S.inner_on) {
+                S.its = its;
+                S.residual_in = residual;
+                S.initial = initial;
+                S.status_in = status;
+                S.done = 1;
+            }
+        } else {
+            PcgScalars* sc = a.sc;
+            sc->iterations = its;
+            sc->residual = residual;
+            sc->initial = initial;
+            sc->status = status;
+            sc->done = 1;
+        }
     }
 }
 
-template <int R>
+template <int R, bool MULTI>
 cudaError_t launch_e(const ExpArgs& a, unsigned G, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_pcg_expanded<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_pcg_expanded<R, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     ExpArgs args = a;
     void* params[] = {&args};
-    return cudaLaunchCooperativeKernel((void*)k_pcg_expanded<R>, dim3(G), dim3(kEThreads), params, smem, st);
+    return cudaLaunchCooperativeKernel((void*)k_pcg_expanded<R, MULTI>, dim3(G), dim3(kEThreads), params, smem, st);
 }
 
 }  // namespace
+
+// The published triples (two parities) and the partials (two parities of kEW
+// rows for up to one block per SM): one device allocation, kept until the
+// scene is released or re-planned.
+static bool exp_buffers(vx_scene* s) {
+    if (s->exp_buf) return true;
+    const size_t n = s->n, G = (size_t)(s->sm_count > 0 ? s->sm_count : 1);
+    const size_t o_b = 2 * n * sizeof(float4);
+    const size_t o_c = o_b + 2 * n * sizeof(float4);
+    const size_t o_p = (o_c + 2 * n * sizeof(float) + 255) & ~size_t(255);
+    const size_t bytes = o_p + 2 * (size_t)kEW * G * sizeof(double);
+    void* buf = nullptr;
+    if (cudaMalloc(&buf, bytes) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    char* B = static_cast<char*>(buf);
+    s->exp_buf = buf;
+    s->exp_pa = reinterpret_cast<float4*>(B);
+    s->exp_pb = reinterpret_cast<float4*>(B + o_b);
+    s->exp_pc = reinterpret_cast<float*>(B + o_c);
+    s->exp_part = reinterpret_cast<double*>(B + o_p);
+    return true;
+}
 
 // The plan: block b owns REVs [b cap, (b + 1) cap), as in the range plan, with
 // 125 B of shared memory per REV; the published triples (two parities) and
@@ -389,21 +464,7 @@ bool expanded_plan(vx_scene* s) {
     const size_t smem = ((size_t)kEBytesPerRev * cap + 15) & ~size_t(15);
     // the kernel's static shared memory (reduction slots) takes under 2 KB
     if (R > 4 || smem + 2048 > (size_t)max_smem) return false;
-    const size_t o_b = (size_t)2 * n * sizeof(float4);
-    const size_t o_c = o_b + (size_t)2 * n * sizeof(float4);
-    const size_t o_p = (o_c + (size_t)2 * n * sizeof(float) + 255) & ~size_t(255);
-    const size_t bytes = o_p + (size_t)2 * kENV * G * sizeof(double);
-    void* buf = nullptr;
-    if (cudaMalloc(&buf, bytes) != cudaSuccess) {
-        (void)cudaGetLastError();
-        return false;
-    }
-    char* B = static_cast<char*>(buf);
-    s->exp_buf = buf;
-    s->exp_pa = reinterpret_cast<float4*>(B);
-    s->exp_pb = reinterpret_cast<float4*>(B + o_b);
-    s->exp_pc = reinterpret_cast<float*>(B + o_c);
-    s->exp_part = reinterpret_cast<double*>(B + o_p);
+    if (!exp_buffers(s)) return false;
     s->exp_G = G;
     s->exp_cap = cap;
     s->exp_R = R <= 1 ? 1 : (R <= 2 ? 2 : 4);
@@ -435,6 +496,8 @@ int32_t solve_inner_expanded(vx_scene* s, double tolerance, uint32_t max_iterati
     a.sc = s->sc32;
     a.tolerance = tolerance;
     a.max_iterations = max_iterations;
+    a.blocks = nullptr;
+    a.st = nullptr;
     a.spin_limit = 4000000ull;  // ~1-2 s of polling at one reduction
     // VXCOROT_BARRIER_SPINS lowers the bound so a test can make the wait run out
     if (const char* v = std::getenv("VXCOROT_BARRIER_SPINS")) {
@@ -444,14 +507,68 @@ int32_t solve_inner_expanded(vx_scene* s, double tolerance, uint32_t max_iterati
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
     if (e == cudaSuccess) {
         switch (s->exp_R) {
-            case 1: e = launch_e<1>(a, s->exp_G, s->exp_smem, s->stream); break;
-            case 2: e = launch_e<2>(a, s->exp_G, s->exp_smem, s->stream); break;
-            default: e = launch_e<4>(a, s->exp_G, s->exp_smem, s->stream); break;
+            case 1: e = launch_e<1, false>(a, s->exp_G, s->exp_smem, s->stream); break;
+            case 2: e = launch_e<2, false>(a, s->exp_G, s->exp_smem, s->stream); break;
+            default: e = launch_e<4, false>(a, s->exp_G, s->exp_smem, s->stream); break;
         }
     }
     s->launches += 1;
     if (e != cudaSuccess) {
         set_error("persistent PCG launch failed: %s", cudaGetErrorString(e));
+        return VX_CUDA_ERROR;
+    }
+    return VX_OK;
+}
+
+// One cooperative launch of the one-reduction inner solve over the pool slots
+// of a wave (rows and slot states as solve_inner_slots in vx_persistent.cu).
+// One instantiation serves every wave, so a slot's bits do not depend on the
+// wave it lands in.
+int32_t solve_inner_slots_expanded(vx_scene* s, const uint4* d_blocks, SlotState* st, unsigned G, uint32_t cap) {
+    int dev = s->device, max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t smem = ((size_t)kEBytesPerRev * cap + 15) & ~size_t(15);
+    if (cap == 0 || cap > 4u * kEThreads || G > (unsigned)s->sm_count || smem + 2048 > (size_t)max_smem) {
+        set_error("persistent pool PCG: a wave of %u blocks of %u REVs does not fit", G, cap);
+        return VX_BAD_INPUT;
+    }
+    if (!exp_buffers(s)) {
+        set_error("persistent pool PCG: the published-direction buffers could not be allocated");
+        return VX_CUDA_ERROR;
+    }
+    ExpArgs a;
+    a.n = s->n;
+    a.cap = cap;
+    a.kn = kstride32(s->n);
+    a.flags = s->flags;
+    a.mh2 = s->mh2_32;
+    a.K = s->bonds.k32;
+    a.Dinv = s->dinv32;
+    a.code = s->nbcode;
+    a.src = s->r64;
+    a.scale_from = nullptr;
+    a.x = s->x32;
+    a.pa = s->exp_pa;
+    a.pb = s->exp_pb;
+    a.pc = s->exp_pc;
+    a.part = s->exp_part;
+    a.count = reinterpret_cast<unsigned long long*>(s->barrier);
+    a.err = reinterpret_cast<int32_t*>(s->barrier + 2);
+    a.sc = nullptr;
+    a.tolerance = 0.0;
+    a.max_iterations = 0;
+    a.blocks = d_blocks;
+    a.st = st;
+    a.spin_limit = 4000000ull;
+    if (const char* v = std::getenv("VXCOROT_BARRIER_SPINS")) {
+        unsigned long long lim = std::strtoull(v, nullptr, 10);
+        if (lim > 0 && lim < a.spin_limit) a.spin_limit = lim;
+    }
+    cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
+    if (e == cudaSuccess) e = launch_e<4, true>(a, G, smem, s->stream);
+    s->launches += 1;
+    if (e != cudaSuccess) {
+        set_error("persistent pool PCG launch failed: %s", cudaGetErrorString(e));
         return VX_CUDA_ERROR;
     }
     return VX_OK;

@@ -87,6 +87,7 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
 bool brick_plan(vx_scene* s, int form);
 bool expanded_plan(vx_scene* s);
 int32_t solve_inner_expanded(vx_scene* s, double tolerance, uint32_t max_iterations);
+int32_t solve_inner_slots_expanded(vx_scene* s, const uint4* d_blocks, SlotState* st, unsigned G, uint32_t cap);
 bool neighbor_deltas_fit(vx_scene* s);
 uint32_t persistent_block_cap();
 int32_t solve_inner_slots(vx_scene* s, const uint4* d_blocks, SlotState* st, unsigned G, uint32_t cap);

@@ -558,8 +558,13 @@ int32_t pool_solve(vx_pool* p, const vx_pass_params* prm, const std::vector<uint
         VX_POOL_TRY(cudaStreamSynchronize(st), "pool outer step");
         if (p->h_flag[0] == 0) break;
         if (waves) {
+            // the one-reduction form (vx_expanded.cu); VXCOROT_PERSISTENT=range
+            // keeps the classic two-reduction form of vx_persistent.cu
+            const char* form = std::getenv("VXCOROT_PERSISTENT");
+            const bool classic = form && std::strcmp(form, "range") == 0;
             for (const uint4& w : p->waves) {
-                int32_t r = solve_inner_slots(s, p->d_wave_rows + w.x, p->st, w.y, w.z);
+                int32_t r = classic ? solve_inner_slots(s, p->d_wave_rows + w.x, p->st, w.y, w.z)
+                                    : solve_inner_slots_expanded(s, p->d_wave_rows + w.x, p->st, w.y, w.z);
                 if (r != VX_OK) return r;
             }
             VX_POOL_TRY(cudaMemcpyAsync(&p->h_flag[3], s->barrier + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
