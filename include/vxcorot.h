@@ -603,7 +603,7 @@ void* vx_scene_stream(vx_scene* scene);
  *     (candidate_blocks = VX_PERSIST_*): the brick plan with one or two
  *     threads per REV and tiles of at least 256 or 128 REVs per block, and
  *     the contiguous-range plan with the classic two reductions per
- *     iteration or with one.
+ *     iteration (at 512, 608, 768 or 896 threads per block) or with one.
  * With cache_path (or NULL), a choice found there for this GPU, precision and
  * scene size (log2 of the REV count) is applied without timing, and a new
  * choice is stored. Positions and bond state are not changed; the solver's
@@ -615,6 +615,9 @@ void* vx_scene_stream(vx_scene* scene);
 #define VX_PERSIST_BRICK_T2_128 4   /* brick plan, 2 threads per REV, >= 128 REVs per block */
 #define VX_PERSIST_RANGE 5          /* contiguous-range plan (classic two-reduction recurrence) */
 #define VX_PERSIST_EXPANDED 6       /* contiguous-range plan, one reduction per iteration */
+#define VX_PERSIST_RANGE_608 7      /* contiguous-range plan, 608 threads per block (up to 3 REVs each) */
+#define VX_PERSIST_RANGE_768 8      /* contiguous-range plan, 768 threads per block (1 REV each) */
+#define VX_PERSIST_RANGE_896 9      /* contiguous-range plan, 896 threads per block (up to 2 REVs each) */
 typedef struct vx_tune_result {
     int32_t kernel;               /* VX_KERNEL_STREAMING or VX_KERNEL_PERSISTENT */
     int32_t blocks_per_sm;        /* streaming: register budget; persistent: VX_PERSIST_* form */

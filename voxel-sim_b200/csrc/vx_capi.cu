@@ -936,7 +936,7 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
                         if (kernel == VX_KERNEL_STREAMING) {
                             usable = blocks >= 3 && blocks <= 5;
                         } else if (kernel == VX_KERNEL_PERSISTENT && blocks >= VX_PERSIST_BRICK_T1_256 &&
-                                   blocks <= VX_PERSIST_EXPANDED) {
+                                   blocks <= VX_PERSIST_RANGE_896) {
                             const int old_form = s->persist_form;
                             apply_tuning(s, kernel, blocks);
                             usable = persistent_plan(s);
@@ -970,7 +970,7 @@ int32_t vx_scene_autotune(vx_scene* s, int32_t precision, const char* cache_path
         // threads per REV (a large scene reaches the same tiles from either
         // minimum) are timed once
         std::vector<std::array<unsigned, 3>> seen;
-        for (int form = VX_PERSIST_BRICK_T1_256; form <= VX_PERSIST_EXPANDED; ++form) {
+        for (int form = VX_PERSIST_BRICK_T1_256; form <= VX_PERSIST_RANGE_896; ++form) {
             s->persist_form = form;
             s->persist_checked = false;
             if (!persistent_plan(s)) continue;

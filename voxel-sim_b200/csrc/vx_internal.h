@@ -190,7 +190,7 @@ struct vx_scene {
     // persistent (on-chip) inner solve plan
     bool persist_checked = false;
     bool persist_ok = false;
-    unsigned persist_G = 0, persist_cap = 0, persist_R = 0;
+    unsigned persist_G = 0, persist_cap = 0, persist_R = 0, persist_T = 512;
     size_t persist_smem = 0;
     int nbcode_state = 0;         // 0 = not yet read back, 1 = all deltas encoded, 2 = some did not fit
     // brick plan of the on-chip inner solve (vx_brick.cu): blocks own spatially

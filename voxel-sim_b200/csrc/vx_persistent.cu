@@ -36,7 +36,7 @@ namespace vx {
 
 namespace {
 
-constexpr int kPThreads = 512;
+constexpr int kPThreads = 512;  // the pool waves' and the default range plan's block size
 // shared memory per REV: K float4[3] + float2[3], (z, p_old) float4 + float2,
 // three delta words, the mass term and one flag byte
 constexpr int kBytesPerRev = 3 * 16 + 3 * 8 + 16 + 8 + 12 + 4 + 1;
@@ -87,8 +87,11 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y
 // where used.
 // MULTI: the blocks work for several pool slots (a.blocks, a.st); otherwise
 // for one scene, whose reductions are grid_reduce's.
-template <int R, bool MULTI>
-__global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) {
+// TH threads per block: the register budget is 65,536 / TH (128 at 512, 107 at
+// 608, 85 at 768, 73 at 896), which holds R = 4, 3, 1 and 2 REVs per thread
+// without spills.
+template <int R, bool MULTI, int TH = kPThreads>
+__global__ void __launch_bounds__(TH, 1) k_pcg_persistent(PersistArgs a) {
     constexpr bool kPrefetch = R <= 2;
     extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
@@ -348,19 +351,32 @@ __global__ void __launch_bounds__(kPThreads, 1) k_pcg_persistent(PersistArgs a) 
     }
 }
 
-template <int R, bool MULTI>
+template <int R, bool MULTI, int TH = kPThreads>
 cudaError_t launch_r(const PersistArgs& a, unsigned G, size_t smem, cudaStream_t st) {
     cudaError_t e =
-        cudaFuncSetAttribute(k_pcg_persistent<R, MULTI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_pcg_persistent<R, MULTI, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     PersistArgs args = a;
     void* params[] = {&args};
-    return cudaLaunchCooperativeKernel((void*)k_pcg_persistent<R, MULTI>, dim3(G), dim3(kPThreads), params, smem, st);
+    return cudaLaunchCooperativeKernel((void*)k_pcg_persistent<R, MULTI, TH>, dim3(G), dim3(TH), params, smem, st);
+}
+
+// Threads per block of a range form, and the most REVs per thread it is built for.
+unsigned range_threads(int form) {
+    switch (form) {
+        case VX_PERSIST_RANGE_608: return 608;
+        case VX_PERSIST_RANGE_768: return 768;
+        case VX_PERSIST_RANGE_896: return 896;
+        default: return (unsigned)kPThreads;
+    }
+}
+unsigned range_max_revs_per_thread(unsigned th) {
+    return th <= 512 ? 4u : (th <= 608 ? 3u : (th <= 768 ? 1u : 2u));  // 2 at 768 spills
 }
 
 }  // namespace
 
-static bool range_plan(vx_scene* s);
+static bool range_plan(vx_scene* s, int form);
 
 // Whether the persistent inner solve fits this scene on this GPU; caches the
 // shape. Without a chosen form the range plan with one reduction per
@@ -383,9 +399,9 @@ bool persistent_plan(vx_scene* s) {
     }
     bool ok;
     if (form == VX_PERSIST_EXPANDED) ok = expanded_plan(s);
-    else if (form == VX_PERSIST_RANGE) ok = range_plan(s);
+    else if (form == VX_PERSIST_RANGE || form >= VX_PERSIST_RANGE_608) ok = range_plan(s, form);
     else if (form != 0) ok = brick_plan(s, form);
-    else ok = expanded_plan(s) || range_plan(s) || brick_plan(s, VX_PERSIST_BRICK_T1_256);
+    else ok = expanded_plan(s) || range_plan(s, VX_PERSIST_RANGE) || brick_plan(s, VX_PERSIST_BRICK_T1_256);
     s->persist_ok = ok;
     return ok;
 }
@@ -403,8 +419,9 @@ bool neighbor_deltas_fit(vx_scene* s) {
     return s->nbcode_state == 1;
 }
 
-// The contiguous-range plan: block b owns REVs [b cap, (b + 1) cap).
-static bool range_plan(vx_scene* s) {
+// The contiguous-range plan: block b owns REVs [b cap, (b + 1) cap), with the
+// block size of the form (range_threads).
+static bool range_plan(vx_scene* s, int form) {
     if (!neighbor_deltas_fit(s)) return false;
     int dev = s->device, max_smem = 0, coop = 0;
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -414,13 +431,16 @@ static bool range_plan(vx_scene* s) {
     unsigned min_blocks = (s->n + 255) / 256;  // at least 256 REVs per block
     if (min_blocks < G) G = min_blocks;
     if (G == 0) G = 1;
+    const unsigned TH = range_threads(form);
     unsigned cap = (s->n + G - 1) / G;
-    unsigned R = (cap + kPThreads - 1) / kPThreads;
+    unsigned R = (cap + TH - 1) / TH;
     size_t smem = ((size_t)kBytesPerRev * cap + 15) & ~size_t(15);
-    if (R > 4 || smem + 4096 > (size_t)max_smem) return false;
+    if (R > range_max_revs_per_thread(TH) || smem + 4096 > (size_t)max_smem) return false;
     s->persist_G = G;
     s->persist_cap = cap;
-    s->persist_R = R <= 1 ? 1 : (R <= 2 ? 2 : 4);
+    s->persist_T = TH;
+    // R = 3 only at 608 threads, whose budget is built for it
+    s->persist_R = R <= 1 ? 1 : (R <= 2 ? 2 : (TH == 608 ? 3 : 4));
     s->persist_smem = smem;
     return true;
 }
@@ -515,10 +535,18 @@ int32_t solve_inner_persistent(vx_scene* s, double tolerance, uint32_t max_itera
     }
     cudaError_t e = cudaMemsetAsync(s->barrier, 0, 4 * sizeof(unsigned), s->stream);
     if (e == cudaSuccess) {
-        switch (s->persist_R) {
-            case 1: e = launch_r<1, false>(a, s->persist_G, s->persist_smem, s->stream); break;
-            case 2: e = launch_r<2, false>(a, s->persist_G, s->persist_smem, s->stream); break;
-            default: e = launch_r<4, false>(a, s->persist_G, s->persist_smem, s->stream); break;
+        const unsigned G = s->persist_G;
+        const size_t sm = s->persist_smem;
+        switch (s->persist_T * 8 + s->persist_R) {
+            case 512 * 8 + 1: e = launch_r<1, false>(a, G, sm, s->stream); break;
+            case 512 * 8 + 2: e = launch_r<2, false>(a, G, sm, s->stream); break;
+            case 608 * 8 + 1: e = launch_r<1, false, 608>(a, G, sm, s->stream); break;
+            case 608 * 8 + 2: e = launch_r<2, false, 608>(a, G, sm, s->stream); break;
+            case 608 * 8 + 3: e = launch_r<3, false, 608>(a, G, sm, s->stream); break;
+            case 768 * 8 + 1: e = launch_r<1, false, 768>(a, G, sm, s->stream); break;
+            case 896 * 8 + 1: e = launch_r<1, false, 896>(a, G, sm, s->stream); break;
+            case 896 * 8 + 2: e = launch_r<2, false, 896>(a, G, sm, s->stream); break;
+            default: e = launch_r<4, false>(a, G, sm, s->stream); break;
         }
     }
     s->launches += 1;

@@ -123,7 +123,9 @@ FIELD_POSITION, FIELD_VELOCITY, FIELD_PREVIOUS = 0, 1, 2
 
 PERSIST_FORMS = {1: "brick, 1 thread/REV, >=256 REVs/block", 2: "brick, 2 threads/REV, >=256 REVs/block",
                  3: "brick, 1 thread/REV, >=128 REVs/block", 4: "brick, 2 threads/REV, >=128 REVs/block",
-                 5: "range (classic recurrence)", 6: "range (one reduction per iteration)"}
+                 5: "range (classic recurrence)", 6: "range (one reduction per iteration)",
+                 7: "range (classic recurrence), 608 threads/block", 8: "range (classic recurrence), 768 threads/block",
+                 9: "range (classic recurrence), 896 threads/block"}
 
 
 def tune_label(kernel: int, blocks: int) -> str:
