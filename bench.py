@@ -115,6 +115,20 @@ def workload_config(args, scene, world):
             "l2": "256 MiB buffer written between timed steps", "parallelism": f"replicas{world}"}
 
 
+def persistent_kernel_name(form, tuning):
+    """The on-chip kernel the scene's inner solve runs: its plan and, for the
+    range plan, the block size the autotuner chose (VX_PERSIST_RANGE_*)."""
+    from vxsim import native as N
+    if form == "brick":
+        return "k_pcg_brick"
+    if form == "expanded":
+        return "k_pcg_expanded, 512 threads/block"
+    threads = 512
+    if tuning and tuning.get("kernel") == N.KERNEL_PERSISTENT:
+        threads = N.RANGE_THREADS.get(tuning["blocks_per_sm"], 512)
+    return f"k_pcg_persistent, {threads} threads/block"
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -402,7 +416,7 @@ def our_arm(args):
         # streamed iteration (matvec + update + direction) per iteration time
         it_bytes = (BYTES_PER_REV["matvec_f32"] + BYTES_PER_REV["update_f32"] + BYTES_PER_REV["direction_f32"]) * active
         achieved = it_bytes / (cold["persistent_iter_us"] * 1e-6) / 1e9
-        kernel = "k_pcg_brick<4>" if cold["persistent_form"] == "brick" else "k_pcg_persistent<4>"
+        kernel = persistent_kernel_name(cold["persistent_form"], tuning)
         bytes_per_launch = it_bytes * cold["persistent_iterations"]
         launch_us = cold["persistent_iter_us"] * cold["persistent_iterations"]
         traffic = prof.get("persistent_dram_bytes_per_rev_iteration")

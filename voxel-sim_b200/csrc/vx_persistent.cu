@@ -383,7 +383,8 @@ static bool range_plan(vx_scene* s, int form);
 // iteration (vx_expanded.cu) is preferred, then the range plan below with the
 // classic two, then the brick plan (vx_brick.cu), which takes the scenes whose
 // neighbour deltas do not fit an int16. A chosen form (the autotuner's, or
-// VXCOROT_PERSISTENT=expanded|range|brick) is that form or nothing.
+// VXCOROT_PERSISTENT=expanded|range|range608|range768|range896|brick) is that
+// form or nothing.
 bool persistent_plan(vx_scene* s) {
     if (s->persist_checked) return s->persist_ok;
     s->persist_checked = true;
@@ -395,6 +396,9 @@ bool persistent_plan(vx_scene* s) {
     if (const char* v = std::getenv("VXCOROT_PERSISTENT")) {
         if (std::strcmp(v, "expanded") == 0) form = VX_PERSIST_EXPANDED;
         else if (std::strcmp(v, "range") == 0) form = VX_PERSIST_RANGE;
+        else if (std::strcmp(v, "range608") == 0) form = VX_PERSIST_RANGE_608;
+        else if (std::strcmp(v, "range768") == 0) form = VX_PERSIST_RANGE_768;
+        else if (std::strcmp(v, "range896") == 0) form = VX_PERSIST_RANGE_896;
         else if (std::strcmp(v, "brick") == 0) form = VX_PERSIST_BRICK_T1_256;
     }
     bool ok;

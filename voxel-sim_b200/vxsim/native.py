@@ -128,6 +128,10 @@ PERSIST_FORMS = {1: "brick, 1 thread/REV, >=256 REVs/block", 2: "brick, 2 thread
                  9: "range (classic recurrence), 896 threads/block"}
 
 
+# threads per block of the range-plan forms (VX_PERSIST_RANGE, _608, _768, _896)
+RANGE_THREADS = {5: 512, 7: 608, 8: 768, 9: 896}
+
+
 def tune_label(kernel: int, blocks: int) -> str:
     """Readable name of an autotuner candidate (kernel, blocks field)."""
     if kernel == KERNEL_PERSISTENT:
