@@ -378,11 +378,28 @@ unsigned range_max_revs_per_thread(unsigned th) {
 
 static bool range_plan(vx_scene* s, int form);
 
+// The on-chip form an untuned scene takes, by its REVs per block (cap): the
+// fastest form measured at that cap on mixed blocks (one autotuner run at
+// 24^3, 48^3 and 64^3: caps 256, 748 and 1,772): one reduction per iteration
+// up to 512 REVs per block, the classic range form at 768 threads up to 768,
+// at 896 threads up to 1,792, and at 512 threads above. A form that does not
+// fit falls through to the next.
+static bool untuned_plan(vx_scene* s) {
+    unsigned G = (unsigned)s->sm_count;
+    const unsigned min_blocks = (s->n + 255) / 256;
+    if (min_blocks < G) G = min_blocks;
+    if (G == 0) G = 1;
+    const unsigned cap = (s->n + G - 1) / G;
+    if (cap <= 512 && expanded_plan(s)) return true;
+    if (cap <= 768 && range_plan(s, VX_PERSIST_RANGE_768)) return true;
+    if (cap <= 1792 && range_plan(s, VX_PERSIST_RANGE_896)) return true;
+    return range_plan(s, VX_PERSIST_RANGE) || expanded_plan(s);
+}
+
 // Whether the persistent inner solve fits this scene on this GPU; caches the
-// shape. Without a chosen form the range plan with one reduction per
-// iteration (vx_expanded.cu) is preferred, then the range plan below with the
-// classic two, then the brick plan (vx_brick.cu), which takes the scenes whose
-// neighbour deltas do not fit an int16. A chosen form (the autotuner's, or
+// shape. Without a chosen form the scene takes untuned_plan's form, and the
+// brick plan (vx_brick.cu) where no range form fits (neighbour deltas beyond
+// an int16). A chosen form (the autotuner's, or
 // VXCOROT_PERSISTENT=expanded|range|range608|range768|range896|brick) is that
 // form or nothing.
 bool persistent_plan(vx_scene* s) {
@@ -405,7 +422,7 @@ bool persistent_plan(vx_scene* s) {
     if (form == VX_PERSIST_EXPANDED) ok = expanded_plan(s);
     else if (form == VX_PERSIST_RANGE || form >= VX_PERSIST_RANGE_608) ok = range_plan(s, form);
     else if (form != 0) ok = brick_plan(s, form);
-    else ok = expanded_plan(s) || range_plan(s, VX_PERSIST_RANGE) || brick_plan(s, VX_PERSIST_BRICK_T1_256);
+    else ok = untuned_plan(s) || brick_plan(s, VX_PERSIST_BRICK_T1_256);
     s->persist_ok = ok;
     return ok;
 }
