@@ -2,8 +2,8 @@
 // working set stays on chip.
 //
 // When a scene is small enough (up to ~2,000 REVs per SM), one cooperative
-// block of 512 threads per SM owns a contiguous range of REVs for the whole
-// inner solve. Shared memory holds, per REV of the range, the stiffness of its
+// block per SM (512, 608, 768 or 896 threads: the form's block size) owns a
+// contiguous range of REVs for the whole inner solve. Shared memory holds, per REV of the range, the stiffness of its
 // three owned bonds, the pair (z, p_old) as float4 + float2 records, its six
 // neighbour deltas as int16, its mass term m/h^2 and its free-axis flags, so an
 // in-range neighbour costs two vector loads from shared memory and no index
