@@ -85,3 +85,17 @@ def test_null_handles_are_rejected(lib):
     assert lib.vx_ctx_create(0, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_step(None, None, None) == N.VX_BAD_INPUT
     assert lib.vx_scene_update_velocities(None, 0, None, None, 0) == N.VX_BAD_INPUT
+
+
+def test_persistent_form_codes_match_the_header():
+    """The VX_PERSIST_* form codes of the header are the ones the binding names
+    (PERSIST_FORMS) and, for the range plan, sizes (RANGE_THREADS)."""
+    import re
+    text = (ROOT / "include" / "vxcorot.h").read_text()
+    codes = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define (VX_PERSIST_\w+) (\d+)", text)}
+    assert set(codes.values()) == set(N.PERSIST_FORMS), codes
+    assert {codes["VX_PERSIST_RANGE"], codes["VX_PERSIST_RANGE_608"], codes["VX_PERSIST_RANGE_768"],
+            codes["VX_PERSIST_RANGE_896"]} == set(N.RANGE_THREADS)
+    for name, threads in (("VX_PERSIST_RANGE", 512), ("VX_PERSIST_RANGE_608", 608), ("VX_PERSIST_RANGE_768", 768),
+                          ("VX_PERSIST_RANGE_896", 896)):
+        assert N.RANGE_THREADS[codes[name]] == threads
