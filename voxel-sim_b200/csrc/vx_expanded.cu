@@ -34,6 +34,11 @@
 // owned bonds (72 B), its triple (36 B: float4 (u, v.x), float4 (v.y, v.z,
 // p.x, p.y), float p.z), its six int16 neighbour deltas (12 B), m/h^2 (4 B)
 // and the free-axis flags (1 B): 125 B, 1,772 REVs in 221 KB at 64^3.
+//
+// Compiled with MULTI the same kernel runs a pool's persistent waves
+// (solve_inner_slots_expanded): a wave's blocks serve several slots, each slot
+// summed over its own blocks, with the grid's count of working blocks as an
+// eighth row of the one reduction.
 #include <cstdlib>
 #include <cstring>
 
