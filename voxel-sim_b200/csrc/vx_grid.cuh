@@ -92,6 +92,77 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], const int (&slot)[N
     return *s_ok != 0;
 }
 
+// grid_reduce in two halves, so that a block can work between its arrival
+// and the wait: grid_arrive sums the block's NV values and publishes them
+// (the __syncthreads in it also makes this block's shared-memory stores
+// visible to all its threads); grid_complete waits for every block's arrival
+// at reduction `seq` and returns the totals, in the same bits as grid_reduce.
+// Between the two a block may not write a partial row or `sh`.
+template <int NV, class A>
+__device__ __forceinline__ void grid_arrive(double (&v)[NV], const int (&slot)[NV], const A& a, double (*sh)[32]) {
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5, G = gridDim.x;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][warp] = v[k];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        double b[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) b[k] = warp_sum(lane < nw ? sh[k][lane] : 0.0);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) a.part[(size_t)slot[k] * G + blockIdx.x] = b[k];
+            red_release_add_u64(a.count, 1ull);
+        }
+    }
+}
+
+template <int NV, class A>
+__device__ __forceinline__ bool grid_complete(const int (&slot)[NV], const A& a, unsigned long long seq, double* tot,
+                                             int* s_ok, double (&out)[NV]) {
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31, G = gridDim.x;
+    if (warp == 0) {
+        int ok = 1;
+        if (lane == 0) {
+            const unsigned long long target = seq * G;
+            unsigned long long spins = 0;
+            while (ld_acquire_u64(a.count) < target) {
+                if (++spins >= a.spin_limit || ((spins & 63) == 0 && *(volatile int32_t*)a.err)) {
+                    ok = 0;
+                    break;
+                }
+            }
+            if (!ok) atomicExch(a.err, 1);
+            else if (*(volatile int32_t*)a.err) ok = 0;
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        double t[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = 0.0;
+        if (ok) {
+            for (unsigned blk = lane; blk < G; blk += 32) {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) t[k] += __ldcg(a.part + (size_t)slot[k] * G + blk);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = warp_sum(t[k]);
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) tot[k] = t[k];
+            *s_ok = ok;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = tot[k];
+    return *s_ok != 0;
+}
+
 // grid_reduce for blocks that work for different problems (the slots of a
 // pool): the NV values are summed over the blocks [fb, fb + nb) of this block's
 // own problem, in block order, and `act` over all G blocks (a count of blocks

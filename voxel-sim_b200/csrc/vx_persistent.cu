@@ -3,18 +3,27 @@
 //
 // When a scene is small enough (up to ~2,000 REVs per SM), one cooperative
 // block per SM (512, 608, 768 or 896 threads: the form's block size) owns a
-// contiguous range of REVs for the whole inner solve. Shared memory holds, per REV of the range, the stiffness of its
-// three owned bonds, the pair (z, p_old) as float4 + float2 records, its six
-// neighbour deltas as int16, its mass term m/h^2 and its free-axis flags, so an
-// in-range neighbour costs two vector loads from shared memory and no index
-// load. x, r, p and Ap live in registers of the owning thread. The operator is
-// the FP32 row of apply_row (vx_pcg_core.cuh): the diagonal comes from the
-// mass term and the bonds, so only its inverse is read from L2 (issued before
-// the grid wait when registers allow).
-// Neighbours outside the range are read from the global copy of (z, p_old),
-// which every block republishes once per iteration. An iteration is the
-// recurrence of k_matvec/k_update in vx_pcg.cu (src/solver.rs:1833-1911) with
-// two grid-wide reductions:
+// contiguous range of REVs for the whole inner solve. Shared memory holds, per
+// REV of the range, the stiffness of its three owned bonds, a float4 + float2
+// record of the iteration's vectors, its six neighbour deltas as int16, its
+// mass term m/h^2 and its free-axis flags, so an in-range neighbour costs
+// vector loads from shared memory and no index load. x, r, p and Ap live in
+// registers of the owning thread. The operator is the FP32 row of apply_row
+// (vx_pcg_core.cuh): the diagonal comes from the mass term and the bonds, so
+// only its inverse is read from L2. Neighbours outside the range are read from
+// a global copy that every block republishes once per iteration. An iteration
+// is the recurrence of k_matvec/k_update in vx_pcg.cu (src/solver.rs:1833-1911)
+// with two grid-wide reductions.
+//
+// One scene: neighbours read z alone, and Ap is formed as A z + beta Ap_old
+// (A is linear, its projection included). The part of A z that needs only the
+// block's own z (the mass term and the in-range bonds) is computed after the
+// block has arrived at reduction B and before it waits there; the out-of-range
+// bonds are added once B has made every block's z visible:
+//   matvec phase  p = z + beta p_old, Ap += out-of-range bonds, p.Ap -> reduction A
+//   update phase  alpha, x, r, z = D^-1 r, partials of r.z, r.r     -> reduction B
+//                 (arrival, the in-range part of A z, the wait)
+// Pools (MULTI): neighbours read the pair (z, p_old) and form p_j themselves:
 //   matvec phase  p = z + beta p_old, Ap, block partial of p.Ap   -> reduction A
 //   update phase  alpha, x, r, z = D^-1 r, partials of r.z, r.r   -> reduction B
 // A reduction is also the grid barrier: a block stores its partial, adds one
@@ -83,8 +92,8 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y
 
 // R REVs per thread. With R <= 2 the inverse diagonal block is loaded into
 // registers before the grid wait of the matvec phase, so its L2 latency
-// overlaps the wait; at R = 4 the registers are not there and it is loaded
-// where used.
+// overlaps the wait; at R = 3 and 4, and for one scene at 896 threads, the
+// registers are not there and it is loaded where used.
 // MULTI: the blocks work for several pool slots (a.blocks, a.st); otherwise
 // for one scene, whose reductions are grid_reduce's.
 // TH threads per block: the register budget is 65,536 / TH (128 at 512, 107 at
@@ -92,7 +101,7 @@ __device__ __forceinline__ float dot3(F3 a, F3 b) { return a.x * b.x + a.y * b.y
 // without spills.
 template <int R, bool MULTI, int TH = kPThreads>
 __global__ void __launch_bounds__(TH, 1) k_pcg_persistent(PersistArgs a) {
-    constexpr bool kPrefetch = R <= 2;
+    constexpr bool kPrefetch = R <= 2 && (MULTI || TH != 896);
     extern __shared__ float4 smem4[];
     __shared__ double red[3][32];
     __shared__ double tot[4];
@@ -137,176 +146,170 @@ __global__ void __launch_bounds__(TH, 1) k_pcg_persistent(PersistArgs a) {
         sFL[li] = __ldg(a.flags + i);
     }
 
-    float x[R][3], r[R][3], p[R][3], ap[R][3];
-    Sym<float> ireg[kPrefetch ? R : 1];
-    const double scale = scale_norm > 0.0 ? 1.0 / scale_norm : 1.0;
-    double acc[2] = {0.0, 0.0};
+    if constexpr (!MULTI) {
+        // One scene. The direction's product is formed as q = A z + beta q_old
+        // (A is linear, its projection included), so the part of A z that
+        // needs only this block's z (the mass term and the in-range bonds) is
+        // computed between the block's arrival at the r.z reduction and its
+        // wait there; the out-of-range bonds are added after the reduction
+        // has made every block's z visible. Neighbours read z alone: from
+        // shared memory in range (sZP4 .xyz) and from the global copy (zp4,
+        // (z, 0)) outside it. The in-range part w waits in the REV's own
+        // shared slots, sZP4.w and sZP2, which neighbours do not read.
+        float x[R][3], r[R][3], p[R][3], q[R][3];
+        Sym<float> ireg[kPrefetch ? R : 1];
+        const double scale = scale_norm > 0.0 ? 1.0 / scale_norm : 1.0;
+        // w = m/h^2 z + sum over in-range bonds of K (z_i - z_j), before the projection
+        auto in_range = [&]() {
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const uint32_t li = threadIdx.x + k * T;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = ap[k][c] = r[k][c] = 0.f;
-        if (li < cnt) {
-            const size_t i = lo + li;
-            const F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale),
-                           (float)(a.src[2 * (size_t)n + i] * scale)};
-            const F3 z = smul(load_sym(a.Dinv, n, i), rr);
-            r[k][0] = rr.x, r[k][1] = rr.y, r[k][2] = rr.z;
-            const float4 q4 = make_float4(z.x, z.y, z.z, 0.f);
-            const float2 q2 = make_float2(0.f, 0.f);
-            sZP4[li] = q4, sZP2[li] = q2;
-            a.zp4[i] = q4, a.zp2[i] = q2;
-            acc[0] += (double)dot3(rr, z);
-            acc[1] += (double)dot3(rr, rr);
-        }
-    }
-    unsigned long long seq = 1;
-    const int su[2] = {1, 2};
-    const int sm[1] = {0};
-    constexpr int kActRow = 3;
-    double t2[2], act = 0.0;
-    // only the matvec-phase reductions carry the count of working blocks (row
-    // kActRow): two of them always have a reduction, so a grid barrier, between
-    bool alive;
-    if constexpr (MULTI) alive = grid_reduce_ranged<2>(acc, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, t2, &act);
-    else alive = grid_reduce<2>(acc, su, a, seq++, red, tot, &s_ok, t2);
-    const double initial = sqrt(t2[1]);
-    double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
-    uint32_t its = 0;
-    int32_t status = alive ? VX_OK : VX_TIMEOUT;
-    if (alive && mine) {
-        if (!isfinite(t2[0]) || !isfinite(t2[1])) {
-            mine = false;
-            status = VX_NONFINITE;
-        } else if (!(initial > 1e-12)) {
-            mine = false;
-        } else if (max_iterations == 0) {
-            mine = false;
-            status = VX_NOT_CONVERGED;
-        }
-    }
-
-    // A problem that has stopped leaves its blocks idle; in a pool they keep
-    // taking part in the reductions until no block of the grid has work left,
-    // so every block leaves the loop at the same reduction. One scene is one
-    // problem: its blocks leave together as soon as it stops.
-    while (alive) {
-        if (!MULTI && !mine) break;
-        const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
-        // ---- matvec phase: p = z + beta p_old,
-        //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
-        double pap[1] = {0.0};
-        const uint32_t cnt_now = mine ? cnt : 0;
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-            const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt_now) continue;
-            const uint32_t i = lo + li;
-            int32_t dl[6];
-#pragma unroll
-            for (int w = 0; w < 3; ++w) {
-                const uint32_t c = sNB[w * cap + li];
-                dl[2 * w] = (int32_t)(int16_t)(c & 0xffffu);
-                dl[2 * w + 1] = (int32_t)(int16_t)(c >> 16);
-            }
-            const uint8_t fl = sFL[li];
-            const float4 o4 = sZP4[li];
-            const float2 o2 = sZP2[li];
-            const F3 pi = {fmaf(beta, o4.w, o4.x), fmaf(beta, o2.x, o4.y), fmaf(beta, o2.y, o4.z)};
-            const float mh = sM[li];
-            F3 s = {mh * pi.x, mh * pi.y, mh * pi.z};
-#pragma unroll
-            for (int t = 0; t < 6; ++t) {
-                const uint32_t j = (uint32_t)((int32_t)i + dl[t]);
-                const int ax = t < 3 ? t : t - 3;
-                const uint32_t lj = j - lo;
-                const bool inb = lj < cnt;
-                float4 q4;
-                float2 q2;
-                Sym<float> Kb;
-                if (inb) {
-                    q4 = sZP4[lj], q2 = sZP2[lj];
-                } else {
-                    q4 = __ldcg(a.zp4 + j), q2 = __ldcg(a.zp2 + j);
-                }
-                if (t < 3) {
-                    Kb = sym_of(sK4[ax * cap + li], sK2[ax * cap + li]);
-                } else if (inb) {
-                    Kb = sym_of(sK4[ax * cap + lj], sK2[ax * cap + lj]);
-                } else {
-                    Kb = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
-                }
-                const F3 pn = {fmaf(beta, q4.w, q4.x), fmaf(beta, q2.x, q4.y), fmaf(beta, q2.y, q4.z)};
-                // a missing neighbour has delta 0: j = i, pn = pi and d = 0 exactly
-                const F3 d = {pi.x - pn.x, pi.y - pn.y, pi.z - pn.z};
-                const F3 kv = smul(Kb, d);
-                s.x += kv.x, s.y += kv.y, s.z += kv.z;
-            }
-            const F3 y = {(fl & 1) ? s.x : pi.x, (fl & 2) ? s.y : pi.y, (fl & 4) ? s.z : pi.z};
-            p[k][0] = pi.x, p[k][1] = pi.y, p[k][2] = pi.z;
-            ap[k][0] = y.x, ap[k][1] = y.y, ap[k][2] = y.z;
-            pap[0] += (double)dot3(pi, y);
-        }
-        if constexpr (kPrefetch) {
-#pragma unroll
-            for (int k = 0; k < R; ++k) {  // in flight during the wait below
+            for (int k = 0; k < R; ++k) {
                 const uint32_t li = threadIdx.x + k * T;
-                if (li < cnt_now) ireg[k] = load_sym(a.Dinv, n, lo + li);
+                if (li >= cnt) continue;
+                const uint32_t i = lo + li;
+                const float4 zi = sZP4[li];
+                const float mh = sM[li];
+                F3 s = {mh * zi.x, mh * zi.y, mh * zi.z};
+#pragma unroll
+                for (int t = 0; t < 6; ++t) {
+                    const uint32_t c = sNB[(t >> 1) * cap + li];
+                    const int32_t dl = (int32_t)(int16_t)((t & 1) ? (c >> 16) : (c & 0xffffu));
+                    const uint32_t lj = (uint32_t)((int32_t)i + dl) - lo;
+                    if (lj >= cnt) continue;
+                    const int ax = t < 3 ? t : t - 3;
+                    const uint32_t ks = ax * cap + (t < 3 ? li : lj);
+                    const Sym<float> Kb = sym_of(sK4[ks], sK2[ks]);
+                    const float4 zj = sZP4[lj];
+                    // a missing neighbour has delta 0: j = i and d = 0 exactly
+                    const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
+                    s.x += kv.x, s.y += kv.y, s.z += kv.z;
+                }
+                reinterpret_cast<float*>(sZP4 + li)[3] = s.x;
+                sZP2[li] = make_float2(s.y, s.z);
             }
-        }
-        double t1[1];
-        bool ok_a;
-        if constexpr (MULTI)
-            ok_a = grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t1, &act);
-        else
-            ok_a = grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1);
-        if (!ok_a) {
-            status = VX_TIMEOUT;
-            break;
-        }
-        if (MULTI && act == 0.0) break;  // no block of the grid has work left
-        const double pap_all = t1[0];
-        if (mine && (!isfinite(pap_all) || pap_all <= 1e-30)) {
-            its += 1;  // the matvec happened (src/solver.rs:1861-1866)
-            if (!isfinite(pap_all)) status = VX_NONFINITE;
-            mine = false;
-            if (!MULTI) break;
-        }
-        const float alpha = mine ? (float)(rz / pap_all) : 0.f;
-        // ---- update phase; every block has read the old (z, p_old): publish the new ----
-        double au[2] = {0.0, 0.0};
-        const uint32_t cnt_up = mine ? cnt : 0;
+        };
+        double acc[2] = {0.0, 0.0};
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             const uint32_t li = threadIdx.x + k * T;
-            if (li >= cnt_up) continue;
-            const size_t i = lo + li;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                x[k][c] = fmaf(alpha, p[k][c], x[k][c]);
-                r[k][c] = fmaf(-alpha, ap[k][c], r[k][c]);
+            for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = q[k][c] = r[k][c] = 0.f;
+            if (li < cnt) {
+                const size_t i = lo + li;
+                const F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale),
+                               (float)(a.src[2 * (size_t)n + i] * scale)};
+                const F3 z = smul(load_sym(a.Dinv, n, i), rr);
+                r[k][0] = rr.x, r[k][1] = rr.y, r[k][2] = rr.z;
+                const float4 z4 = make_float4(z.x, z.y, z.z, 0.f);
+                sZP4[li] = z4;
+                a.zp4[i] = z4;
+                acc[0] += (double)dot3(rr, z);
+                acc[1] += (double)dot3(rr, rr);
             }
-            const F3 rr = {r[k][0], r[k][1], r[k][2]};
-            Sym<float> Di;
-            if constexpr (kPrefetch) Di = ireg[k];
-            else Di = load_sym(a.Dinv, n, i);
-            const F3 z = smul(Di, rr);
-            const float4 q4 = make_float4(z.x, z.y, z.z, p[k][0]);
-            const float2 q2 = make_float2(p[k][1], p[k][2]);
-            sZP4[li] = q4, sZP2[li] = q2;
-            a.zp4[i] = q4, a.zp2[i] = q2;
-            au[0] += (double)dot3(rr, z);
-            au[1] += (double)dot3(rr, rr);
         }
-        double tu[2], act_u = 0.0;
-        bool ok_b;
-        if constexpr (MULTI) ok_b = grid_reduce_ranged<2>(au, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u);
-        else ok_b = grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu);
-        if (!ok_b) {
-            status = VX_TIMEOUT;
-            break;
+        unsigned long long seq = 1;
+        const int su[2] = {1, 2};
+        const int sm[1] = {0};
+        double t2[2];
+        grid_arrive<2>(acc, su, a, red);
+        in_range();
+        const bool alive = grid_complete<2>(su, a, seq++, tot, &s_ok, t2);
+        const double initial = sqrt(t2[1]);
+        double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
+        uint32_t its = 0;
+        int32_t status = alive ? VX_OK : VX_TIMEOUT;
+        if (alive) {
+            if (!isfinite(t2[0]) || !isfinite(t2[1])) {
+                mine = false;
+                status = VX_NONFINITE;
+            } else if (!(initial > 1e-12)) {
+                mine = false;
+            } else if (max_iterations == 0) {
+                mine = false;
+                status = VX_NOT_CONVERGED;
+            }
         }
-        if (mine) {
+        while (alive && mine) {
+            const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
+            // ---- matvec phase: p = z + beta p_old, q = A z + beta q_old ----
+            double pq[1] = {0.0};
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const uint32_t li = threadIdx.x + k * T;
+                if (li >= cnt) continue;
+                const uint32_t i = lo + li;
+                const float4 zi = sZP4[li];  // (z, w.x)
+                const float2 wyz = sZP2[li];
+                F3 s = {zi.w, wyz.x, wyz.y};
+#pragma unroll
+                for (int t = 0; t < 6; ++t) {
+                    const uint32_t c = sNB[(t >> 1) * cap + li];
+                    const int32_t dl = (int32_t)(int16_t)((t & 1) ? (c >> 16) : (c & 0xffffu));
+                    const uint32_t j = (uint32_t)((int32_t)i + dl);
+                    if (j - lo < cnt) continue;
+                    const int ax = t < 3 ? t : t - 3;
+                    const Sym<float> Kb = t < 3 ? sym_of(sK4[ax * cap + li], sK2[ax * cap + li])
+                                                : load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
+                    const float4 zj = __ldcg(a.zp4 + j);
+                    const F3 kv = smul(Kb, F3{zi.x - zj.x, zi.y - zj.y, zi.z - zj.z});
+                    s.x += kv.x, s.y += kv.y, s.z += kv.z;
+                }
+                const uint8_t fl = sFL[li];
+                const F3 y = {(fl & 1) ? s.x : zi.x, (fl & 2) ? s.y : zi.y, (fl & 4) ? s.z : zi.z};
+                p[k][0] = fmaf(beta, p[k][0], zi.x), p[k][1] = fmaf(beta, p[k][1], zi.y),
+                p[k][2] = fmaf(beta, p[k][2], zi.z);
+                q[k][0] = fmaf(beta, q[k][0], y.x), q[k][1] = fmaf(beta, q[k][1], y.y),
+                q[k][2] = fmaf(beta, q[k][2], y.z);
+                pq[0] += (double)dot3(F3{p[k][0], p[k][1], p[k][2]}, F3{q[k][0], q[k][1], q[k][2]});
+            }
+            if constexpr (kPrefetch) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {  // in flight during the wait below
+                    const uint32_t li = threadIdx.x + k * T;
+                    if (li < cnt) ireg[k] = load_sym(a.Dinv, n, lo + li);
+                }
+            }
+            double t1[1];
+            if (!grid_reduce<1>(pq, sm, a, seq++, red, tot, &s_ok, t1)) {
+                status = VX_TIMEOUT;
+                break;
+            }
+            const double pq_all = t1[0];
+            if (!isfinite(pq_all) || pq_all <= 1e-30) {
+                its += 1;  // the matvec happened (src/solver.rs:1861-1866)
+                if (!isfinite(pq_all)) status = VX_NONFINITE;
+                break;
+            }
+            const float alpha = (float)(rz / pq_all);
+            // ---- update phase; every block has read the old z: publish the new ----
+            double au[2] = {0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const uint32_t li = threadIdx.x + k * T;
+                if (li >= cnt) continue;
+                const size_t i = lo + li;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    x[k][c] = fmaf(alpha, p[k][c], x[k][c]);
+                    r[k][c] = fmaf(-alpha, q[k][c], r[k][c]);
+                }
+                const F3 rr = {r[k][0], r[k][1], r[k][2]};
+                Sym<float> Di;
+                if constexpr (kPrefetch) Di = ireg[k];
+                else Di = load_sym(a.Dinv, n, i);
+                const F3 z = smul(Di, rr);
+                const float4 z4 = make_float4(z.x, z.y, z.z, 0.f);
+                sZP4[li] = z4;
+                a.zp4[i] = z4;
+                au[0] += (double)dot3(rr, z);
+                au[1] += (double)dot3(rr, rr);
+            }
+            double tu[2];
+            grid_arrive<2>(au, su, a, red);
+            in_range();  // overlaps the other blocks' arrivals
+            if (!grid_complete<2>(su, a, seq++, tot, &s_ok, tu)) {
+                status = VX_TIMEOUT;
+                break;
+            }
             its += 1;
             residual = sqrt(tu[1]) / initial;
             if (!isfinite(tu[0]) || !isfinite(tu[1])) {
@@ -318,35 +321,237 @@ __global__ void __launch_bounds__(TH, 1) k_pcg_persistent(PersistArgs a) {
                 status = VX_NOT_CONVERGED;
                 mine = false;
             }
+            rz_prev = rz;
+            rz = tu[0];
         }
-        rz_prev = rz;
-        rz = tu[0];
-    }
-    if (*(volatile int32_t*)a.err) status = VX_TIMEOUT;
+        if (*(volatile int32_t*)a.err) status = VX_TIMEOUT;
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const uint32_t li = threadIdx.x + k * T;
-        if (li >= cnt) continue;
-        const size_t i = lo + li;
-        a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
-    }
-    if (threadIdx.x == 0 && blockIdx.x == fb) {
-        if constexpr (MULTI) {
-            SlotState& S = a.st[slot];
-            if (S.enabled && S.inner_on) {
-                S.its = its;
-                S.residual_in = residual;
-                S.initial = initial;
-                S.status_in = status;
-                S.done = 1;
-            }
-        } else {
+        for (int k = 0; k < R; ++k) {
+            const uint32_t li = threadIdx.x + k * T;
+            if (li >= cnt) continue;
+            const size_t i = lo + li;
+            a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
+        }
+        if (threadIdx.x == 0 && blockIdx.x == 0) {
             PcgScalars* sc = a.sc;
             sc->iterations = its;
             sc->residual = residual;
             sc->initial = initial;
             sc->status = status;
             sc->done = 1;
+        }
+    } else {
+        float x[R][3], r[R][3], p[R][3], ap[R][3];
+        Sym<float> ireg[kPrefetch ? R : 1];
+        const double scale = scale_norm > 0.0 ? 1.0 / scale_norm : 1.0;
+        double acc[2] = {0.0, 0.0};
+    #pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t li = threadIdx.x + k * T;
+    #pragma unroll
+            for (int c = 0; c < 3; ++c) x[k][c] = p[k][c] = ap[k][c] = r[k][c] = 0.f;
+            if (li < cnt) {
+                const size_t i = lo + li;
+                const F3 rr = {(float)(a.src[i] * scale), (float)(a.src[n + i] * scale),
+                               (float)(a.src[2 * (size_t)n + i] * scale)};
+                const F3 z = smul(load_sym(a.Dinv, n, i), rr);
+                r[k][0] = rr.x, r[k][1] = rr.y, r[k][2] = rr.z;
+                const float4 q4 = make_float4(z.x, z.y, z.z, 0.f);
+                const float2 q2 = make_float2(0.f, 0.f);
+                sZP4[li] = q4, sZP2[li] = q2;
+                a.zp4[i] = q4, a.zp2[i] = q2;
+                acc[0] += (double)dot3(rr, z);
+                acc[1] += (double)dot3(rr, rr);
+            }
+        }
+        unsigned long long seq = 1;
+        const int su[2] = {1, 2};
+        const int sm[1] = {0};
+        constexpr int kActRow = 3;
+        double t2[2], act = 0.0;
+        // only the matvec-phase reductions carry the count of working blocks (row
+        // kActRow): two of them always have a reduction, so a grid barrier, between
+        bool alive;
+        if constexpr (MULTI) alive = grid_reduce_ranged<2>(acc, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, t2, &act);
+        else alive = grid_reduce<2>(acc, su, a, seq++, red, tot, &s_ok, t2);
+        const double initial = sqrt(t2[1]);
+        double rz = t2[0], rz_prev = INFINITY, residual = 0.0;
+        uint32_t its = 0;
+        int32_t status = alive ? VX_OK : VX_TIMEOUT;
+        if (alive && mine) {
+            if (!isfinite(t2[0]) || !isfinite(t2[1])) {
+                mine = false;
+                status = VX_NONFINITE;
+            } else if (!(initial > 1e-12)) {
+                mine = false;
+            } else if (max_iterations == 0) {
+                mine = false;
+                status = VX_NOT_CONVERGED;
+            }
+        }
+
+        // A problem that has stopped leaves its blocks idle; in a pool they keep
+        // taking part in the reductions until no block of the grid has work left,
+        // so every block leaves the loop at the same reduction. One scene is one
+        // problem: its blocks leave together as soon as it stops.
+        while (alive) {
+            if (!MULTI && !mine) break;
+            const float beta = its == 0 ? 0.f : (float)(rz / rz_prev);
+            // ---- matvec phase: p = z + beta p_old,
+            //      Ap = P (m/h^2 p + sum K (p - p_nbr)) + (I - P) p ----
+            double pap[1] = {0.0};
+            const uint32_t cnt_now = mine ? cnt : 0;
+    #pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const uint32_t li = threadIdx.x + k * T;
+                if (li >= cnt_now) continue;
+                const uint32_t i = lo + li;
+                int32_t dl[6];
+    #pragma unroll
+                for (int w = 0; w < 3; ++w) {
+                    const uint32_t c = sNB[w * cap + li];
+                    dl[2 * w] = (int32_t)(int16_t)(c & 0xffffu);
+                    dl[2 * w + 1] = (int32_t)(int16_t)(c >> 16);
+                }
+                const uint8_t fl = sFL[li];
+                const float4 o4 = sZP4[li];
+                const float2 o2 = sZP2[li];
+                const F3 pi = {fmaf(beta, o4.w, o4.x), fmaf(beta, o2.x, o4.y), fmaf(beta, o2.y, o4.z)};
+                const float mh = sM[li];
+                F3 s = {mh * pi.x, mh * pi.y, mh * pi.z};
+    #pragma unroll
+                for (int t = 0; t < 6; ++t) {
+                    const uint32_t j = (uint32_t)((int32_t)i + dl[t]);
+                    const int ax = t < 3 ? t : t - 3;
+                    const uint32_t lj = j - lo;
+                    const bool inb = lj < cnt;
+                    float4 q4;
+                    float2 q2;
+                    Sym<float> Kb;
+                    if (inb) {
+                        q4 = sZP4[lj], q2 = sZP2[lj];
+                    } else {
+                        q4 = __ldcg(a.zp4 + j), q2 = __ldcg(a.zp2 + j);
+                    }
+                    if (t < 3) {
+                        Kb = sym_of(sK4[ax * cap + li], sK2[ax * cap + li]);
+                    } else if (inb) {
+                        Kb = sym_of(sK4[ax * cap + lj], sK2[ax * cap + lj]);
+                    } else {
+                        Kb = load_sym(a.K + (size_t)ax * 6 * a.kn, a.kn, j);
+                    }
+                    const F3 pn = {fmaf(beta, q4.w, q4.x), fmaf(beta, q2.x, q4.y), fmaf(beta, q2.y, q4.z)};
+                    // a missing neighbour has delta 0: j = i, pn = pi and d = 0 exactly
+                    const F3 d = {pi.x - pn.x, pi.y - pn.y, pi.z - pn.z};
+                    const F3 kv = smul(Kb, d);
+                    s.x += kv.x, s.y += kv.y, s.z += kv.z;
+                }
+                const F3 y = {(fl & 1) ? s.x : pi.x, (fl & 2) ? s.y : pi.y, (fl & 4) ? s.z : pi.z};
+                p[k][0] = pi.x, p[k][1] = pi.y, p[k][2] = pi.z;
+                ap[k][0] = y.x, ap[k][1] = y.y, ap[k][2] = y.z;
+                pap[0] += (double)dot3(pi, y);
+            }
+            if constexpr (kPrefetch) {
+    #pragma unroll
+                for (int k = 0; k < R; ++k) {  // in flight during the wait below
+                    const uint32_t li = threadIdx.x + k * T;
+                    if (li < cnt_now) ireg[k] = load_sym(a.Dinv, n, lo + li);
+                }
+            }
+            double t1[1];
+            bool ok_a;
+            if constexpr (MULTI)
+                ok_a = grid_reduce_ranged<1>(pap, mine ? 1.0 : 0.0, sm, kActRow, a, seq++, fb, nb, red, tot, &s_ok, t1, &act);
+            else
+                ok_a = grid_reduce<1>(pap, sm, a, seq++, red, tot, &s_ok, t1);
+            if (!ok_a) {
+                status = VX_TIMEOUT;
+                break;
+            }
+            if (MULTI && act == 0.0) break;  // no block of the grid has work left
+            const double pap_all = t1[0];
+            if (mine && (!isfinite(pap_all) || pap_all <= 1e-30)) {
+                its += 1;  // the matvec happened (src/solver.rs:1861-1866)
+                if (!isfinite(pap_all)) status = VX_NONFINITE;
+                mine = false;
+                if (!MULTI) break;
+            }
+            const float alpha = mine ? (float)(rz / pap_all) : 0.f;
+            // ---- update phase; every block has read the old (z, p_old): publish the new ----
+            double au[2] = {0.0, 0.0};
+            const uint32_t cnt_up = mine ? cnt : 0;
+    #pragma unroll
+            for (int k = 0; k < R; ++k) {
+                const uint32_t li = threadIdx.x + k * T;
+                if (li >= cnt_up) continue;
+                const size_t i = lo + li;
+    #pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    x[k][c] = fmaf(alpha, p[k][c], x[k][c]);
+                    r[k][c] = fmaf(-alpha, ap[k][c], r[k][c]);
+                }
+                const F3 rr = {r[k][0], r[k][1], r[k][2]};
+                Sym<float> Di;
+                if constexpr (kPrefetch) Di = ireg[k];
+                else Di = load_sym(a.Dinv, n, i);
+                const F3 z = smul(Di, rr);
+                const float4 q4 = make_float4(z.x, z.y, z.z, p[k][0]);
+                const float2 q2 = make_float2(p[k][1], p[k][2]);
+                sZP4[li] = q4, sZP2[li] = q2;
+                a.zp4[i] = q4, a.zp2[i] = q2;
+                au[0] += (double)dot3(rr, z);
+                au[1] += (double)dot3(rr, rr);
+            }
+            double tu[2], act_u = 0.0;
+            bool ok_b;
+            if constexpr (MULTI) ok_b = grid_reduce_ranged<2>(au, 0.0, su, -1, a, seq++, fb, nb, red, tot, &s_ok, tu, &act_u);
+            else ok_b = grid_reduce<2>(au, su, a, seq++, red, tot, &s_ok, tu);
+            if (!ok_b) {
+                status = VX_TIMEOUT;
+                break;
+            }
+            if (mine) {
+                its += 1;
+                residual = sqrt(tu[1]) / initial;
+                if (!isfinite(tu[0]) || !isfinite(tu[1])) {
+                    status = VX_NONFINITE;
+                    mine = false;
+                } else if (residual < tolerance) {
+                    mine = false;
+                } else if (its >= max_iterations) {
+                    status = VX_NOT_CONVERGED;
+                    mine = false;
+                }
+            }
+            rz_prev = rz;
+            rz = tu[0];
+        }
+        if (*(volatile int32_t*)a.err) status = VX_TIMEOUT;
+    #pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t li = threadIdx.x + k * T;
+            if (li >= cnt) continue;
+            const size_t i = lo + li;
+            a.x[i] = x[k][0], a.x[n + i] = x[k][1], a.x[2 * (size_t)n + i] = x[k][2];
+        }
+        if (threadIdx.x == 0 && blockIdx.x == fb) {
+            if constexpr (MULTI) {
+                SlotState& S = a.st[slot];
+                if (S.enabled && S.inner_on) {
+                    S.its = its;
+                    S.residual_in = residual;
+                    S.initial = initial;
+                    S.status_in = status;
+                    S.done = 1;
+                }
+            } else {
+                PcgScalars* sc = a.sc;
+                sc->iterations = its;
+                sc->residual = residual;
+                sc->initial = initial;
+                sc->status = status;
+                sc->done = 1;
+            }
         }
     }
 }
