@@ -1,5 +1,8 @@
-"""The one-reduction recurrence of the on-chip inner solve, emulated in FP32 on
-the oracle's packed rows against the classic recurrence.
+"""The recurrences of the on-chip inner solve, emulated in FP32 on the
+oracle's packed rows against the classic recurrence: the one-reduction form
+(k_pcg_expanded) and the regrouped product of the one-scene range kernel
+(k_pcg_persistent), which forms q = A p as A z + beta q_old so that the
+in-range part of A z can be computed inside the r.z reduction.
 
 The classic PCG loop (src/solver.rs:1857-1911) sums p.Ap for alpha, then the
 updated r.z for beta: two grid-wide reductions per iteration on the device. The
@@ -107,4 +110,43 @@ def test_expanded_recurrence_takes_the_classic_iterations(make):
         xe, ke = expanded(A, M, b, tol, 5000)
         err = np.linalg.norm(xe - xc) / np.linalg.norm(xc)
         assert ke == kc, (tol, kc, ke)
+        assert err < 2e-6, (tol, err)
+
+
+def regrouped(A, M, b, tol, maxit):
+    """The classic loop with q = A p formed as A z + beta q_old (A is linear)."""
+    x = np.zeros_like(b)
+    r = b.copy()
+    z = M(r)
+    p, q = np.zeros_like(b), np.zeros_like(b)
+    rz, rz_prev = dot(r, z), None
+    init = np.sqrt(dot(r, r))
+    for k in range(maxit):
+        beta = np.float32(0.0) if k == 0 else np.float32(rz / rz_prev)
+        az = A(z)
+        p = (beta * p + z).astype(np.float32)
+        q = (beta * q + az).astype(np.float32)
+        alpha = np.float32(rz / dot(p, q))
+        x = (x + alpha * p).astype(np.float32)
+        r = (r - alpha * q).astype(np.float32)
+        z = M(r)
+        rz_prev, rz = rz, dot(r, z)
+        if np.sqrt(dot(r, r)) / init < tol:
+            return x, k + 1
+    return x, maxit
+
+
+@pytest.mark.parametrize("make", [lambda: S.mixed_block(8, seed=1), lambda: S.mixed_block(12, seed=3),
+                                  lambda: S.damaged_lattice(10, seed=2)], ids=["mixed_8", "mixed_12", "damaged_10"])
+def test_regrouped_product_takes_the_classic_iterations(make):
+    s = make()
+    o = O.OracleScene(s)
+    o.fit_rotations()
+    o.assemble(1e-3)
+    A, M, b = operator(o.pack_rows())
+    for tol in (1e-4, 1e-5, 1e-6):
+        xc, kc = classic(A, M, b, tol, 5000)
+        xg, kg = regrouped(A, M, b, tol, 5000)
+        err = np.linalg.norm(xg - xc) / np.linalg.norm(xc)
+        assert kg == kc, (tol, kc, kg)
         assert err < 2e-6, (tol, err)
